@@ -1,0 +1,172 @@
+/*
+ * sht.h -- C ABI of libsht, a B200 (sm_100a) spherical harmonic transform for
+ * SpeedyWeather.jl's SpeedyTransforms.
+ *
+ * Every entry point takes plain pointers and sizes. Array arguments are
+ * caller-owned DEVICE memory in the reference layouts:
+ *
+ *   grid   : float  field[k * ldg + ij]      ij ring-major (0..360E within a ring,
+ *                                             rings north to south), ldg >= npoints
+ *            (RingGrids/src/field.jl:1-20, Field{T,N}.data[npoints, k])
+ *   coeffs : float2 coeffs[k * ldc + lm]     complex, packed lower triangle,
+ *                                             order m outer, degree l inner,
+ *                                             ldc >= nlm (interleaved re, im)
+ *            (LowerTriangularArrays/src/lower_triangular_array.jl:10-19,
+ *             LowerTriangularArrays/src/spectrum.jl:99-131)
+ *
+ * lmax and mmax are the reference's 1-based sizes (Spectrum(lmax, mmax)).
+ * All calls return an int status: SHT_OK, or SHT_EINVAL for sizes that do not
+ * match the plan (the reference throws DimensionMismatch,
+ * SpeedyTransforms/src/spectral_transform.jl:387-423), SHT_ECUDA for a CUDA
+ * error, SHT_ENOMEM when device memory runs out. sht_last_error() gives the
+ * message of the last failure on the calling thread.
+ *
+ * Work is enqueued on the given stream (NULL = legacy default stream) and is
+ * asynchronous; no call on the hot path allocates or synchronises.
+ */
+#ifndef SHT_H
+#define SHT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SHT_API __attribute__((visibility("default")))
+#else
+#define SHT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHT_OK 0
+#define SHT_EINVAL 1
+#define SHT_ECUDA 2
+#define SHT_ENOMEM 3
+#define SHT_EUNSUPPORTED 4
+
+/* grid kinds (RingGrids/src/grids/full_gaussian.jl, octahedral_gaussian.jl) */
+#define SHT_GRID_FULL_GAUSSIAN 0
+#define SHT_GRID_OCTAHEDRAL_GAUSSIAN 1
+
+/* Legendre-stage arithmetic */
+#define SHT_PREC_FP32 0          /* FP32 CUDA-core FMA, matches the reference's Float32 */
+#define SHT_PREC_BF16X3 1        /* tcgen05, split-BF16 hi/lo operands, 3 products, FP32 accumulate */
+#define SHT_PREC_FP16X3 2        /* tcgen05, split-FP16 hi/lo with power-of-2 per-(m, ring) and
+                                    per-(m, column) scaling, 3 products, FP32 accumulate */
+
+/* Legendre shortcuts (SpeedyTransforms/src/legendre_shortcuts.jl:21-49) */
+#define SHT_SHORTCUT_LINEAR 0
+#define SHT_SHORTCUT_QUADRATIC 1
+#define SHT_SHORTCUT_CUBIC 2
+#define SHT_SHORTCUT_LINQUADCOSLAT2 3
+#define SHT_SHORTCUT_LINCUBCOSLAT 4
+
+/* flags */
+#define SHT_UNSCALE_COSLAT 1u    /* synthesis: divide by cos(latitude) on the fly */
+#define SHT_ADD 2u               /* accumulate into the output instead of overwriting */
+#define SHT_FLIPSIGN 4u          /* operators: negate the result */
+#define SHT_INVERSE 8u           /* laplace: inverse Laplacian */
+
+typedef struct sht_plan sht_plan;
+
+typedef struct {
+    int grid;          /* SHT_GRID_* */
+    int nlat_half;     /* rings per hemisphere */
+    int lmax;          /* 1-based number of degrees (Spectrum.lmax) */
+    int mmax;          /* 1-based number of orders  (Spectrum.mmax) */
+    int nlayers;       /* largest K any call may pass (sizes the plan's scratch) */
+    int precision;     /* SHT_PREC_* */
+    int shortcut;      /* SHT_SHORTCUT_* */
+    int device;        /* CUDA device ordinal the plan lives on */
+} sht_desc;
+
+typedef struct {
+    int64_t npoints;        /* grid points of one layer */
+    int64_t nlm;            /* packed spectral coefficients of one layer */
+    int32_t nlat;           /* rings */
+    int32_t nlat_half;
+    int32_t nlon_max;
+    int32_t nfreq_max;
+    int32_t lmax, mmax;
+    int32_t nlayers;
+    int32_t precision;
+    int64_t scratch_bytes;  /* device scratch the plan owns (Fourier coefficients) */
+    int64_t table_bytes;    /* device bytes of precomputed tables */
+} sht_info;
+
+/* SpectralTransform(spectrum, grid; NF, nlayers, LegendreShortcut)
+ * replaces SpeedyTransforms/src/spectral_transform.jl:118-302 (precompute: Gaussian
+ * latitudes and weights, mmax_truncation, Legendre polynomials, solid angles,
+ * gradient factors, scratch). All tables are computed in FP64 on the host and
+ * rounded once. */
+SHT_API int sht_plan_create(const sht_desc* desc, sht_plan** plan);
+SHT_API int sht_plan_destroy(sht_plan* plan);
+SHT_API int sht_plan_info(const sht_plan* plan, sht_info* info);
+
+/* Host copies of the plan's FP64 tables (for users and tests): latitudes in
+ * degrees (nlat), Gaussian weights (nlat), ring lengths (nlat), mmax_truncation
+ * (nlat_half). Any pointer may be NULL. */
+SHT_API int sht_plan_tables(const sht_plan* plan, double* latd, double* weights, int32_t* nlons,
+                    int32_t* mmax_truncation);
+
+/* transform!(field, coeffs, S; unscale_coslat) -- spectral to grid (synthesis)
+ * replaces SpeedyTransforms/src/spectral_transform.jl:515-570
+ *   (_legendre! legendre.jl:38-101 / legendre_ka.jl:74-123, _fourier! fourier.jl:14-21,215-250).
+ * flags: SHT_UNSCALE_COSLAT, SHT_ADD. */
+SHT_API int sht_synthesize(sht_plan* plan, const void* coeffs, int64_t ldc, float* grid, int64_t ldg,
+                   int K, unsigned flags, void* stream);
+
+/* transform!(coeffs, field, S) -- grid to spectral (analysis)
+ * replaces SpeedyTransforms/src/spectral_transform.jl:579-631
+ *   (_fourier! fourier.jl:5-12,129-166, _legendre! legendre.jl:131-195 / legendre_ka.jl:163-200).
+ * flags: SHT_ADD (accumulate onto coeffs, legendre.jl:137-163). */
+SHT_API int sht_analyze(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, int64_t ldc,
+                int K, unsigned flags, void* stream);
+
+/* Split stages, for callers that batch their own Fourier or Legendre work.
+ * The Fourier scratch is the plan's own. sht_legendre_synthesis writes it,
+ * sht_fourier_synthesis reads it; sht_fourier_analysis writes it,
+ * sht_legendre_analysis reads it.
+ * replaces _legendre!/_fourier! (legendre.jl:38,131; fourier.jl:5-21). */
+SHT_API int sht_legendre_synthesis(sht_plan* plan, const void* coeffs, int64_t ldc, int K, void* stream);
+SHT_API int sht_fourier_synthesis(sht_plan* plan, float* grid, int64_t ldg, int K, unsigned flags, void* stream);
+SHT_API int sht_fourier_analysis(sht_plan* plan, const float* grid, int64_t ldg, int K, void* stream);
+SHT_API int sht_legendre_analysis(sht_plan* plan, void* coeffs, int64_t ldc, int K, unsigned flags, void* stream);
+
+/* curl!(curl, u, v, S; flipsign, add, radius) / divergence!(div, u, v, S; ...)
+ * replaces SpeedyTransforms/src/spectral_gradients.jl:30-125. u, v, out: [nlm, K] complex,
+ * leading dimension ldc. flags: SHT_FLIPSIGN, SHT_ADD. Requires lmax = mmax + 1 for the
+ * result to be a correct vector operator (as the reference). */
+SHT_API int sht_curl(sht_plan* plan, void* out, const void* u, const void* v, int64_t ldc, int K,
+             unsigned flags, double radius, void* stream);
+SHT_API int sht_divergence(sht_plan* plan, void* out, const void* u, const void* v, int64_t ldc, int K,
+                   unsigned flags, double radius, void* stream);
+
+/* UV_from_vor!(U, V, vor, S; radius) and UV_from_vordiv!(U, V, vor, div, S; radius)
+ * replaces SpeedyTransforms/src/spectral_gradients.jl:248-366. div may be NULL (UV_from_vor). */
+SHT_API int sht_uv_from_vordiv(sht_plan* plan, void* U, void* V, const void* vor, const void* div,
+                       int64_t ldc, int K, double radius, void* stream);
+
+/* ∇²!(out, alms, S; add, flipsign, inverse, radius)
+ * replaces SpeedyTransforms/src/spectral_gradients.jl:386-421 (∇⁻²! with SHT_INVERSE). */
+SHT_API int sht_laplace(sht_plan* plan, void* out, const void* alms, int64_t ldc, int K, unsigned flags,
+                double radius, void* stream);
+
+/* ∇!(dpdx, dpdy, p, S; radius)
+ * replaces SpeedyTransforms/src/spectral_gradients.jl:483-527. */
+SHT_API int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p, int64_t ldc, int K,
+                 double radius, void* stream);
+
+/* Message of the last failed call on this thread ("" if none). */
+SHT_API const char* sht_last_error(void);
+
+/* Library version string. */
+SHT_API const char* sht_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHT_H */

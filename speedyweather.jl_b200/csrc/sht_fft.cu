@@ -1,0 +1,311 @@
+// Fourier stage of the spherical harmonic transform: one launch per direction
+// covers every ring pair and every layer of a full or octahedral Gaussian grid.
+//
+// Replaces the per-ring FFTW/cuFFT plans of SpeedyTransforms/src/fourier.jl:129-292
+// and the gather/FFT/scatter CUDA graph of SpeedyTransforms/ext/gpu_graphs_common.jl:199-260.
+//
+// Design: one CTA per (northern ring j, chunk of C layers). The northern and the
+// mirrored southern ring have the same length n, so their real sequences are
+// packed into one complex sequence z = f_N + i f_S and transformed together by a
+// mixed-radix Stockham FFT in shared memory (radices 2, 3, 4, 5, 7 in registers,
+// any larger prime by a symmetric direct DFT). Twiddles come from a per-ring
+// table exp(-2 pi i t / n) computed in FP64 on the host.
+//
+// The Fourier scratch holds, per ring j and order m <= mt(j), the even and odd
+// hemispheric combinations the Legendre stage contracts with
+//   E = dOmega_j (F_N + F_S),  O = dOmega_j (F_N - F_S)         (analysis)
+//   G_N = E + O,  G_S = E - O                                   (synthesis)
+// laid out [row = gofs_j + m][eo][k] complex FP32 (k = layer, fastest).
+// FFTW's conventions are kept: r2c and c2r are unnormalised and c2r ignores the
+// imaginary parts of the DC and Nyquist bins.
+#include "sht_internal.h"
+
+namespace sht {
+
+namespace {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+template <bool INV>
+__device__ __forceinline__ float2 twmul(float2 v, float2 w) {
+    return INV ? cmulc(v, w) : cmul(v, w);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// y = DFT_P(v) (forward: exp(-2 pi i rs/P); inverse: exp(+...)). W is the ring's
+// table exp(-2 pi i t / n); W_P^t = W[t * (n / P)].
+template <int P, bool INV>
+__device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P], const float2* W, int pstride) {
+    if constexpr (P == 2) {
+        y[0] = cadd(v[0], v[1]);
+        y[1] = csub(v[0], v[1]);
+    } else if constexpr (P == 4) {
+        const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        const float2 s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
+        // forward: y1 = d02 - i d13, y3 = d02 + i d13
+        const float2 jd = INV ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);
+        y[0] = cadd(s02, s13);
+        y[2] = csub(s02, s13);
+        y[1] = cadd(d02, jd);
+        y[3] = csub(d02, jd);
+    } else {
+        // odd P: symmetric direct DFT, y_r and y_{P-r} share the sums
+        constexpr int H = (P - 1) / 2;
+        float2 s = v[0];
+#pragma unroll
+        for (int q = 1; q < P; ++q) s = cadd(s, v[q]);
+        y[0] = s;
+#pragma unroll
+        for (int r = 1; r <= H; ++r) {
+            float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int q = 1; q <= H; ++q) {
+                const float2 w = W[((r * q) % P) * pstride];
+                const float cs = w.x, sn = -w.y;
+                const float2 a = cadd(v[q], v[P - q]);
+                const float2 b = csub(v[q], v[P - q]);
+                A.x = fmaf(a.x, cs, A.x); A.y = fmaf(a.y, cs, A.y);
+                B.x = fmaf(b.x, sn, B.x); B.y = fmaf(b.y, sn, B.y);
+            }
+            if (!INV) {
+                y[r] = make_float2(v[0].x + A.x + B.y, v[0].y + A.y - B.x);
+                y[P - r] = make_float2(v[0].x + A.x - B.y, v[0].y + A.y + B.x);
+            } else {
+                y[r] = make_float2(v[0].x + A.x - B.y, v[0].y + A.y + B.x);
+                y[P - r] = make_float2(v[0].x + A.x + B.y, v[0].y + A.y - B.x);
+            }
+        }
+    }
+}
+
+// One Stockham stage of radix P over C vectors of length n; Ns = product of the
+// radices of earlier stages. Output in natural order after the last stage.
+template <int P, bool INV>
+__device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y, int n, int C, int Ns,
+                            const float2* __restrict__ W) {
+    const int nb = n / P;
+    const int tstride = n / (Ns * P);
+    for (int w = threadIdx.x; w < C * nb; w += blockDim.x) {
+        const int c = w / nb;
+        const int b = w - c * nb;
+        const int k = b % Ns;
+        const float2* x = X + (size_t)c * n + b;
+        float2 v[P];
+#pragma unroll
+        for (int r = 0; r < P; ++r) {
+            float2 t = x[r * nb];
+            if (r > 0) t = twmul<INV>(t, W[r * k * tstride]);
+            v[r] = t;
+        }
+        float2 y[P];
+        dft_small<P, INV>(v, y, W, nb);
+        float2* yo = Y + (size_t)c * n + (b - k) * P + k;
+#pragma unroll
+        for (int r = 0; r < P; ++r) yo[r * Ns] = y[r];
+    }
+}
+
+// Stage of a large odd prime radix p: twiddle in place, then the symmetric direct DFT
+// with one work item per output pair (y_r, y_{p-r}).
+template <bool INV>
+__device__ void stage_generic(float2* __restrict__ X, float2* __restrict__ Y, int n, int C, int Ns, int p,
+                              const float2* __restrict__ W) {
+    const int nb = n / p;
+    const int tstride = n / (Ns * p);
+    for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
+        const int c = w / n;
+        const int i = w - c * n;
+        const int r = i / nb;
+        const int b = i - r * nb;
+        const int k = b % Ns;
+        if (r > 0 && k > 0) X[(size_t)c * n + i] = twmul<INV>(X[(size_t)c * n + i], W[r * k * tstride]);
+    }
+    __syncthreads();
+    const int half = (p - 1) / 2;
+    const int items = C * nb * (half + 1);
+    for (int w = threadIdx.x; w < items; w += blockDim.x) {
+        const int r = w % (half + 1);
+        const int cb = w / (half + 1);
+        const int c = cb / nb;
+        const int b = cb - c * nb;
+        const int k = b % Ns;
+        const float2* x = X + (size_t)c * n + b;
+        float2* yo = Y + (size_t)c * n + (b - k) * p + k;
+        const float2 x0 = x[0];
+        if (r == 0) {
+            float2 s = x0;
+            for (int q = 1; q < p; ++q) s = cadd(s, x[q * nb]);
+            yo[0] = s;
+        } else {
+            float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
+            int idx = 0;
+            for (int q = 1; q <= half; ++q) {
+                idx += r;
+                if (idx >= p) idx -= p;
+                const float2 w_ = W[idx * nb];
+                const float cs = w_.x, sn = -w_.y;
+                const float2 a = x[q * nb], bq = x[(p - q) * nb];
+                A.x = fmaf(a.x + bq.x, cs, A.x); A.y = fmaf(a.y + bq.y, cs, A.y);
+                B.x = fmaf(a.x - bq.x, sn, B.x); B.y = fmaf(a.y - bq.y, sn, B.y);
+            }
+            float2 yr, ypr;
+            if (!INV) {
+                yr = make_float2(x0.x + A.x + B.y, x0.y + A.y - B.x);
+                ypr = make_float2(x0.x + A.x - B.y, x0.y + A.y + B.x);
+            } else {
+                yr = make_float2(x0.x + A.x - B.y, x0.y + A.y + B.x);
+                ypr = make_float2(x0.x + A.x + B.y, x0.y + A.y - B.x);
+            }
+            yo[r * Ns] = yr;
+            yo[(p - r) * Ns] = ypr;
+        }
+    }
+}
+
+// Runs all stages; returns the buffer holding the result.
+template <bool INV>
+__device__ float2* run_fft(float2* X, float2* Y, int n, int C, const RingDesc& rd, const float2* W) {
+    int Ns = 1;
+    for (int s = 0; s < rd.nfac; ++s) {
+        const int p = rd.fac[s];
+        switch (p) {
+            case 2: stage_small<2, INV>(X, Y, n, C, Ns, W); break;
+            case 3: stage_small<3, INV>(X, Y, n, C, Ns, W); break;
+            case 4: stage_small<4, INV>(X, Y, n, C, Ns, W); break;
+            case 5: stage_small<5, INV>(X, Y, n, C, Ns, W); break;
+            case 7: stage_small<7, INV>(X, Y, n, C, Ns, W); break;
+            default: stage_generic<INV>(X, Y, n, C, Ns, p, W); break;
+        }
+        __syncthreads();
+        float2* t = X; X = Y; Y = t;
+        Ns *= p;
+    }
+    return X;
+}
+
+__device__ __forceinline__ int smem_tw_len(int n) { return (n + 1) & ~1; }
+
+// grid -> Fourier scratch (E/O combinations weighted by the solid angle)
+__global__ void __launch_bounds__(512) fft_analysis_kernel(const RingDesc* __restrict__ rings,
+                                                           const float2* __restrict__ twiddle,
+                                                           const float* __restrict__ grid, int64_t ldg,
+                                                           float2* __restrict__ four, int K) {
+    extern __shared__ float2 sm[];
+    const RingDesc& rd = rings[blockIdx.x];
+    const int k0 = blockIdx.y * rd.chunk;
+    if (k0 >= K) return;
+    const int C = min(rd.chunk, K - k0);
+    const int n = rd.n;
+    float2* W = sm;
+    float2* X = sm + smem_tw_len(n);
+    float2* Y = X + (size_t)C * n;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) W[t] = twiddle[rd.tw_off + t];
+    for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
+        const int c = w / n;
+        const int i = w - c * n;
+        const float* g = grid + (int64_t)(k0 + c) * ldg;
+        X[w] = make_float2(g[rd.off_north + i], g[rd.off_south + i]);
+    }
+    __syncthreads();
+    const float2* Z = run_fft<false>(X, Y, n, C, rd, W);
+    const float half_domega = 0.5f * rd.domega;
+    const int nm = rd.mt + 1;
+    for (int w = threadIdx.x; w < C * nm; w += blockDim.x) {
+        const int c = w % C;
+        const int m = w / C;
+        const float2 a = Z[(size_t)c * n + m];
+        const float2 b = Z[(size_t)c * n + (m == 0 ? 0 : n - m)];
+        // F_N = (a + conj b)/2, F_S = (a - conj b)/(2i)
+        const float2 fn = make_float2(a.x + b.x, a.y - b.y);
+        const float2 fs = make_float2(a.y + b.y, b.x - a.x);
+        const float2 e = make_float2(half_domega * (fn.x + fs.x), half_domega * (fn.y + fs.y));
+        const float2 o = make_float2(half_domega * (fn.x - fs.x), half_domega * (fn.y - fs.y));
+        const int64_t row = (rd.gofs + m) * 2;
+        four[row * K + k0 + c] = e;
+        four[(row + 1) * K + k0 + c] = o;
+    }
+}
+
+// Fourier scratch -> grid
+__global__ void __launch_bounds__(512) fft_synthesis_kernel(const RingDesc* __restrict__ rings,
+                                                            const float2* __restrict__ twiddle,
+                                                            const float2* __restrict__ four, float* __restrict__ grid,
+                                                            int64_t ldg, int K, int unscale, int add) {
+    extern __shared__ float2 sm[];
+    const RingDesc& rd = rings[blockIdx.x];
+    const int k0 = blockIdx.y * rd.chunk;
+    if (k0 >= K) return;
+    const int C = min(rd.chunk, K - k0);
+    const int n = rd.n;
+    float2* W = sm;
+    float2* X = sm + smem_tw_len(n);
+    float2* Y = X + (size_t)C * n;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) W[t] = twiddle[rd.tw_off + t];
+    const float scale = unscale ? rd.coslat_inv : 1.0f;
+    const int nhalf = n / 2;   // highest source frequency
+    for (int w = threadIdx.x; w < C * (nhalf + 1); w += blockDim.x) {
+        const int c = w % C;
+        const int m = w / C;
+        float2 gn = make_float2(0.f, 0.f), gs = make_float2(0.f, 0.f);
+        if (m <= rd.mt) {
+            const int64_t row = (rd.gofs + m) * 2;
+            const float2 e = four[row * K + k0 + c];
+            const float2 o = four[(row + 1) * K + k0 + c];
+            gn = make_float2(scale * (e.x + o.x), scale * (e.y + o.y));
+            gs = make_float2(scale * (e.x - o.x), scale * (e.y - o.y));
+        }
+        const bool selfconj = (m == 0) || (2 * m == n);
+        if (selfconj) {
+            X[(size_t)c * n + m] = make_float2(gn.x, gs.x);
+        } else {
+            X[(size_t)c * n + m] = make_float2(gn.x - gs.y, gn.y + gs.x);
+            X[(size_t)c * n + (n - m)] = make_float2(gn.x + gs.y, gs.x - gn.y);
+        }
+    }
+    __syncthreads();
+    const float2* z = run_fft<true>(X, Y, n, C, rd, W);
+    for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
+        const int c = w / n;
+        const int i = w - c * n;
+        float* g = grid + (int64_t)(k0 + c) * ldg;
+        const float2 v = z[w];
+        if (add) {
+            g[rd.off_north + i] += v.x;
+            g[rd.off_south + i] += v.y;
+        } else {
+            g[rd.off_north + i] = v.x;
+            g[rd.off_south + i] = v.y;
+        }
+    }
+}
+
+}  // namespace
+
+static int fft_threads(const Plan&) { return 512; }
+
+cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s) {
+    dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);
+    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_rings, p.d_twiddle, grid, ldg, p.d_four, K);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags, cudaStream_t s) {
+    dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);
+    fft_synthesis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_rings, p.d_twiddle, p.d_four, grid, ldg, K,
+                                                               (flags & SHT_UNSCALE_COSLAT) ? 1 : 0,
+                                                               (flags & SHT_ADD) ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t fft_set_smem(int bytes) {
+    cudaError_t e = cudaFuncSetAttribute(fft_analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(fft_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+}  // namespace sht

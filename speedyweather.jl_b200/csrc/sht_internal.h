@@ -1,0 +1,107 @@
+// Internal declarations of libsht: the plan object, its device tables and the
+// kernel launchers. Not part of the C ABI (include/sht.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/sht.h"
+
+namespace sht {
+
+constexpr int kMaxFactors = 24;      // radices per ring FFT (n <= 2^24)
+
+// Per-ring real-FFT description, indexed by the northern ring j (0-based).
+// The southern mirror ring has the same length.
+struct RingDesc {
+    int32_t n;            // points on the ring
+    int32_t mt;           // mmax_truncation (0-based highest order kept)
+    int32_t nfac;         // number of Stockham stages
+    int32_t chunk;        // layers per CTA in the FFT kernels
+    int64_t off_north;    // first grid point of the northern ring
+    int64_t off_south;    // first grid point of the southern ring
+    int64_t gofs;         // first Fourier-scratch row (m = 0) of this ring
+    int64_t tw_off;       // offset of this ring's twiddle table (n entries)
+    float domega;         // solid angle w_j 2pi / n_j
+    float coslat_inv;     // 1 / cos(latitude)
+    int32_t fac[kMaxFactors];
+};
+
+// One tile of the Legendre contraction of order m.
+struct LegItem {
+    int32_t m;
+    int32_t tile;         // ring tile (synthesis) or parity-row tile (analysis)
+};
+
+struct Plan {
+    sht_desc d{};
+    int nh = 0, nlat = 0, lmax = 0, mmax = 0, nlon_max = 0, nfreq_max = 0;
+    int64_t npoints = 0, nlm = 0;
+    int64_t scratch_rows = 0;           // sum_j (mt_j + 1)
+    int device = 0;
+
+    // host copies (FP64 where computed so)
+    std::vector<double> latd, weights;  // nlat
+    std::vector<int32_t> nlons;         // nlat
+    std::vector<int32_t> mt;            // nh
+    std::vector<int32_t> j0;            // per m: first northern ring with mt >= m (nh if none)
+    std::vector<int64_t> lm_off;        // per m: packed offset of (l = m, m)
+    std::vector<int32_t> rows;          // per m: parity rows ceil((lmax - m) / 2)
+    std::vector<int64_t> lam_off;       // per m: offset into the FP32 Legendre table
+    int nh_pad = 0;
+
+    // device tables
+    RingDesc* d_rings = nullptr;
+    float2* d_twiddle = nullptr;
+    float* d_lam = nullptr;             // [m][parity][row][nh_pad], FP32
+    int64_t* d_lam_off = nullptr;
+    int32_t* d_j0 = nullptr;
+    int32_t* d_rows = nullptr;
+    int64_t* d_lm_off = nullptr;
+    LegItem* d_syn_items = nullptr;  int n_syn_items = 0;
+    LegItem* d_ana_items = nullptr;  int n_ana_items = 0;
+    int32_t* d_mt = nullptr;
+    int64_t* d_gofs = nullptr;
+
+    // spectral operator factors, per packed lm (FP32, computed in FP64)
+    float* d_grad = nullptr;            // 8 arrays of nlm: see GradIdx
+    int32_t* d_l_of = nullptr;          // 0-based degree of each lm
+    int32_t* d_m_of = nullptr;          // 0-based order of each lm
+    float* d_eig = nullptr;             // lmax: -l(l+1)
+    float* d_eig_inv = nullptr;         // lmax: 1/(-l(l+1)), 0 at l = 0
+
+    // scratch: Fourier coefficients, [row = gofs_j + m][eo][k] complex FP32
+    float2* d_four = nullptr;
+    int64_t four_elems = 0;
+
+    int64_t table_bytes = 0;
+    int smem_fft = 0;                   // dynamic shared memory of the FFT kernels
+    int max_chunk_groups = 0;           // grid.y upper bound factor for FFT launch
+    int min_chunk = 1;
+};
+
+enum GradIdx {
+    G_GRAD_Y1 = 0, G_GRAD_Y2, G_GRAD_Y_VORDIV1, G_GRAD_Y_VORDIV2, G_GRAD_X_VORDIV,
+    G_VORDIV_TO_UV_X, G_VORDIV_TO_UV1, G_VORDIV_TO_UV2, G_COUNT
+};
+
+// ---- launchers (return cudaError_t of the launch) ----------------------------------
+cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s);
+cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags,
+                                 cudaStream_t s);
+cudaError_t launch_legendre_synthesis_fp32(const Plan& p, const float2* coeffs, int64_t ldc, int K,
+                                           cudaStream_t s);
+cudaError_t launch_legendre_analysis_fp32(const Plan& p, float2* coeffs, int64_t ldc, int K, bool add,
+                                          cudaStream_t s);
+cudaError_t launch_divcurl(const Plan& p, float2* out, const float2* u, const float2* v, int64_t ldc,
+                           int K, bool curl, bool flipsign, bool add, float inv_radius, cudaStream_t s);
+cudaError_t launch_uv_from_vordiv(const Plan& p, float2* U, float2* V, const float2* vor,
+                                  const float2* div, int64_t ldc, int K, float radius, cudaStream_t s);
+cudaError_t launch_laplace(const Plan& p, float2* out, const float2* in, int64_t ldc, int K,
+                           bool inverse, bool flipsign, bool add, float scale, cudaStream_t s);
+cudaError_t launch_gradient(const Plan& p, float2* dpdx, float2* dpdy, const float2* in, int64_t ldc,
+                            int K, float inv_radius, cudaStream_t s);
+
+}  // namespace sht

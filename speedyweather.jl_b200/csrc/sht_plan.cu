@@ -1,0 +1,624 @@
+// libsht host side: the plan (precomputed tables, computed once in FP64 on the
+// host and rounded once), argument checking, and the C ABI of include/sht.h.
+//
+// Replaces the SpectralTransform constructor, SpeedyTransforms/src/spectral_transform.jl:118-302,
+// and the transform!/operator entry points (spectral_transform.jl:515-631,
+// spectral_gradients.jl).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <new>
+#include <thread>
+
+#include "sht_internal.h"
+
+namespace sht {
+cudaError_t fft_set_smem(int bytes);
+cudaError_t tc_prepare(Plan& p);       // tensor-core Legendre tables (sht_legendre_tc.cu)
+void tc_release(Plan& p);
+int tc_supported();
+cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, int64_t ldc, int K, cudaStream_t s);
+cudaError_t launch_legendre_analysis_tc(const Plan& p, float2* coeffs, int64_t ldc, int K, bool add, cudaStream_t s);
+}  // namespace sht
+
+using namespace sht;
+
+struct sht_plan {
+    Plan p;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    if (e == cudaErrorMemoryAllocation) return fail(SHT_ENOMEM, "%s: %s", where, cudaGetErrorString(e));
+    return fail(SHT_ECUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+// n-point Gauss-Legendre nodes (ascending) and weights in FP64: Newton iteration on
+// P_n (restates FastGaussQuadrature.gausslegendre, RingGrids/src/quadrature_weights.jl:11).
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    const int half = (n + 1) / 2;
+    for (int i = 0; i < half; ++i) {
+        double z = std::cos(M_PI * (i + 0.75) / (n + 0.5));
+        double dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= n; ++k) {
+                const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1.0);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        double p0 = 1.0, p1 = z;
+        for (int k = 2; k <= n; ++k) {
+            const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+            p0 = p1;
+            p1 = p2;
+        }
+        dp = n * (z * p1 - p0) / (z * z - 1.0);
+        const double wt = 2.0 / ((1.0 - z * z) * dp * dp);
+        // z is descending from ~1; store ascending
+        x[n - 1 - i] = z;
+        w[n - 1 - i] = wt;
+        x[i] = -z;
+        w[i] = wt;
+    }
+    if (n % 2 == 1) x[n / 2] = 0.0;
+}
+
+// Prime factorisation into Stockham radices: 4s first, then 2, 3, 5, 7, larger primes.
+int factorize(int n, int32_t* fac) {
+    std::vector<int> f;
+    int m = n;
+    for (int p = 2; (int64_t)p * p <= m; ++p)
+        while (m % p == 0) {
+            f.push_back(p);
+            m /= p;
+        }
+    if (m > 1) f.push_back(m);
+    const int twos = (int)std::count(f.begin(), f.end(), 2);
+    std::vector<int> out;
+    for (int i = 0; i < twos / 2; ++i) out.push_back(4);
+    if (twos % 2) out.push_back(2);
+    for (int q : f)
+        if (q != 2) out.push_back(q);
+    if ((int)out.size() > kMaxFactors) return -1;
+    for (size_t i = 0; i < out.size(); ++i) fac[i] = out[i];
+    return (int)out.size();
+}
+
+int shortcut_mt(int kind, int nlon, double latd) {
+    switch (kind) {
+        case SHT_SHORTCUT_LINEAR: return nlon / 2;
+        case SHT_SHORTCUT_QUADRATIC: return nlon / 3;
+        case SHT_SHORTCUT_CUBIC: return nlon / 4;
+        case SHT_SHORTCUT_LINQUADCOSLAT2: {
+            const double c = std::cos(latd * M_PI / 180.0);
+            return (int)std::floor(nlon / (2.0 + c * c));
+        }
+        case SHT_SHORTCUT_LINCUBCOSLAT: {
+            const double c = std::cos(latd * M_PI / 180.0);
+            return (int)std::floor(nlon / (2.0 + 2.0 * c));
+        }
+        default: return -1;
+    }
+}
+
+template <class T>
+cudaError_t upload(T** dst, const std::vector<T>& src, int64_t& bytes) {
+    const size_t nb = std::max<size_t>(1, src.size()) * sizeof(T);
+    cudaError_t e = cudaMalloc((void**)dst, nb);
+    if (e != cudaSuccess) return e;
+    bytes += (int64_t)nb;
+    if (!src.empty()) e = cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+void release(Plan& p) {
+    tc_release(p);
+    void* ptrs[] = {p.d_rings, p.d_twiddle, p.d_lam, p.d_lam_off, p.d_j0, p.d_rows, p.d_lm_off, p.d_syn_items,
+                    p.d_ana_items, p.d_mt, p.d_gofs, p.d_grad, p.d_l_of, p.d_m_of, p.d_eig, p.d_eig_inv, p.d_four};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            ok = false;
+            return;
+        }
+        if (prev != dev && cudaSetDevice(dev) != cudaSuccess) ok = false;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int build_plan(Plan& p) {
+    const sht_desc& d = p.d;
+    p.nh = d.nlat_half;
+    p.nlat = 2 * d.nlat_half;
+    p.lmax = d.lmax;
+    p.mmax = d.mmax;
+    const int nh = p.nh;
+    p.nlm = (int64_t)p.lmax * p.mmax - (int64_t)p.mmax * (p.mmax - 1) / 2;
+
+    // --- grid (RingGrids) ---
+    std::vector<int32_t> half(nh);
+    for (int j = 0; j < nh; ++j)
+        half[j] = d.grid == SHT_GRID_FULL_GAUSSIAN ? 4 * nh : 16 + 4 * (j + 1);  // full_gaussian.jl:45,
+                                                                                // octahedral_gaussian.jl:64-70
+    p.nlons.resize(p.nlat);
+    for (int j = 0; j < nh; ++j) {
+        p.nlons[j] = half[j];
+        p.nlons[p.nlat - 1 - j] = half[j];
+    }
+    std::vector<int64_t> ring_start(p.nlat + 1, 0);
+    for (int j = 0; j < p.nlat; ++j) ring_start[j + 1] = ring_start[j] + p.nlons[j];
+    p.npoints = ring_start[p.nlat];
+    p.nlon_max = *std::max_element(p.nlons.begin(), p.nlons.end());
+    p.nfreq_max = p.nlon_max / 2 + 1;
+
+    std::vector<double> x, w;
+    gauss_legendre(p.nlat, x, w);
+    p.latd.resize(p.nlat);
+    p.weights = w;
+    for (int j = 0; j < p.nlat; ++j) p.latd[j] = std::acos(x[j]) * 180.0 / M_PI - 90.0;  // full_gaussian.jl:48-50
+
+    // --- Legendre shortcut (spectral_transform.jl:154-155) ---
+    p.mt.resize(nh);
+    for (int j = 0; j < nh; ++j) {
+        const int t = shortcut_mt(d.shortcut, half[j], p.latd[j]);
+        if (t < 0) return fail(SHT_EINVAL, "unknown Legendre shortcut %d", d.shortcut);
+        p.mt[j] = std::min(t, p.mmax - 1);
+    }
+    p.j0.assign(p.mmax, nh);
+    for (int m = 0; m < p.mmax; ++m)
+        for (int j = 0; j < nh; ++j)
+            if (p.mt[j] >= m) {
+                p.j0[m] = j;
+                break;
+            }
+
+    // --- spectral layout + Legendre table layout ---
+    p.lm_off.resize(p.mmax);
+    p.rows.resize(p.mmax);
+    p.lam_off.resize(p.mmax);
+    p.nh_pad = (nh + 63) / 64 * 64;
+    int64_t lo = 0;
+    for (int m = 0; m < p.mmax; ++m) {
+        p.lm_off[m] = (int64_t)m * p.lmax - (int64_t)m * (m - 1) / 2;
+        p.rows[m] = (p.lmax - m + 1) / 2;
+        p.lam_off[m] = lo;
+        lo += 2LL * p.rows[m] * p.nh_pad;
+    }
+    const int64_t lam_elems = lo;
+
+    // --- Legendre polynomials in FP64, stored FP32: [m][parity][row][nh_pad] ---
+    // lambda_lm (4pi-orthonormal, Condon-Shortley phase), the arithmetic of
+    // AssociatedLegendrePolynomials.lambdalm! called at spectral_transform.jl:167-172.
+    std::vector<float> lam((size_t)lam_elems, 0.0f);
+    {
+        const int nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        auto work = [&](int tid) {
+            std::vector<double> col(p.lmax);
+            for (int j = tid; j < nh; j += nthreads) {
+                const double colat = M_PI / 2 - p.latd[j] * M_PI / 180.0;   // grid.jl:142-143
+                const double xc = std::cos(colat);
+                const double s = std::sqrt(std::max(0.0, 1.0 - xc * xc));
+                double pmm = 1.0 / std::sqrt(4.0 * M_PI);
+                for (int m = 0; m <= p.mt[j]; ++m) {
+                    if (m > 0) pmm = -std::sqrt((2.0 * m + 1.0) / (2.0 * m)) * s * pmm;
+                    const int L = p.lmax - m;
+                    col[0] = pmm;
+                    if (L >= 2) {
+                        double p0 = pmm, p1 = std::sqrt(2.0 * m + 3.0) * xc * pmm;
+                        col[1] = p1;
+                        double a_prev = std::sqrt((4.0 * (m + 1) * (m + 1) - 1.0) / ((m + 1.0) * (m + 1.0) - 1.0 * m * m));
+                        for (int l = m + 2; l < p.lmax; ++l) {
+                            const double a = std::sqrt((4.0 * l * l - 1.0) / (1.0 * l * l - 1.0 * m * m));
+                            const double p2 = a * (xc * p1 - p0 / a_prev);
+                            col[l - m] = p2;
+                            p0 = p1;
+                            p1 = p2;
+                            a_prev = a;
+                        }
+                    }
+                    float* base = lam.data() + p.lam_off[m];
+                    for (int i = 0; i < L; ++i) {
+                        const int par = i & 1, row = i >> 1;
+                        base[((int64_t)par * p.rows[m] + row) * p.nh_pad + j] = (float)col[i];
+                    }
+                }
+            }
+        };
+        std::vector<std::thread> th;
+        for (int t = 0; t < nthreads; ++t) th.emplace_back(work, t);
+        for (auto& t : th) t.join();
+    }
+
+    // --- per-ring FFT descriptors and twiddles (FP64 -> FP32) ---
+    std::vector<RingDesc> rings(nh);
+    std::vector<float2> tw;
+    int64_t gofs = 0;
+    const int smem_budget = 200 * 1024;
+    int max_smem = 0;
+    p.min_chunk = 1 << 30;
+    for (int j = 0; j < nh; ++j) {
+        RingDesc& r = rings[j];
+        std::memset(&r, 0, sizeof r);
+        r.n = half[j];
+        r.mt = p.mt[j];
+        r.nfac = factorize(r.n, r.fac);
+        if (r.nfac < 0) return fail(SHT_EINVAL, "ring length %d has too many factors", r.n);
+        r.off_north = ring_start[j];
+        r.off_south = ring_start[p.nlat - 1 - j];
+        r.gofs = gofs;
+        gofs += r.mt + 1;
+        r.tw_off = (int64_t)tw.size();
+        for (int t = 0; t < r.n; ++t) {
+            const double a = -2.0 * M_PI * t / r.n;
+            tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+        }
+        r.domega = (float)(p.weights[j] * (2.0 * M_PI / r.n));                  // quadrature_weights.jl:48-49
+        r.coslat_inv = (float)(1.0 / std::cos(p.latd[j] * M_PI / 180.0));       // spectral_transform.jl:150-151
+        const int tw_bytes = ((r.n + 1) & ~1) * 8;
+        int chunk = 1;
+        while (chunk * 2 <= 32 && tw_bytes + 2 * (chunk * 2) * r.n * 8 <= smem_budget) chunk *= 2;
+        r.chunk = chunk;
+        p.min_chunk = std::min(p.min_chunk, chunk);
+        max_smem = std::max(max_smem, tw_bytes + 2 * chunk * r.n * 8);
+    }
+    p.scratch_rows = gofs;
+    p.smem_fft = max_smem;
+
+    // --- work lists of the Legendre kernels (64-row tiles, heavy orders first) ---
+    std::vector<LegItem> syn, ana;
+    for (int m = 0; m < p.mmax; ++m) {
+        if (p.j0[m] < nh)
+            for (int t = p.j0[m] / 64; t * 64 < nh; ++t) syn.push_back({m, t});
+        for (int t = 0; t * 64 < p.rows[m]; ++t) ana.push_back({m, t});   // every coefficient is written
+    }
+
+    // --- spectral operator factors (gradient_arrays.jl:1-215) in FP64 -> FP32 ---
+    const int64_t nlm = p.nlm;
+    std::vector<float> grad((size_t)G_COUNT * nlm, 0.0f);
+    std::vector<int32_t> l_of(nlm), m_of(nlm);
+    auto eps = [](double l, double m) { return std::sqrt((l * l - m * m) / (4.0 * l * l - 1.0)); };
+    for (int m = 0; m < p.mmax; ++m)
+        for (int l = m; l < p.lmax; ++l) {
+            const int64_t lm = p.lm_off[m] + (l - m);
+            l_of[lm] = l;
+            m_of[lm] = m;
+            const bool last = (l == p.lmax - 1);
+            const double L1 = l + 1.0;                 // 1-based degree
+            const double e_l = (l == 0 && m == 0) ? 0.0 : eps(l, m);
+            const double e_lp = eps(l + 1.0, m);
+            grad[G_GRAD_Y1 * nlm + lm] = (float)(-(L1 - 2.0) * e_l);
+            grad[G_GRAD_Y2 * nlm + lm] = last ? 0.f : (float)((L1 + 1.0) * e_lp);
+            grad[G_GRAD_Y_VORDIV1 * nlm + lm] = last ? 0.f : (float)(L1 * e_l);
+            grad[G_GRAD_Y_VORDIV2 * nlm + lm] = last ? 0.f : (float)((L1 - 1.0) * e_lp);
+            grad[G_GRAD_X_VORDIV * nlm + lm] = last ? 0.f : (float)m;
+            grad[G_VORDIV_TO_UV_X * nlm + lm] = (lm == 0) ? 0.f : (float)(-m / (L1 * (L1 - 1.0)));
+            grad[G_VORDIV_TO_UV1 * nlm + lm] = (lm == 0) ? 0.f : (float)(e_l / (L1 - 1.0));
+            grad[G_VORDIV_TO_UV2 * nlm + lm] = last ? 0.f : (float)(e_lp / L1);
+        }
+    std::vector<float> eig(p.lmax), eig_inv(p.lmax);
+    for (int l = 0; l < p.lmax; ++l) {
+        const double e = -(double)l * (l + 1.0);
+        eig[l] = (float)e;
+        eig_inv[l] = l == 0 ? 0.f : (float)(1.0 / e);     // gradient_arrays.jl:165-170
+    }
+
+    // --- device upload ---
+    int64_t tb = 0;
+    cudaError_t e;
+#define UP(dst, src)                                          \
+    if ((e = upload(&(dst), (src), tb)) != cudaSuccess) {     \
+        return cuda_fail(e, "sht_plan_create upload " #dst); \
+    }
+    UP(p.d_rings, rings);
+    UP(p.d_twiddle, tw);
+    UP(p.d_lam, lam);
+    UP(p.d_lam_off, p.lam_off);
+    UP(p.d_j0, p.j0);
+    UP(p.d_rows, p.rows);
+    UP(p.d_lm_off, p.lm_off);
+    UP(p.d_syn_items, syn);
+    UP(p.d_ana_items, ana);
+    UP(p.d_mt, p.mt);
+    UP(p.d_grad, grad);
+    UP(p.d_l_of, l_of);
+    UP(p.d_m_of, m_of);
+    UP(p.d_eig, eig);
+    UP(p.d_eig_inv, eig_inv);
+#undef UP
+    std::vector<int64_t> gofs_v(nh);
+    for (int j = 0; j < nh; ++j) gofs_v[j] = rings[j].gofs;
+    if ((e = upload(&p.d_gofs, gofs_v, tb)) != cudaSuccess) return cuda_fail(e, "sht_plan_create upload gofs");
+    p.n_syn_items = (int)syn.size();
+    p.n_ana_items = (int)ana.size();
+    p.table_bytes = tb;
+
+    p.four_elems = p.scratch_rows * 2 * std::max(1, d.nlayers);
+    if ((e = cudaMalloc((void**)&p.d_four, p.four_elems * sizeof(float2))) != cudaSuccess)
+        return cuda_fail(e, "sht_plan_create scratch");
+    if ((e = fft_set_smem(p.smem_fft)) != cudaSuccess) return cuda_fail(e, "sht_plan_create fft smem");
+    if (d.precision != SHT_PREC_FP32) {
+        if (!tc_supported()) return fail(SHT_EUNSUPPORTED, "tensor-core Legendre precision %d not available", d.precision);
+        if ((e = tc_prepare(p)) != cudaSuccess) return cuda_fail(e, "sht_plan_create tensor-core tables");
+    }
+    return SHT_OK;
+}
+
+bool ok_ptr(const void* q) { return q != nullptr; }
+
+int check_call(const sht_plan* plan, int K, const char* what) {
+    if (!plan) return fail(SHT_EINVAL, "%s: plan is NULL", what);
+    if (K < 0 || K > plan->p.d.nlayers)
+        return fail(SHT_EINVAL, "%s: DimensionMismatch: K = %d layers, plan has nlayers = %d", what, K,
+                    plan->p.d.nlayers);
+    return SHT_OK;
+}
+
+int check_ldc(const Plan& p, int64_t ldc, const char* what) {
+    if (ldc < p.nlm)
+        return fail(SHT_EINVAL, "%s: DimensionMismatch: leading dimension %lld < nlm = %lld (lmax=%d, mmax=%d)", what,
+                    (long long)ldc, (long long)p.nlm, p.lmax, p.mmax);
+    return SHT_OK;
+}
+
+int check_ldg(const Plan& p, int64_t ldg, const char* what) {
+    if (ldg < p.npoints)
+        return fail(SHT_EINVAL, "%s: DimensionMismatch: leading dimension %lld < npoints = %lld", what, (long long)ldg,
+                    (long long)p.npoints);
+    return SHT_OK;
+}
+
+int finish(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return SHT_OK;
+}
+
+cudaError_t legendre_synthesis(const Plan& p, const float2* coeffs, int64_t ldc, int K, cudaStream_t s) {
+    if (p.d.precision == SHT_PREC_FP32) return launch_legendre_synthesis_fp32(p, coeffs, ldc, K, s);
+    return launch_legendre_synthesis_tc(p, coeffs, ldc, K, s);
+}
+
+cudaError_t legendre_analysis(const Plan& p, float2* coeffs, int64_t ldc, int K, bool add, cudaStream_t s) {
+    if (p.d.precision == SHT_PREC_FP32) return launch_legendre_analysis_fp32(p, coeffs, ldc, K, add, s);
+    return launch_legendre_analysis_tc(p, coeffs, ldc, K, add, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sht_last_error(void) { return g_last_error.c_str(); }
+const char* sht_version(void) { return "libsht 0.1 (sm_100a)"; }
+
+int sht_plan_create(const sht_desc* desc, sht_plan** out) {
+    if (!desc || !out) return fail(SHT_EINVAL, "sht_plan_create: NULL argument");
+    *out = nullptr;
+    const sht_desc& d = *desc;
+    if (d.grid != SHT_GRID_FULL_GAUSSIAN && d.grid != SHT_GRID_OCTAHEDRAL_GAUSSIAN)
+        return fail(SHT_EUNSUPPORTED, "grid kind %d not supported (full or octahedral Gaussian only)", d.grid);
+    if (d.nlat_half < 1 || d.nlat_half > 8192) return fail(SHT_EINVAL, "nlat_half %d out of range", d.nlat_half);
+    if (d.mmax < 1 || d.lmax < d.mmax || d.lmax > 8192)
+        return fail(SHT_EINVAL, "spectrum lmax=%d mmax=%d invalid (need 1 <= mmax <= lmax)", d.lmax, d.mmax);
+    if (d.nlayers < 1) return fail(SHT_EINVAL, "nlayers %d must be >= 1", d.nlayers);
+    if (d.precision < SHT_PREC_FP32 || d.precision > SHT_PREC_FP16X3)
+        return fail(SHT_EINVAL, "precision %d unknown", d.precision);
+    DeviceGuard g(d.device);
+    if (!g.ok) return fail(SHT_ECUDA, "sht_plan_create: cannot select device %d", d.device);
+    sht_plan* h = new (std::nothrow) sht_plan();
+    if (!h) return fail(SHT_ENOMEM, "sht_plan_create: host allocation failed");
+    h->p.d = d;
+    h->p.device = d.device;
+    const int rc = build_plan(h->p);
+    if (rc != SHT_OK) {
+        release(h->p);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return SHT_OK;
+}
+
+int sht_plan_destroy(sht_plan* plan) {
+    if (!plan) return SHT_OK;
+    DeviceGuard g(plan->p.device);
+    release(plan->p);
+    delete plan;
+    return SHT_OK;
+}
+
+int sht_plan_info(const sht_plan* plan, sht_info* info) {
+    if (!plan || !info) return fail(SHT_EINVAL, "sht_plan_info: NULL argument");
+    const Plan& p = plan->p;
+    info->npoints = p.npoints;
+    info->nlm = p.nlm;
+    info->nlat = p.nlat;
+    info->nlat_half = p.nh;
+    info->nlon_max = p.nlon_max;
+    info->nfreq_max = p.nfreq_max;
+    info->lmax = p.lmax;
+    info->mmax = p.mmax;
+    info->nlayers = p.d.nlayers;
+    info->precision = p.d.precision;
+    info->scratch_bytes = p.four_elems * (int64_t)sizeof(float2);
+    info->table_bytes = p.table_bytes;
+    return SHT_OK;
+}
+
+int sht_plan_tables(const sht_plan* plan, double* latd, double* weights, int32_t* nlons, int32_t* mmax_truncation) {
+    if (!plan) return fail(SHT_EINVAL, "sht_plan_tables: NULL plan");
+    const Plan& p = plan->p;
+    if (latd) std::memcpy(latd, p.latd.data(), p.nlat * sizeof(double));
+    if (weights) std::memcpy(weights, p.weights.data(), p.nlat * sizeof(double));
+    if (nlons) std::memcpy(nlons, p.nlons.data(), p.nlat * sizeof(int32_t));
+    if (mmax_truncation) std::memcpy(mmax_truncation, p.mt.data(), p.nh * sizeof(int32_t));
+    return SHT_OK;
+}
+
+int sht_legendre_synthesis(sht_plan* plan, const void* coeffs, int64_t ldc, int K, void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_legendre_synthesis")) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, "sht_legendre_synthesis")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(coeffs)) return fail(SHT_EINVAL, "sht_legendre_synthesis: NULL coeffs");
+    DeviceGuard g(plan->p.device);
+    return finish(legendre_synthesis(plan->p, (const float2*)coeffs, ldc, K, (cudaStream_t)stream),
+                  "sht_legendre_synthesis");
+}
+
+int sht_fourier_synthesis(sht_plan* plan, float* grid, int64_t ldg, int K, unsigned flags, void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_fourier_synthesis")) != SHT_OK) return rc;
+    if ((rc = check_ldg(plan->p, ldg, "sht_fourier_synthesis")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(grid)) return fail(SHT_EINVAL, "sht_fourier_synthesis: NULL grid");
+    DeviceGuard g(plan->p.device);
+    return finish(launch_fft_synthesis(plan->p, grid, ldg, K, flags, (cudaStream_t)stream), "sht_fourier_synthesis");
+}
+
+int sht_fourier_analysis(sht_plan* plan, const float* grid, int64_t ldg, int K, void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_fourier_analysis")) != SHT_OK) return rc;
+    if ((rc = check_ldg(plan->p, ldg, "sht_fourier_analysis")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(grid)) return fail(SHT_EINVAL, "sht_fourier_analysis: NULL grid");
+    DeviceGuard g(plan->p.device);
+    return finish(launch_fft_analysis(plan->p, grid, ldg, K, (cudaStream_t)stream), "sht_fourier_analysis");
+}
+
+int sht_legendre_analysis(sht_plan* plan, void* coeffs, int64_t ldc, int K, unsigned flags, void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_legendre_analysis")) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, "sht_legendre_analysis")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(coeffs)) return fail(SHT_EINVAL, "sht_legendre_analysis: NULL coeffs");
+    DeviceGuard g(plan->p.device);
+    return finish(legendre_analysis(plan->p, (float2*)coeffs, ldc, K, (flags & SHT_ADD) != 0, (cudaStream_t)stream),
+                  "sht_legendre_analysis");
+}
+
+int sht_synthesize(sht_plan* plan, const void* coeffs, int64_t ldc, float* grid, int64_t ldg, int K, unsigned flags,
+                   void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_synthesize")) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, "sht_synthesize")) != SHT_OK) return rc;
+    if ((rc = check_ldg(plan->p, ldg, "sht_synthesize")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(coeffs) || !ok_ptr(grid)) return fail(SHT_EINVAL, "sht_synthesize: NULL array");
+    DeviceGuard g(plan->p.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = legendre_synthesis(plan->p, (const float2*)coeffs, ldc, K, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sht_synthesize (Legendre)");
+    return finish(launch_fft_synthesis(plan->p, grid, ldg, K, flags, s), "sht_synthesize (Fourier)");
+}
+
+int sht_analyze(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, int64_t ldc, int K, unsigned flags,
+                void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_analyze")) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, "sht_analyze")) != SHT_OK) return rc;
+    if ((rc = check_ldg(plan->p, ldg, "sht_analyze")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(coeffs) || !ok_ptr(grid)) return fail(SHT_EINVAL, "sht_analyze: NULL array");
+    DeviceGuard g(plan->p.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = launch_fft_analysis(plan->p, grid, ldg, K, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sht_analyze (Fourier)");
+    return finish(legendre_analysis(plan->p, (float2*)coeffs, ldc, K, (flags & SHT_ADD) != 0, s),
+                  "sht_analyze (Legendre)");
+}
+
+static int ops_check(sht_plan* plan, int64_t ldc, int K, const char* what, std::initializer_list<const void*> ptrs) {
+    int rc;
+    if ((rc = check_call(plan, K, what)) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, what)) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    for (const void* q : ptrs)
+        if (!q) return fail(SHT_EINVAL, "%s: NULL array", what);
+    if (plan->p.nlm < 2) return fail(SHT_EINVAL, "%s: spectrum too small for operators", what);
+    return SHT_OK;
+}
+
+int sht_curl(sht_plan* plan, void* out, const void* u, const void* v, int64_t ldc, int K, unsigned flags,
+             double radius, void* stream) {
+    int rc = ops_check(plan, ldc, K, "sht_curl", {out, u, v});
+    if (rc != SHT_OK || K == 0) return rc;
+    DeviceGuard g(plan->p.device);
+    return finish(launch_divcurl(plan->p, (float2*)out, (const float2*)u, (const float2*)v, ldc, K, true,
+                                 flags & SHT_FLIPSIGN, flags & SHT_ADD, (float)(1.0 / radius), (cudaStream_t)stream),
+                  "sht_curl");
+}
+
+int sht_divergence(sht_plan* plan, void* out, const void* u, const void* v, int64_t ldc, int K, unsigned flags,
+                   double radius, void* stream) {
+    int rc = ops_check(plan, ldc, K, "sht_divergence", {out, u, v});
+    if (rc != SHT_OK || K == 0) return rc;
+    DeviceGuard g(plan->p.device);
+    return finish(launch_divcurl(plan->p, (float2*)out, (const float2*)u, (const float2*)v, ldc, K, false,
+                                 flags & SHT_FLIPSIGN, flags & SHT_ADD, (float)(1.0 / radius), (cudaStream_t)stream),
+                  "sht_divergence");
+}
+
+int sht_uv_from_vordiv(sht_plan* plan, void* U, void* V, const void* vor, const void* div, int64_t ldc, int K,
+                       double radius, void* stream) {
+    int rc = ops_check(plan, ldc, K, "sht_uv_from_vordiv", {U, V, vor});
+    if (rc != SHT_OK || K == 0) return rc;
+    DeviceGuard g(plan->p.device);
+    return finish(launch_uv_from_vordiv(plan->p, (float2*)U, (float2*)V, (const float2*)vor, (const float2*)div, ldc,
+                                        K, (float)radius, (cudaStream_t)stream),
+                  "sht_uv_from_vordiv");
+}
+
+int sht_laplace(sht_plan* plan, void* out, const void* alms, int64_t ldc, int K, unsigned flags, double radius,
+                void* stream) {
+    int rc = ops_check(plan, ldc, K, "sht_laplace", {out, alms});
+    if (rc != SHT_OK || K == 0) return rc;
+    DeviceGuard g(plan->p.device);
+    const bool inv = flags & SHT_INVERSE;
+    const double scale = radius == 1.0 ? 1.0 : (inv ? radius * radius : 1.0 / (radius * radius));
+    return finish(launch_laplace(plan->p, (float2*)out, (const float2*)alms, ldc, K, inv, flags & SHT_FLIPSIGN,
+                                 flags & SHT_ADD, (float)scale, (cudaStream_t)stream),
+                  "sht_laplace");
+}
+
+int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p_, int64_t ldc, int K, double radius,
+                 void* stream) {
+    int rc = ops_check(plan, ldc, K, "sht_gradient", {dpdx, dpdy, p_});
+    if (rc != SHT_OK || K == 0) return rc;
+    DeviceGuard g(plan->p.device);
+    return finish(launch_gradient(plan->p, (float2*)dpdx, (float2*)dpdy, (const float2*)p_, ldc, K,
+                                  (float)(1.0 / radius), (cudaStream_t)stream),
+                  "sht_gradient");
+}
+
+}  // extern "C"

@@ -1,0 +1,45 @@
+"""speedytransforms: SpeedyTransforms' spectral transform on B200 (sm_100a).
+
+Host-side mirror of the reference interface (SpeedyTransforms/src/spectral_transform.jl,
+SpeedyTransforms/src/spectral_gradients.jl) over the C ABI of libsht.so:
+
+* ``Spectrum``, ``FullGaussianGrid``, ``OctahedralGaussianGrid``,
+  ``LowerTriangularArray``, ``Field`` -- the reference's data layouts;
+* ``SpectralTransform(spectrum, grid; NF, nlayers, LegendreShortcut, precision)``;
+* ``transform_(out, in, S)`` is ``transform!`` (direction by argument types),
+  ``transform(in, S)`` allocates;
+* operators ``curl_``, ``divergence_``, ``UV_from_vor_``, ``UV_from_vordiv_``,
+  ``laplace_`` (``∇²!``), ``inverse_laplace_`` (``∇⁻²!``), ``gradient_`` (``∇!``)
+  and their allocating forms.
+
+Every compute call runs the CUDA kernels of libsht; there is no CPU path.
+"""
+from ._lib import DimensionMismatch, ShtError  # noqa: F401
+from .core import (  # noqa: F401
+    Field,
+    FullGaussianGrid,
+    LowerTriangularArray,
+    OctahedralGaussianGrid,
+    SpectralTransform,
+    Spectrum,
+    UV_from_vor,
+    UV_from_vor_,
+    UV_from_vordiv,
+    UV_from_vordiv_,
+    curl,
+    curl_,
+    divergence,
+    divergence_,
+    get_nlat_half,
+    get_truncation,
+    gradient,
+    gradient_,
+    inverse_laplace,
+    inverse_laplace_,
+    laplace,
+    laplace_,
+    transform,
+    transform_,
+)
+
+__version__ = "0.1.0"
