@@ -239,7 +239,7 @@ def time_stages(S, lt, field, out, reps):
         "fourier_analysis": lambda: L.sht_fourier_analysis(h, field.data.data_ptr(), npts, LAYERS, sp),
         "legendre_analysis": lambda: L.sht_legendre_analysis(h, out.data.data_ptr(), nlm, LAYERS, 0, sp),
     }
-    out = {}
+    res = {}
     for name, fn in stages.items():
         for _ in range(3):
             _lib.check(fn())
@@ -250,8 +250,8 @@ def time_stages(S, lt, field, out, reps):
             fn()
         e1.record(st)
         torch.cuda.synchronize()
-        out[name] = e0.elapsed_time(e1) / reps
-    return out
+        res[name] = e0.elapsed_time(e1) / reps
+    return res
 
 
 def run_ours(args):
@@ -271,7 +271,7 @@ def run_ours(args):
     spec = st.Spectrum(T, T)
     grid = st.OctahedralGaussianGrid(NLAT_HALF)
     c_np = O.random_coeffs(O.Spectrum(T, T), LAYERS, seed=2)
-    host_c = torch.tensor(c_np.T, dtype=torch.complex64).pin_memory()
+    host_c = torch.tensor(np.ascontiguousarray(c_np.T), dtype=torch.complex64).pin_memory()
     lt = st.LowerTriangularArray(host_c.to(device), spec)
     field = st.Field.zeros(grid, LAYERS, device=device)
     out = st.LowerTriangularArray.zeros(spec, LAYERS, device=device)

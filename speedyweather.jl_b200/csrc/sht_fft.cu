@@ -111,55 +111,81 @@ __device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y
 }
 
 // Stage of a large odd prime radix p: twiddle in place, then the symmetric direct DFT
-// with one work item per output pair (y_r, y_{p-r}).
+//   u_q = x_q + x_{p-q}, v_q = x_q - x_{p-q},  A_r = sum_q u_q cos(2 pi r q / p),
+//   B_r = sum_q v_q sin(2 pi r q / p),  y_r = x_0 + A_r -+ i B_r,  y_{p-r} = x_0 + A_r +- i B_r.
+// Work items are (column, group of GR outputs r) with the column index fastest, so the
+// lanes of a warp share r (the DFT-table reads broadcast) and read consecutive x.
+// Wp is a contiguous copy of exp(-2 pi i t / p), t < p.
+constexpr int GR = 8;
+
 template <bool INV>
-__device__ void stage_generic(float2* __restrict__ X, float2* __restrict__ Y, int n, int C, int Ns, int p,
-                              const float2* __restrict__ W) {
+__device__ void stage_generic(float2* __restrict__ X, float2* __restrict__ Y, float2* __restrict__ Wp, int n, int C,
+                              int Ns, int p, const float2* __restrict__ W) {
     const int nb = n / p;
     const int tstride = n / (Ns * p);
+    const int cols = C * nb;
+    for (int t = threadIdx.x; t < p; t += blockDim.x) Wp[t] = W[t * nb];
     for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
-        const int c = w / n;
-        const int i = w - c * n;
-        const int r = i / nb;
-        const int b = i - r * nb;
+        const int col = w % cols;
+        const int r = w / cols;
+        const int c = col / nb;
+        const int b = col - c * nb;
         const int k = b % Ns;
-        if (r > 0 && k > 0) X[(size_t)c * n + i] = twmul<INV>(X[(size_t)c * n + i], W[r * k * tstride]);
+        if (r > 0 && k > 0) {
+            float2* xp = X + (size_t)c * n + b + r * nb;
+            *xp = twmul<INV>(*xp, W[r * k * tstride]);
+        }
     }
     __syncthreads();
-    const int half = (p - 1) / 2;
-    const int items = C * nb * (half + 1);
-    for (int w = threadIdx.x; w < items; w += blockDim.x) {
-        const int r = w % (half + 1);
-        const int cb = w / (half + 1);
-        const int c = cb / nb;
-        const int b = cb - c * nb;
+    const int h = (p - 1) / 2;
+    const int ngroups = (h + GR) / GR;          // r in [0, h]
+    for (int w = threadIdx.x; w < cols * ngroups; w += blockDim.x) {
+        const int col = w % cols;
+        const int r0 = (w / cols) * GR;
+        const int c = col / nb;
+        const int b = col - c * nb;
         const int k = b % Ns;
         const float2* x = X + (size_t)c * n + b;
-        float2* yo = Y + (size_t)c * n + (b - k) * p + k;
         const float2 x0 = x[0];
-        if (r == 0) {
-            float2 s = x0;
-            for (int q = 1; q < p; ++q) s = cadd(s, x[q * nb]);
-            yo[0] = s;
-        } else {
-            float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
-            int idx = 0;
-            for (int q = 1; q <= half; ++q) {
-                idx += r;
-                if (idx >= p) idx -= p;
-                const float2 w_ = W[idx * nb];
-                const float cs = w_.x, sn = -w_.y;
-                const float2 a = x[q * nb], bq = x[(p - q) * nb];
-                A.x = fmaf(a.x + bq.x, cs, A.x); A.y = fmaf(a.y + bq.y, cs, A.y);
-                B.x = fmaf(a.x - bq.x, sn, B.x); B.y = fmaf(a.y - bq.y, sn, B.y);
+        float ar[GR], ai[GR], br[GR], bi[GR];
+        int idx[GR];
+#pragma unroll
+        for (int i = 0; i < GR; ++i) {
+            ar[i] = ai[i] = br[i] = bi[i] = 0.f;
+            idx[i] = 0;
+        }
+        for (int q = 1; q <= h; ++q) {
+            const float2 xq = x[q * nb], xm = x[(p - q) * nb];
+            const float ur = xq.x + xm.x, ui = xq.y + xm.y;
+            const float vr = xq.x - xm.x, vi = xq.y - xm.y;
+#pragma unroll
+            for (int i = 0; i < GR; ++i) {
+                idx[i] += r0 + i;
+                if (idx[i] >= p) idx[i] -= p;
+                const float2 wv = Wp[idx[i]];
+                const float cs = wv.x, sn = -wv.y;
+                ar[i] = fmaf(ur, cs, ar[i]);
+                ai[i] = fmaf(ui, cs, ai[i]);
+                br[i] = fmaf(vr, sn, br[i]);
+                bi[i] = fmaf(vi, sn, bi[i]);
+            }
+        }
+        float2* yo = Y + (size_t)c * n + (b - k) * p + k;
+#pragma unroll
+        for (int i = 0; i < GR; ++i) {
+            const int r = r0 + i;
+            if (r > h) break;
+            if (r == 0) {
+                yo[0] = make_float2(x0.x + ar[0], x0.y + ai[0]);
+                continue;
             }
             float2 yr, ypr;
             if (!INV) {
-                yr = make_float2(x0.x + A.x + B.y, x0.y + A.y - B.x);
-                ypr = make_float2(x0.x + A.x - B.y, x0.y + A.y + B.x);
+                yr = make_float2(x0.x + ar[i] + bi[i], x0.y + ai[i] - br[i]);
+                ypr = make_float2(x0.x + ar[i] - bi[i], x0.y + ai[i] + br[i]);
             } else {
-                yr = make_float2(x0.x + A.x - B.y, x0.y + A.y + B.x);
-                ypr = make_float2(x0.x + A.x + B.y, x0.y + A.y - B.x);
+                yr = make_float2(x0.x + ar[i] - bi[i], x0.y + ai[i] + br[i]);
+                ypr = make_float2(x0.x + ar[i] + bi[i], x0.y + ai[i] - br[i]);
             }
             yo[r * Ns] = yr;
             yo[(p - r) * Ns] = ypr;
@@ -169,7 +195,7 @@ __device__ void stage_generic(float2* __restrict__ X, float2* __restrict__ Y, in
 
 // Runs all stages; returns the buffer holding the result.
 template <bool INV>
-__device__ float2* run_fft(float2* X, float2* Y, int n, int C, const RingDesc& rd, const float2* W) {
+__device__ float2* run_fft(float2* X, float2* Y, float2* Wp, int n, int C, const RingDesc& rd, const float2* W) {
     int Ns = 1;
     for (int s = 0; s < rd.nfac; ++s) {
         const int p = rd.fac[s];
@@ -179,7 +205,7 @@ __device__ float2* run_fft(float2* X, float2* Y, int n, int C, const RingDesc& r
             case 4: stage_small<4, INV>(X, Y, n, C, Ns, W); break;
             case 5: stage_small<5, INV>(X, Y, n, C, Ns, W); break;
             case 7: stage_small<7, INV>(X, Y, n, C, Ns, W); break;
-            default: stage_generic<INV>(X, Y, n, C, Ns, p, W); break;
+            default: stage_generic<INV>(X, Y, Wp, n, C, Ns, p, W); break;
         }
         __syncthreads();
         float2* t = X; X = Y; Y = t;
@@ -189,9 +215,10 @@ __device__ float2* run_fft(float2* X, float2* Y, int n, int C, const RingDesc& r
 }
 
 __device__ __forceinline__ int smem_tw_len(int n) { return (n + 1) & ~1; }
+// shared memory: W (n twiddles) | Wp (n, per-stage DFT table) | X (C n) | Y (C n)
 
 // grid -> Fourier scratch (E/O combinations weighted by the solid angle)
-__global__ void __launch_bounds__(512) fft_analysis_kernel(const RingDesc* __restrict__ rings,
+__global__ void __launch_bounds__(1024) fft_analysis_kernel(const RingDesc* __restrict__ rings,
                                                            const float2* __restrict__ twiddle,
                                                            const float* __restrict__ grid, int64_t ldg,
                                                            float2* __restrict__ four, int K) {
@@ -202,7 +229,8 @@ __global__ void __launch_bounds__(512) fft_analysis_kernel(const RingDesc* __res
     const int C = min(rd.chunk, K - k0);
     const int n = rd.n;
     float2* W = sm;
-    float2* X = sm + smem_tw_len(n);
+    float2* Wp = sm + smem_tw_len(n);
+    float2* X = Wp + rd.wp_len;
     float2* Y = X + (size_t)C * n;
     for (int t = threadIdx.x; t < n; t += blockDim.x) W[t] = twiddle[rd.tw_off + t];
     for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
@@ -212,7 +240,7 @@ __global__ void __launch_bounds__(512) fft_analysis_kernel(const RingDesc* __res
         X[w] = make_float2(g[rd.off_north + i], g[rd.off_south + i]);
     }
     __syncthreads();
-    const float2* Z = run_fft<false>(X, Y, n, C, rd, W);
+    const float2* Z = run_fft<false>(X, Y, Wp, n, C, rd, W);
     const float half_domega = 0.5f * rd.domega;
     const int nm = rd.mt + 1;
     for (int w = threadIdx.x; w < C * nm; w += blockDim.x) {
@@ -232,7 +260,7 @@ __global__ void __launch_bounds__(512) fft_analysis_kernel(const RingDesc* __res
 }
 
 // Fourier scratch -> grid
-__global__ void __launch_bounds__(512) fft_synthesis_kernel(const RingDesc* __restrict__ rings,
+__global__ void __launch_bounds__(1024) fft_synthesis_kernel(const RingDesc* __restrict__ rings,
                                                             const float2* __restrict__ twiddle,
                                                             const float2* __restrict__ four, float* __restrict__ grid,
                                                             int64_t ldg, int K, int unscale, int add) {
@@ -243,7 +271,8 @@ __global__ void __launch_bounds__(512) fft_synthesis_kernel(const RingDesc* __re
     const int C = min(rd.chunk, K - k0);
     const int n = rd.n;
     float2* W = sm;
-    float2* X = sm + smem_tw_len(n);
+    float2* Wp = sm + smem_tw_len(n);
+    float2* X = Wp + rd.wp_len;
     float2* Y = X + (size_t)C * n;
     for (int t = threadIdx.x; t < n; t += blockDim.x) W[t] = twiddle[rd.tw_off + t];
     const float scale = unscale ? rd.coslat_inv : 1.0f;
@@ -268,7 +297,7 @@ __global__ void __launch_bounds__(512) fft_synthesis_kernel(const RingDesc* __re
         }
     }
     __syncthreads();
-    const float2* z = run_fft<true>(X, Y, n, C, rd, W);
+    const float2* z = run_fft<true>(X, Y, Wp, n, C, rd, W);
     for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
         const int c = w / n;
         const int i = w - c * n;
@@ -286,7 +315,7 @@ __global__ void __launch_bounds__(512) fft_synthesis_kernel(const RingDesc* __re
 
 }  // namespace
 
-static int fft_threads(const Plan&) { return 512; }
+static int fft_threads(const Plan&) { return 1024; }
 
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s) {
     dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);

@@ -20,6 +20,7 @@ struct RingDesc {
     int32_t mt;           // mmax_truncation (0-based highest order kept)
     int32_t nfac;         // number of Stockham stages
     int32_t chunk;        // layers per CTA in the FFT kernels
+    int32_t wp_len;       // shared-memory entries of the per-stage DFT table (even, >= largest radix)
     int64_t off_north;    // first grid point of the northern ring
     int64_t off_south;    // first grid point of the southern ring
     int64_t gofs;         // first Fourier-scratch row (m = 0) of this ring

@@ -265,7 +265,7 @@ int build_plan(Plan& p) {
     std::vector<RingDesc> rings(nh);
     std::vector<float2> tw;
     int64_t gofs = 0;
-    const int smem_budget = 200 * 1024;
+    const int smem_budget = 224 * 1024;
     int max_smem = 0;
     p.min_chunk = 1 << 30;
     for (int j = 0; j < nh; ++j) {
@@ -286,7 +286,12 @@ int build_plan(Plan& p) {
         }
         r.domega = (float)(p.weights[j] * (2.0 * M_PI / r.n));                  // quadrature_weights.jl:48-49
         r.coslat_inv = (float)(1.0 / std::cos(p.latd[j] * M_PI / 180.0));       // spectral_transform.jl:150-151
-        const int tw_bytes = ((r.n + 1) & ~1) * 8;
+        // shared memory of the FFT kernels: twiddles (n), the per-stage DFT table of the
+        // largest prime (<= n/4 + 1 for these grids) and two buffers of chunk x n complex
+        int pmax = 2;
+        for (int s = 0; s < r.nfac; ++s) pmax = std::max(pmax, (int)r.fac[s]);
+        r.wp_len = (pmax + 1) & ~1;
+        const int tw_bytes = (((r.n + 1) & ~1) + r.wp_len) * 8;
         int chunk = 1;
         while (chunk * 2 <= 32 && tw_bytes + 2 * (chunk * 2) * r.n * 8 <= smem_budget) chunk *= 2;
         r.chunk = chunk;
