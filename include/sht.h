@@ -55,6 +55,8 @@ extern "C" {
 #define SHT_PREC_BF16X3 1        /* tcgen05, split-BF16 hi/lo operands, 3 products, FP32 accumulate */
 #define SHT_PREC_FP16X3 2        /* tcgen05, split-FP16 hi/lo with power-of-2 per-(m, ring) and
                                     per-(m, column) scaling, 3 products, FP32 accumulate */
+#define SHT_PREC_BF16X5 3        /* tcgen05, Legendre polynomials in 3 bf16 pieces (from FP64), data
+                                    in 2, the 5 products above the split residual, FP32 accumulate */
 
 /* Legendre shortcuts (SpeedyTransforms/src/legendre_shortcuts.jl:21-49) */
 #define SHT_SHORTCUT_LINEAR 0
@@ -158,6 +160,12 @@ SHT_API int sht_laplace(sht_plan* plan, void* out, const void* alms, int64_t ldc
  * replaces SpeedyTransforms/src/spectral_gradients.jl:483-527. */
 SHT_API int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p, int64_t ldc, int K,
                  double radius, void* stream);
+
+/* Synchronises the device and returns (then clears) the plan's device status word:
+ * 0 = no kernel gave up waiting; otherwise the code of the first bounded wait in a
+ * tensor-core kernel that expired (1 s limit), whose outputs are then incomplete.
+ * No counterpart in the reference (its kernels have no waits). */
+SHT_API int sht_device_status(sht_plan* plan, int32_t* status);
 
 /* Message of the last failed call on this thread ("" if none). */
 SHT_API const char* sht_last_error(void);

@@ -18,6 +18,8 @@
 // laid out [row = gofs_j + m][eo][k] complex FP32 (k = layer, fastest).
 // FFTW's conventions are kept: r2c and c2r are unnormalised and c2r ignores the
 // imaginary parts of the DC and Nyquist bins.
+#include <cuda_bf16.h>
+
 #include "sht_internal.h"
 
 namespace sht {
@@ -221,7 +223,7 @@ __device__ __forceinline__ int smem_tw_len(int n) { return (n + 1) & ~1; }
 __global__ void __launch_bounds__(1024) fft_analysis_kernel(const RingDesc* __restrict__ rings,
                                                            const float2* __restrict__ twiddle,
                                                            const float* __restrict__ grid, int64_t ldg,
-                                                           float2* __restrict__ four, int K) {
+                                                           float2* __restrict__ four, int K, const TcImage img) {
     extern __shared__ float2 sm[];
     const RingDesc& rd = rings[blockIdx.x];
     const int k0 = blockIdx.y * rd.chunk;
@@ -243,6 +245,75 @@ __global__ void __launch_bounds__(1024) fft_analysis_kernel(const RingDesc* __re
     const float2* Z = run_fft<false>(X, Y, Wp, n, C, rd, W);
     const float half_domega = 0.5f * rd.domega;
     const int nm = rd.mt + 1;
+    if (img.base != nullptr) {
+        // tensor-core operand: E (parity 0) and O (parity 1) split into 16-bit pieces,
+        // written into the swizzled MN-major tile of (m, parity, ring block) at ring
+        // row j - j0(m); 8 real columns (4 layers) form one 16-byte chunk
+        const int cbeg = 2 * k0, cend = 2 * (k0 + C);
+        const int gbeg = cbeg / 8, ngr = (cend + 7) / 8 - gbeg;
+        const int j = blockIdx.x;
+        for (int w = threadIdx.x; w < ngr * nm; w += blockDim.x) {
+            const int g = gbeg + w % ngr;
+            const int m = w / ngr;
+            float ev[8], ov[8];
+            bool have[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int c = 8 * g + q;
+                have[q] = c >= cbeg && c < cend;
+                ev[q] = ov[q] = 0.f;
+                if (!have[q]) continue;
+                const int cl = c / 2 - k0;
+                const float2 a = Z[(size_t)cl * n + m];
+                const float2 b = Z[(size_t)cl * n + (m == 0 ? 0 : n - m)];
+                const float2 fn = make_float2(a.x + b.x, a.y - b.y);
+                const float2 fs = make_float2(a.y + b.y, b.x - a.x);
+                if (c % 2 == 0) {
+                    ev[q] = half_domega * (fn.x + fs.x);
+                    ov[q] = half_domega * (fn.x - fs.x);
+                } else {
+                    ev[q] = half_domega * (fn.y + fs.y);
+                    ov[q] = half_domega * (fn.y - fs.y);
+                }
+            }
+            const bool full = have[0] && have[7];
+            const int jj = j - img.j0[m];
+            const int r = jj % 64;
+            // column block of 64 (8 KB apart), 8-row group, row, swizzled 16-byte chunk
+            const int64_t row_off = (int64_t)(g / 8) * 8192 + (r / 8) * 1024 + (r % 8) * 128 + (((g % 8) ^ (r % 8)) * 16);
+            for (int par = 0; par < 2; ++par) {
+                const float* v = par ? ov : ev;
+                const int64_t tile = img.tile_base[m] + (int64_t)par * img.njt[m] + jj / 64;
+                uint16_t pc[3][8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    float x = v[q];
+#pragma unroll
+                    for (int pp = 0; pp < 3; ++pp) {
+                        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+                        pc[pp][q] = __bfloat16_as_ushort(h);
+                        x -= __bfloat162float(h);
+                    }
+                }
+                for (int pp = 0; pp < img.npieces; ++pp) {
+                    uint8_t* dst = reinterpret_cast<uint8_t*>(img.base) + (tile * img.npieces + pp) * img.tile_bytes + row_off;
+                    if (full) {
+                        uint4 u;
+                        u.x = (uint32_t)pc[pp][0] | ((uint32_t)pc[pp][1] << 16);
+                        u.y = (uint32_t)pc[pp][2] | ((uint32_t)pc[pp][3] << 16);
+                        u.z = (uint32_t)pc[pp][4] | ((uint32_t)pc[pp][5] << 16);
+                        u.w = (uint32_t)pc[pp][6] | ((uint32_t)pc[pp][7] << 16);
+                        *reinterpret_cast<uint4*>(dst) = u;
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 8; ++q)
+                            if (have[q]) reinterpret_cast<uint16_t*>(dst)[q] = pc[pp][q];
+                    }
+                }
+            }
+        }
+        return;
+    }
     for (int w = threadIdx.x; w < C * nm; w += blockDim.x) {
         const int c = w % C;
         const int m = w / C;
@@ -317,9 +388,11 @@ __global__ void __launch_bounds__(1024) fft_synthesis_kernel(const RingDesc* __r
 
 static int fft_threads(const Plan&) { return 1024; }
 
-cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s) {
+cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, bool to_image) {
     dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);
-    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_rings, p.d_twiddle, grid, ldg, p.d_four, K);
+    const TcImage none{};
+    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_rings, p.d_twiddle, grid, ldg, p.d_four, K,
+                                                              (to_image || p.tc) ? p.ana_img : none);
     return cudaGetLastError();
 }
 

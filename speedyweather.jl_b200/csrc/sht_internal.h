@@ -36,6 +36,21 @@ struct LegItem {
     int32_t tile;         // ring tile (synthesis) or parity-row tile (analysis)
 };
 
+// Layout of the analysis data operand the FFT writes for the tensor-core Legendre
+// stage: pre-swizzled (SWIZZLE_128B, MN-major) 16-bit tiles of 64 rings x N columns,
+// one tile per (order m, parity, ring block, piece).
+struct TcImage {
+    uint16_t* base = nullptr;           // 16-bit words (bf16 or fp16 bits)
+    const int64_t* tile_base = nullptr; // per m: tile index of (m, parity 0, ring block 0)
+    const int32_t* njt = nullptr;       // per m: ring blocks of 64 rings
+    const int32_t* j0 = nullptr;        // per m: first ring
+    int32_t npieces = 0;
+    int32_t tile_bytes = 0;             // bytes of one tile
+    int32_t fp16 = 0;                   // 0: bf16 pieces, 1: fp16 pieces
+    const float* col_scale = nullptr;   // fp16: per layer scale of the data (device)
+    const float* ring_scale = nullptr;  // fp16: per (m, ring) 1 / scale of the Legendre table
+};
+
 struct Plan {
     sht_desc d{};
     int nh = 0, nlat = 0, lmax = 0, mmax = 0, nlon_max = 0, nfreq_max = 0;
@@ -78,6 +93,9 @@ struct Plan {
     int64_t four_elems = 0;
 
     int64_t table_bytes = 0;
+    int32_t* d_err = nullptr;           // device status word of the bounded waits (0 = ok)
+    void* tc = nullptr;                 // tensor-core Legendre state (sht_legendre_tc.cu)
+    TcImage ana_img;                    // analysis data image written by the FFT (tensor-core plans)
     int smem_fft = 0;                   // dynamic shared memory of the FFT kernels
     int max_chunk_groups = 0;           // grid.y upper bound factor for FFT launch
     int min_chunk = 1;
@@ -89,7 +107,8 @@ enum GradIdx {
 };
 
 // ---- launchers (return cudaError_t of the launch) ----------------------------------
-cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s);
+cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s,
+                                bool to_image = false);
 cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags,
                                  cudaStream_t s);
 cudaError_t launch_legendre_synthesis_fp32(const Plan& p, const float2* coeffs, int64_t ldc, int K,

@@ -1,16 +1,705 @@
-// Tensor-core (tcgen05) Legendre stage: placeholder until the split-precision
-// kernels land; plans asking for SHT_PREC_BF16X3 / SHT_PREC_FP16X3 fail with
-// SHT_EUNSUPPORTED.
+// Legendre stage on the 5th-generation tensor cores (tcgen05) in split precision.
+//
+// Replaces SpeedyTransforms/src/legendre_ka.jl:19-200 (and the CPU loops of
+// SpeedyTransforms/src/legendre.jl:2-195) for plans with SHT_PREC_BF16X3 / SHT_PREC_BF16X5.
+//
+// Per order m and parity p of l - m the stage is one GEMM (see sht_legendre_simt.cu):
+//   synthesis  D[j, c] = sum_i Lam[m][p][i][j] B[i, c]     (M = rings, K = parity rows)
+//   analysis   D[i, c] = sum_j Lam[m][p][i][j] B[j, c]     (M = parity rows, K = rings)
+// FP32 operands are split into 16-bit pieces x = x_0 + x_1 (+ x_2) and the product
+// is the sum of the cross products whose magnitude is above the split's residual,
+// accumulated in FP32 in tensor memory:
+//   SHT_PREC_BF16X3: Lam in 2 bf16 pieces, data in 2: L0 B0 + L0 B1 + L1 B0
+//   SHT_PREC_BF16X5: Lam in 3 bf16 pieces (from FP64), data in 2:
+//                    L0 B0 + L0 B1 + L1 B0 + L1 B1 + L2 B0
+//
+// Operands in shared memory use the SWIZZLE_128B canonical layouts of tcgen05:
+// * Lam[m][p] is stored [piece][i][j - j0(m)] in global memory; one TMA tensor map
+//   per (m, p) loads 64 x 64 boxes (rows i, 128 B of j). The same box is the
+//   MN-major A block of the synthesis (M = j) and the K-major A block of the
+//   analysis (K = j). Out-of-range parts of a box are zero-filled by the TMA without
+//   memory traffic.
+// * The data operands are written by their producers (a pre-pass over the
+//   coefficients for the synthesis, the FFT kernel for the analysis) directly as
+//   swizzled shared-memory images in global memory and loaded with 1-D bulk copies.
+//
+// One CTA computes one 128 x N output tile (N <= 256 real columns): warp 0 issues
+// the copies, warp 1 owns the tensor memory and one of its threads issues the
+// MMAs, warps 2-5 read the accumulator (tcgen05.ld) and store. Every wait is
+// bounded by a one-second global-timer limit; on expiry the CTA records an error
+// in the plan's status word, drains, frees its tensor memory and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
 #include "sht_internal.h"
 
 namespace sht {
-int tc_supported() { return 0; }
-cudaError_t tc_prepare(Plan&) { return cudaErrorNotSupported; }
-void tc_release(Plan&) {}
-cudaError_t launch_legendre_synthesis_tc(const Plan&, const float2*, int64_t, int, cudaStream_t) {
-    return cudaErrorNotSupported;
+
+namespace {
+
+constexpr int TC_THREADS = 192;
+constexpr int BLK = 64;                     // Legendre box edge (rows x rings)
+constexpr int BOX_BYTES = BLK * BLK * 2;    // 8 KB
+constexpr int A_PIECE_BYTES = 2 * BOX_BYTES;
+constexpr uint64_t WAIT_NS = 1000000000ull;  // bounded waits: 1 s
+
+struct TcItem {
+    int32_t m, par, tile, pad;
+};
+
+// Everything the kernels need, passed by value.
+struct TcDev {
+    const CUtensorMap* maps;       // per (m, par)
+    const int32_t* nr;             // per m: rings [j0, nh)
+    const int32_t* j0;             // per m
+    const int32_t* rows;           // per m: parity rows
+    const int64_t* lm_off;         // per m
+    const int64_t* syn_tile_base;  // per m: image tile index of (m, par 0, kt 0)
+    const int64_t* ana_tile_base;  // per m
+    const int32_t* nkt;            // per m: ceil(rows / 64)
+    const int32_t* njt;            // per m: ceil(nr / 64)
+    const RingDesc* rings;
+    const uint16_t* syn_img;
+    const uint16_t* ana_img;
+    int32_t* err;
+    int nh, lmax, mmax;
+    int npa, npb, nprod;
+    uint32_t prod;                 // product i: A piece (prod >> 4i) & 3, B piece (prod >> (4i + 2)) & 3
+    int64_t syn_tile_bytes;        // one (m, p, kt, piece) synthesis data tile at nmax columns
+    int64_t ana_tile_bytes;        // one (m, p, jt, piece) analysis data tile
+    int nmax;                      // columns of the data images (multiple of 64)
+};
+
+struct TcState {
+    int npa = 2, npb = 2, nprod = 3;
+    uint32_t prod = 0;
+    int nmax = 0;
+    CUtensorMap* d_maps = nullptr;
+    uint16_t* d_lam = nullptr;
+    int32_t *d_nr = nullptr, *d_nkt = nullptr, *d_njt = nullptr;
+    int64_t *d_syn_base = nullptr, *d_ana_base = nullptr;
+    uint16_t* d_syn_img = nullptr;
+    uint16_t* d_ana_img = nullptr;
+    int64_t syn_tile_bytes = 0, ana_tile_bytes = 0;
+    TcItem* d_syn_items = nullptr;
+    int n_syn_items = 0;
+    TcItem* d_ana_items = nullptr;
+    int n_ana_items = 0;
+    int max_smem = 0;
+};
+
+// ---------------------------------------------------------------- PTX wrappers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-cudaError_t launch_legendre_analysis_tc(const Plan&, float2*, int64_t, int, bool, cudaStream_t) {
-    return cudaErrorNotSupported;
+__device__ __forceinline__ uint64_t gtime() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase with the given parity; false after WAIT_NS.
+__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = gtime();
+    while (!mbar_try_wait(bar, parity))
+        if (gtime() - t0 > WAIT_NS) return false;
+    return true;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// SWIZZLE_128B shared-memory matrix descriptor (Blackwell version bit set).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+// kind::f16 instruction descriptor: FP32 accumulate, A/B bf16 (fmt 1) or f16 (fmt 0), M = 128.
+__device__ __forceinline__ uint32_t idesc_f16(uint32_t fmt, uint32_t a_mn, uint32_t b_mn, uint32_t n) {
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (a_mn << 15) | (b_mn << 16) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------- the GEMM kernel
+// SYN: A = Lam^T (MN-major), B = synthesis image (K-major), D -> Fourier scratch.
+// ANA: A = Lam (K-major), B = analysis image (MN-major), D -> coefficients.
+template <bool SYN>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    legendre_tc_kernel(const TcDev t, const TcItem* __restrict__ items, int K, int nt_cols, int stages,
+                       uint32_t tmem_cols, float2* __restrict__ four, float2* __restrict__ coeffs, int64_t ldc,
+                       int add) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const TcItem it = items[blockIdx.x];
+    const int m = it.m, par = it.par, tile = it.tile;
+    const int ct = blockIdx.y;                       // column tile (256 columns)
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int nsteps = SYN ? t.nkt[m] : t.njt[m];
+    const int a_bytes = t.npa * A_PIECE_BYTES;
+    const int b_piece_bytes = nt_cols * 128;
+    const int stage_bytes = a_bytes + t.npb * b_piece_bytes;
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + (size_t)stages * stage_bytes);
+    uint64_t* empty_bar = full_bar + stages;
+    uint64_t* acc_bar = empty_bar + stages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_bar + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int rows_m = t.rows[m];
+    const int j0 = t.j0[m];
+    const int64_t lmo = t.lm_off[m];
+
+    if (nsteps == 0) {          // analysis of an order no ring carries: coefficients are zero
+        if (!SYN && !add && warp >= 2) {
+            const int r = (warp % 4) * 32 + lane;
+            const int i = tile * 128 + r;
+            if (i < rows_m && m + 2 * i + par < t.lmax)
+                for (int c = 0; c < nt_cols && ct * 256 + c < 2 * K; c += 2)
+                    coeffs[(int64_t)((ct * 256 + c) / 2) * ldc + lmo + 2 * i + par] = make_float2(0.f, 0.f);
+        }
+        return;
+    }
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        mbar_init(acc_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const CUtensorMap* map = t.maps + (2 * m + par);
+    if (warp == 0 && lane == 0) {
+        // ------------------------------------------------ producer
+        const int64_t tb = SYN ? t.syn_tile_base[m] + (int64_t)par * t.nkt[m] : t.ana_tile_base[m] + (int64_t)par * t.njt[m];
+        const int64_t img_tile_bytes = SYN ? t.syn_tile_bytes : t.ana_tile_bytes;
+        const uint8_t* img = reinterpret_cast<const uint8_t*>(SYN ? t.syn_img : t.ana_img);
+        const int64_t col_off = SYN ? (int64_t)ct * 256 * 128 : (int64_t)ct * 4 * BOX_BYTES;
+        for (int ks = 0; ks < nsteps; ++ks) {
+            const int s = ks % stages;
+            if (ks >= stages && !mbar_wait(&empty_bar[s], ((ks / stages) - 1) & 1)) {
+                *abort_flag = 1;
+                atomicExch(t.err, 1);
+                break;
+            }
+            if (*abort_flag) break;
+            uint8_t* st = smem + (size_t)s * stage_bytes;
+            mbar_expect_tx(&full_bar[s], (uint32_t)stage_bytes);
+            for (int pa = 0; pa < t.npa; ++pa) {
+                uint8_t* a = st + pa * A_PIECE_BYTES;
+                if (SYN) {   // rings [128 tile, +128) of rows [64 ks, +64)
+                    tma_load_3d(a, map, tile * 128, ks * BLK, pa, &full_bar[s]);
+                    tma_load_3d(a + BOX_BYTES, map, tile * 128 + BLK, ks * BLK, pa, &full_bar[s]);
+                } else {     // rows [128 tile, +128) of rings [64 ks, +64)
+                    tma_load_3d(a, map, ks * BLK, tile * 128, pa, &full_bar[s]);
+                    tma_load_3d(a + BOX_BYTES, map, ks * BLK, tile * 128 + BLK, pa, &full_bar[s]);
+                }
+            }
+            for (int pb = 0; pb < t.npb; ++pb) {
+                const uint8_t* src = img + ((tb + ks) * t.npb + pb) * img_tile_bytes + col_off;
+                bulk_load(st + a_bytes + pb * b_piece_bytes, src, (uint32_t)b_piece_bytes, &full_bar[s]);
+            }
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------------------------ MMA issuer
+        const uint32_t idesc = idesc_f16(1u, SYN ? 1u : 0u, SYN ? 0u : 1u, (uint32_t)nt_cols);
+        bool ok = true;
+        for (int ks = 0; ks < nsteps && ok; ++ks) {
+            const int s = ks % stages;
+            if (!mbar_wait(&full_bar[s], (ks / stages) & 1)) {
+                *abort_flag = 1;
+                atomicExch(t.err, 2);
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t st = smem_u32(smem + (size_t)s * stage_bytes);
+            for (int kk = 0; kk < BLK / 16; ++kk) {
+                for (int q = 0; q < t.nprod; ++q) {
+                    const int pa = (t.prod >> (4 * q)) & 3, pb = (t.prod >> (4 * q + 2)) & 3;
+                    const uint32_t a = st + pa * A_PIECE_BYTES;
+                    const uint32_t b = st + a_bytes + pb * b_piece_bytes;
+                    uint64_t da, db;
+                    if (SYN) {
+                        da = sdesc(a + kk * 2048, BOX_BYTES, 1024);     // MN-major: 16 rows per step
+                        db = sdesc(b + kk * 32, 16, 1024);              // K-major: 32 B per step
+                    } else {
+                        da = sdesc(a + kk * 32, 16, 1024);
+                        db = sdesc(b + kk * 2048, BOX_BYTES, 1024);
+                    }
+                    umma_f16(tmem, da, db, idesc, (ks | kk | q) ? 1u : 0u);
+                }
+            }
+            umma_commit(&empty_bar[s]);      // frees the stage once these MMAs complete
+        }
+        umma_commit(acc_bar);                // accumulator ready (or drained after an abort)
+    } else if (warp >= 2) {
+        // ------------------------------------------------ epilogue
+        const bool ok = mbar_wait(acc_bar, 0);
+        if (!ok) {
+            *abort_flag = 1;
+            atomicExch(t.err, 3);
+        }
+        tc_fence_after();
+        const int quarter = warp % 4;
+        const int r = quarter * 32 + lane;
+        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
+        const bool good = ok && !*abort_flag;
+        if (SYN) {
+            const int j = j0 + tile * 128 + r;
+            const bool valid = good && j < t.nh && m <= t.rings[j].mt;
+            float2* dst = valid ? four + ((t.rings[j].gofs + m) * 2 + par) * K : nullptr;
+            for (int c0 = 0; c0 < nt_cols; c0 += 32) {
+                float v[32];
+                tmem_ld32(taddr + c0, v);
+                if (!valid) continue;
+#pragma unroll
+                for (int q = 0; q < 16; q += 2) {
+                    const int k = (ct * 256 + c0) / 2 + q;
+                    if (k + 1 < K && (K % 2) == 0) {    // 16-byte aligned: row * K and k even
+                        *reinterpret_cast<float4*>(dst + k) = make_float4(v[2 * q], v[2 * q + 1], v[2 * q + 2], v[2 * q + 3]);
+                    } else {
+                        if (k < K) dst[k] = make_float2(v[2 * q], v[2 * q + 1]);
+                        if (k + 1 < K) dst[k + 1] = make_float2(v[2 * q + 2], v[2 * q + 3]);
+                    }
+                }
+            }
+        } else {
+            const int i = tile * 128 + r;
+            const bool valid = good && i < rows_m && m + 2 * i + par < t.lmax;
+            for (int c0 = 0; c0 < nt_cols; c0 += 32) {
+                float v[32];
+                tmem_ld32(taddr + c0, v);
+                if (!valid) continue;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int k = (ct * 256 + c0) / 2 + q;
+                    if (k >= K) break;
+                    float2* d = coeffs + (int64_t)k * ldc + lmo + 2 * i + par;
+                    float2 val = make_float2(v[2 * q], v[2 * q + 1]);
+                    if (add) {
+                        const float2 o = *d;
+                        val.x += o.x;
+                        val.y += o.y;
+                    }
+                    *d = val;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------- synthesis data image
+// coefficients [k][lm] complex FP32 -> per (m, p, kt, piece) K-major SWIZZLE_128B tiles
+// of nmax rows (columns c = 2k + re/im) x 64 parity rows (128 B).
+__device__ __forceinline__ void split_bf16(float x, uint16_t* out, int npieces) {
+    float r = x;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        if (q >= npieces) break;
+        const __nv_bfloat16 h = __float2bfloat16_rn(r);
+        out[q] = __bfloat16_as_ushort(h);
+        r -= __bfloat162float(h);
+    }
+}
+
+__global__ void syn_image_kernel(const TcDev t, const float2* __restrict__ coeffs, int64_t ldc, int K) {
+    const int m = blockIdx.x;
+    const int kt = blockIdx.y;
+    if (kt >= t.nkt[m]) return;
+    const int rows_m = t.rows[m];
+    const int64_t lmo = t.lm_off[m];
+    uint8_t* img = reinterpret_cast<uint8_t*>(const_cast<uint16_t*>(t.syn_img));
+    for (int w = threadIdx.x; w < K * 8; w += blockDim.x) {
+        const int ib8 = w % 8;
+        const int k = w / 8;
+        // 8 parity rows [64 kt + 8 ib8, +8) of both parities = 16 consecutive lm
+        float re[2][8], im[2][8];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int par = q & 1, ii = q >> 1;
+            const int i = kt * BLK + ib8 * 8 + ii;
+            const int l = m + 2 * i + par;
+            float2 v = make_float2(0.f, 0.f);
+            if (i < rows_m && l < t.lmax) v = coeffs[(int64_t)k * ldc + lmo + 2 * i + par];
+            re[par][ii] = v.x;
+            im[par][ii] = v.y;
+        }
+#pragma unroll
+        for (int par = 0; par < 2; ++par) {
+            const int64_t tile = t.syn_tile_base[m] + (int64_t)par * t.nkt[m] + kt;
+#pragma unroll
+            for (int ri = 0; ri < 2; ++ri) {
+                const int c = 2 * k + ri;
+                const float* src = ri ? im[par] : re[par];
+                uint16_t pc[3][8];
+#pragma unroll
+                for (int ii = 0; ii < 8; ++ii) {
+                    uint16_t tmp[3];
+                    split_bf16(src[ii], tmp, t.npb);
+                    for (int q = 0; q < t.npb; ++q) pc[q][ii] = tmp[q];
+                }
+                const int64_t off = (int64_t)(c / 8) * 1024 + (c % 8) * 128 + ((ib8 ^ (c % 8)) * 16);
+                for (int q = 0; q < t.npb; ++q) {
+                    uint8_t* dst = img + (tile * t.npb + q) * t.syn_tile_bytes + off;
+                    uint4 u;
+                    u.x = (uint32_t)pc[q][0] | ((uint32_t)pc[q][1] << 16);
+                    u.y = (uint32_t)pc[q][2] | ((uint32_t)pc[q][3] << 16);
+                    u.z = (uint32_t)pc[q][4] | ((uint32_t)pc[q][5] << 16);
+                    u.w = (uint32_t)pc[q][6] | ((uint32_t)pc[q][7] << 16);
+                    *reinterpret_cast<uint4*>(dst) = u;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- host side
+PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+TcDev make_dev(const Plan& p) {
+    const TcState& s = *static_cast<const TcState*>(p.tc);
+    TcDev t{};
+    t.maps = s.d_maps;
+    t.nr = s.d_nr;
+    t.j0 = p.d_j0;
+    t.rows = p.d_rows;
+    t.lm_off = p.d_lm_off;
+    t.syn_tile_base = s.d_syn_base;
+    t.ana_tile_base = s.d_ana_base;
+    t.nkt = s.d_nkt;
+    t.njt = s.d_njt;
+    t.rings = p.d_rings;
+    t.syn_img = s.d_syn_img;
+    t.ana_img = s.d_ana_img;
+    t.err = p.d_err;
+    t.nh = p.nh;
+    t.lmax = p.lmax;
+    t.mmax = p.mmax;
+    t.npa = s.npa;
+    t.npb = s.npb;
+    t.nprod = s.nprod;
+    t.prod = s.prod;
+    t.syn_tile_bytes = s.syn_tile_bytes;
+    t.ana_tile_bytes = s.ana_tile_bytes;
+    t.nmax = s.nmax;
+    return t;
+}
+
+int smem_for(int npa, int npb, int nt_cols, int& stages) {
+    const int stage_bytes = npa * A_PIECE_BYTES + npb * nt_cols * 128;
+    const int budget = 227 * 1024 - 1024 - 256;      // alignment slack + barriers
+    stages = std::min(4, budget / stage_bytes);
+    return 1024 + stages * stage_bytes + 256;
+}
+
+}  // namespace
+
+int tc_supported() { return get_encoder() != nullptr; }
+
+cudaError_t tc_prepare(Plan& p) {
+    TcState* s = new TcState();
+    p.tc = s;
+    if (p.d.precision == SHT_PREC_BF16X3) {
+        s->npa = 2; s->npb = 2; s->nprod = 3;
+        s->prod = (0u | (0u << 2)) | ((0u | (1u << 2)) << 4) | ((1u | (0u << 2)) << 8);
+    } else if (p.d.precision == SHT_PREC_BF16X5) {
+        s->npa = 3; s->npb = 2; s->nprod = 5;
+        s->prod = (0u | (0u << 2)) | ((0u | (1u << 2)) << 4) | ((1u | (0u << 2)) << 8) | ((1u | (1u << 2)) << 12) |
+                  ((2u | (0u << 2)) << 16);
+    } else {
+        return cudaErrorNotSupported;
+    }
+    const int nh = p.nh, mmax = p.mmax;
+    // image columns: whole 256-column tiles once a call can need more than one
+    s->nmax = 2 * p.d.nlayers <= 256 ? (2 * p.d.nlayers + 63) / 64 * 64 : (2 * p.d.nlayers + 255) / 256 * 256;
+
+    // --- Legendre pieces [m][p][piece][i][j - j0] with row pitch rounded to 8 rings ---
+    std::vector<int32_t> nr(mmax), pitch(mmax), nkt(mmax), njt(mmax);
+    std::vector<int64_t> blk_off(2 * mmax);
+    int64_t total = 0;
+    for (int m = 0; m < mmax; ++m) {
+        nr[m] = nh - p.j0[m];
+        pitch[m] = std::max(8, (nr[m] + 7) / 8 * 8);
+        nkt[m] = (p.rows[m] + BLK - 1) / BLK;
+        njt[m] = (nr[m] + BLK - 1) / BLK;
+        for (int par = 0; par < 2; ++par) {
+            blk_off[2 * m + par] = total;
+            total += (int64_t)s->npa * p.rows[m] * pitch[m];
+        }
+    }
+    std::vector<uint16_t> lam((size_t)total, 0);
+    {
+        const int nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        auto work = [&](int tid) {
+            std::vector<double> col(p.lmax);
+            for (int j = tid; j < nh; j += nthreads) {
+                const double colat = M_PI / 2 - p.latd[j] * M_PI / 180.0;
+                const double xc = std::cos(colat);
+                const double sn = std::sqrt(std::max(0.0, 1.0 - xc * xc));
+                double pmm = 1.0 / std::sqrt(4.0 * M_PI);
+                for (int m = 0; m <= p.mt[j]; ++m) {
+                    if (m > 0) pmm = -std::sqrt((2.0 * m + 1.0) / (2.0 * m)) * sn * pmm;
+                    const int L = p.lmax - m;
+                    col[0] = pmm;
+                    if (L >= 2) {
+                        double p0 = pmm, p1 = std::sqrt(2.0 * m + 3.0) * xc * pmm;
+                        col[1] = p1;
+                        double a_prev = std::sqrt((4.0 * (m + 1) * (m + 1) - 1.0) / ((m + 1.0) * (m + 1.0) - 1.0 * m * m));
+                        for (int l = m + 2; l < p.lmax; ++l) {
+                            const double a = std::sqrt((4.0 * l * l - 1.0) / (1.0 * l * l - 1.0 * m * m));
+                            const double p2 = a * (xc * p1 - p0 / a_prev);
+                            col[l - m] = p2;
+                            p0 = p1;
+                            p1 = p2;
+                            a_prev = a;
+                        }
+                    }
+                    const int jj = j - p.j0[m];
+                    for (int i = 0; i < L; ++i) {
+                        const int par = i & 1, row = i >> 1;
+                        double r = col[i];
+                        for (int q = 0; q < s->npa; ++q) {
+                            const __nv_bfloat16 h = __float2bfloat16_rn((float)r);
+                            lam[blk_off[2 * m + par] + ((int64_t)q * p.rows[m] + row) * pitch[m] + jj] =
+                                __bfloat16_as_ushort(h);
+                            r -= (double)__bfloat162float(h);
+                        }
+                    }
+                }
+            }
+        };
+        std::vector<std::thread> th;
+        for (int t = 0; t < nthreads; ++t) th.emplace_back(work, t);
+        for (auto& t : th) t.join();
+    }
+    cudaError_t e;
+    if ((e = cudaMalloc(&s->d_lam, std::max<int64_t>(16, total) * 2)) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(s->d_lam, lam.data(), total * 2, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    p.table_bytes += total * 2;
+
+    // --- tensor maps, one per (m, p): dims {rings, parity rows, pieces}, box 64 x 64 x 1 ---
+    auto enc = get_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    std::vector<CUtensorMap> maps(2 * mmax);
+    std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+    for (int m = 0; m < mmax; ++m)
+        for (int par = 0; par < 2; ++par) {
+            if (nr[m] == 0) continue;
+            cuuint64_t dims[3] = {(cuuint64_t)nr[m], (cuuint64_t)p.rows[m], (cuuint64_t)s->npa};
+            cuuint64_t strides[2] = {(cuuint64_t)pitch[m] * 2, (cuuint64_t)pitch[m] * 2 * p.rows[m]};
+            cuuint32_t box[3] = {BLK, BLK, 1};
+            cuuint32_t estr[3] = {1, 1, 1};
+            CUresult r = enc(&maps[2 * m + par], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
+                             s->d_lam + blk_off[2 * m + par], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+        }
+    if ((e = cudaMalloc(&s->d_maps, maps.size() * sizeof(CUtensorMap))) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(s->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+        return e;
+
+    // --- data images ---
+    s->syn_tile_bytes = (int64_t)s->nmax * 128;
+    s->ana_tile_bytes = (int64_t)(s->nmax / 64) * BOX_BYTES;
+    std::vector<int64_t> syn_base(mmax), ana_base(mmax);
+    int64_t ns = 0, na = 0;
+    for (int m = 0; m < mmax; ++m) {
+        syn_base[m] = ns;
+        ns += 2LL * nkt[m];
+        ana_base[m] = na;
+        na += 2LL * njt[m];
+    }
+    if ((e = cudaMalloc(&s->d_syn_img, std::max<int64_t>(1, ns) * s->npb * s->syn_tile_bytes)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&s->d_ana_img, std::max<int64_t>(1, na) * s->npb * s->ana_tile_bytes)) != cudaSuccess) return e;
+    if ((e = cudaMemset(s->d_syn_img, 0, std::max<int64_t>(1, ns) * s->npb * s->syn_tile_bytes)) != cudaSuccess) return e;
+    if ((e = cudaMemset(s->d_ana_img, 0, std::max<int64_t>(1, na) * s->npb * s->ana_tile_bytes)) != cudaSuccess) return e;
+
+    auto up32 = [&](int32_t** d, const std::vector<int32_t>& v) {
+        cudaError_t ee = cudaMalloc(d, v.size() * 4);
+        return ee != cudaSuccess ? ee : cudaMemcpy(*d, v.data(), v.size() * 4, cudaMemcpyHostToDevice);
+    };
+    auto up64 = [&](int64_t** d, const std::vector<int64_t>& v) {
+        cudaError_t ee = cudaMalloc(d, v.size() * 8);
+        return ee != cudaSuccess ? ee : cudaMemcpy(*d, v.data(), v.size() * 8, cudaMemcpyHostToDevice);
+    };
+    if ((e = up32(&s->d_nr, nr)) != cudaSuccess) return e;
+    if ((e = up32(&s->d_nkt, nkt)) != cudaSuccess) return e;
+    if ((e = up32(&s->d_njt, njt)) != cudaSuccess) return e;
+    if ((e = up64(&s->d_syn_base, syn_base)) != cudaSuccess) return e;
+    if ((e = up64(&s->d_ana_base, ana_base)) != cudaSuccess) return e;
+
+    // --- work items (heavy orders first) ---
+    std::vector<TcItem> syn, ana;
+    for (int m = 0; m < mmax; ++m)
+        for (int par = 0; par < 2; ++par) {
+            for (int tl = 0; tl * 128 < nr[m]; ++tl) syn.push_back({m, par, tl, 0});
+            for (int tl = 0; tl * 128 < p.rows[m]; ++tl) ana.push_back({m, par, tl, 0});
+        }
+    auto upi = [&](TcItem** d, const std::vector<TcItem>& v) {
+        cudaError_t ee = cudaMalloc(d, std::max<size_t>(1, v.size()) * sizeof(TcItem));
+        return ee != cudaSuccess ? ee : cudaMemcpy(*d, v.data(), v.size() * sizeof(TcItem), cudaMemcpyHostToDevice);
+    };
+    if ((e = upi(&s->d_syn_items, syn)) != cudaSuccess) return e;
+    if ((e = upi(&s->d_ana_items, ana)) != cudaSuccess) return e;
+    s->n_syn_items = (int)syn.size();
+    s->n_ana_items = (int)ana.size();
+
+    // --- the image the FFT analysis kernel writes ---
+    p.ana_img.base = s->d_ana_img;
+    p.ana_img.tile_base = s->d_ana_base;
+    p.ana_img.njt = s->d_njt;
+    p.ana_img.j0 = p.d_j0;
+    p.ana_img.npieces = s->npb;
+    p.ana_img.tile_bytes = (int32_t)s->ana_tile_bytes;
+    p.ana_img.fp16 = 0;
+
+    s->max_smem = 227 * 1024;
+    if ((e = cudaFuncSetAttribute(legendre_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  s->max_smem)) != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(legendre_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s->max_smem);
+}
+
+void tc_release(Plan& p) {
+    TcState* s = static_cast<TcState*>(p.tc);
+    if (!s) return;
+    void* ptrs[] = {s->d_maps, s->d_lam, s->d_nr, s->d_nkt, s->d_njt, s->d_syn_base, s->d_ana_base,
+                    s->d_syn_img, s->d_ana_img, s->d_syn_items, s->d_ana_items};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    delete s;
+    p.tc = nullptr;
+}
+
+static uint32_t tmem_cols_for(int n) {
+    uint32_t c = 32;
+    while ((int)c < n) c <<= 1;
+    return c;
+}
+
+cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, int64_t ldc, int K, cudaStream_t st) {
+    const TcState& s = *static_cast<const TcState*>(p.tc);
+    const TcDev t = make_dev(p);
+    syn_image_kernel<<<dim3(p.mmax, (p.rows[0] + BLK - 1) / BLK), 256, 0, st>>>(t, coeffs, ldc, K);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || s.n_syn_items == 0) return e;
+    const int ncols = 2 * K;
+    const int nct = (ncols + 255) / 256;
+    const int nt_cols = std::min(256, (ncols + 63) / 64 * 64);
+    int stages;
+    const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
+    legendre_tc_kernel<true><<<dim3(s.n_syn_items, nct), TC_THREADS, smem, st>>>(
+        t, s.d_syn_items, K, nt_cols, stages, tmem_cols_for(nt_cols), p.d_four, nullptr, 0, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_legendre_analysis_tc(const Plan& p, float2* coeffs, int64_t ldc, int K, bool add, cudaStream_t st) {
+    const TcState& s = *static_cast<const TcState*>(p.tc);
+    if (s.n_ana_items == 0) return cudaSuccess;
+    const TcDev t = make_dev(p);
+    const int ncols = 2 * K;
+    const int nct = (ncols + 255) / 256;
+    const int nt_cols = std::min(256, (ncols + 63) / 64 * 64);
+    int stages;
+    const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
+    legendre_tc_kernel<false><<<dim3(s.n_ana_items, nct), TC_THREADS, smem, st>>>(
+        t, s.d_ana_items, K, nt_cols, stages, tmem_cols_for(nt_cols), nullptr, coeffs, ldc, add ? 1 : 0);
+    return cudaGetLastError();
+}
+
 }  // namespace sht

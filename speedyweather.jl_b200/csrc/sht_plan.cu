@@ -137,7 +137,8 @@ cudaError_t upload(T** dst, const std::vector<T>& src, int64_t& bytes) {
 void release(Plan& p) {
     tc_release(p);
     void* ptrs[] = {p.d_rings, p.d_twiddle, p.d_lam, p.d_lam_off, p.d_j0, p.d_rows, p.d_lm_off, p.d_syn_items,
-                    p.d_ana_items, p.d_mt, p.d_gofs, p.d_grad, p.d_l_of, p.d_m_of, p.d_eig, p.d_eig_inv, p.d_four};
+                    p.d_ana_items, p.d_mt, p.d_gofs, p.d_grad, p.d_l_of, p.d_m_of, p.d_eig, p.d_eig_inv, p.d_four,
+                    p.d_err};
     for (void* q : ptrs)
         if (q) cudaFree(q);
 }
@@ -372,6 +373,8 @@ int build_plan(Plan& p) {
     p.four_elems = p.scratch_rows * 2 * std::max(1, d.nlayers);
     if ((e = cudaMalloc((void**)&p.d_four, p.four_elems * sizeof(float2))) != cudaSuccess)
         return cuda_fail(e, "sht_plan_create scratch");
+    if ((e = cudaMalloc((void**)&p.d_err, sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, "sht_plan_create");
+    if ((e = cudaMemset(p.d_err, 0, sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, "sht_plan_create");
     if ((e = fft_set_smem(p.smem_fft)) != cudaSuccess) return cuda_fail(e, "sht_plan_create fft smem");
     if (d.precision != SHT_PREC_FP32) {
         if (!tc_supported()) return fail(SHT_EUNSUPPORTED, "tensor-core Legendre precision %d not available", d.precision);
@@ -436,8 +439,12 @@ int sht_plan_create(const sht_desc* desc, sht_plan** out) {
     if (d.mmax < 1 || d.lmax < d.mmax || d.lmax > 8192)
         return fail(SHT_EINVAL, "spectrum lmax=%d mmax=%d invalid (need 1 <= mmax <= lmax)", d.lmax, d.mmax);
     if (d.nlayers < 1) return fail(SHT_EINVAL, "nlayers %d must be >= 1", d.nlayers);
-    if (d.precision < SHT_PREC_FP32 || d.precision > SHT_PREC_FP16X3)
+    if (d.precision < SHT_PREC_FP32 || d.precision > SHT_PREC_BF16X5)
         return fail(SHT_EINVAL, "precision %d unknown", d.precision);
+    if (d.precision == SHT_PREC_FP16X3)
+        return fail(SHT_EUNSUPPORTED, "precision SHT_PREC_FP16X3 (scaled split FP16) is not built in this library");
+    if (d.precision != SHT_PREC_FP32 && d.nlayers > 1024)
+        return fail(SHT_EINVAL, "tensor-core precisions support nlayers <= 1024");
     DeviceGuard g(d.device);
     if (!g.ok) return fail(SHT_ECUDA, "sht_plan_create: cannot select device %d", d.device);
     sht_plan* h = new (std::nothrow) sht_plan();
@@ -487,6 +494,17 @@ int sht_plan_tables(const sht_plan* plan, double* latd, double* weights, int32_t
     if (weights) std::memcpy(weights, p.weights.data(), p.nlat * sizeof(double));
     if (nlons) std::memcpy(nlons, p.nlons.data(), p.nlat * sizeof(int32_t));
     if (mmax_truncation) std::memcpy(mmax_truncation, p.mt.data(), p.nh * sizeof(int32_t));
+    return SHT_OK;
+}
+
+int sht_device_status(sht_plan* plan, int32_t* status) {
+    if (!plan || !status) return fail(SHT_EINVAL, "sht_device_status: NULL argument");
+    DeviceGuard g(plan->p.device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(e, "sht_device_status");
+    if ((e = cudaMemcpy(status, plan->p.d_err, sizeof(int32_t), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_fail(e, "sht_device_status");
+    if ((e = cudaMemset(plan->p.d_err, 0, sizeof(int32_t))) != cudaSuccess) return cuda_fail(e, "sht_device_status");
     return SHT_OK;
 }
 

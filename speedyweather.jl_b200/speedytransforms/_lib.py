@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "libsht.so")
 
 SHT_OK, SHT_EINVAL, SHT_ECUDA, SHT_ENOMEM, SHT_EUNSUPPORTED = 0, 1, 2, 3, 4
 GRID_FULL_GAUSSIAN, GRID_OCTAHEDRAL_GAUSSIAN = 0, 1
-PREC_FP32, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2
+PREC_FP32, PREC_BF16X3, PREC_FP16X3, PREC_BF16X5 = 0, 1, 2, 3
 SHORTCUTS = {"linear": 0, "quadratic": 1, "cubic": 2, "linquadcoslat2": 3, "lincubcoslat": 4}
 UNSCALE_COSLAT, ADD, FLIPSIGN, INVERSE = 1, 2, 4, 8
 
@@ -50,6 +50,7 @@ SIGNATURES = {
     "sht_uv_from_vordiv": (C.c_int, [_P, _P, _P, _P, _P, _I64, C.c_int, C.c_double, _P]),
     "sht_laplace": (C.c_int, [_P, _P, _P, _I64, C.c_int, C.c_uint, C.c_double, _P]),
     "sht_gradient": (C.c_int, [_P, _P, _P, _P, _I64, C.c_int, C.c_double, _P]),
+    "sht_device_status": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "sht_last_error": (C.c_char_p, []),
     "sht_version": (C.c_char_p, []),
 }

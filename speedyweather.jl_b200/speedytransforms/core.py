@@ -235,7 +235,8 @@ def _field_arg(f: Field, S, what):
 # ------------------------------------------------------------------------------------------
 # SpectralTransform
 # ------------------------------------------------------------------------------------------
-_PRECISIONS = {"fp32": _lib.PREC_FP32, "bf16x3": _lib.PREC_BF16X3, "fp16x3": _lib.PREC_FP16X3}
+_PRECISIONS = {"fp32": _lib.PREC_FP32, "bf16x3": _lib.PREC_BF16X3, "bf16x5": _lib.PREC_BF16X5,
+               "fp16x3": _lib.PREC_FP16X3}
 
 
 class SpectralTransform:
@@ -246,7 +247,8 @@ class SpectralTransform:
     ``SpectralTransform(grid=..., truncation=..., one_more_degree=...)`` and
     ``SpectralTransform(spectrum, Grid=OctahedralGaussianGrid, nlat_half=0, dealiasing=2)``.
     ``precision`` selects the Legendre arithmetic: "fp32" (CUDA cores), "bf16x3"
-    (tensor cores, split BF16) or "fp16x3" (tensor cores, scaled split FP16).
+    (tensor cores, split BF16, 3 products), "bf16x5" (tensor cores, Legendre
+    polynomials in 3 BF16 pieces, 5 products) or "fp16x3" (scaled split FP16).
     """
 
     def __init__(self, spectrum: Spectrum | None = None, grid: _GaussianGrid | None = None, *, NF=torch.float32,
@@ -303,6 +305,12 @@ class SpectralTransform:
     @property
     def handle(self):
         return self._plan
+
+    def device_status(self) -> int:
+        """Synchronise and return (then clear) the plan's device status word (0 = ok)."""
+        v = C.c_int32(0)
+        check(lib.sht_device_status(self._plan, C.byref(v)))
+        return int(v.value)
 
     def __repr__(self):
         return (f"SpectralTransform({self.spectrum}, {self.grid}, nlayers={self.nlayers}, "
