@@ -161,6 +161,26 @@ SHT_API int sht_laplace(sht_plan* plan, void* out, const void* alms, int64_t ldc
 SHT_API int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p, int64_t ldc, int K,
                  double radius, void* stream);
 
+/* Grid to spectral analysis that allocates nothing, for callers that cannot call
+ * cudaMalloc where they transform (inside a CUDA-graph capture they do not own,
+ * under a fixed start-up memory pool, or in a runtime that forbids allocation
+ * after initialisation). It has no counterpart in the reference.
+ * Same arguments and result as sht_analyze on an SHT_PREC_FP32 plan (FP32 Fourier
+ * and Legendre stages); the Fourier coefficients between the two kernels live in a
+ * fixed 8 MiB __device__ array of the library instead of the plan's scratch, which
+ * every GPU that loads the library holds until the process exits.
+ * Limit: scratch rows x 2 x K x 8 bytes <= 8 MiB (octahedral T63: K <= 223, T127: K <= 59,
+ * T255: K <= 15);
+ * larger calls return SHT_EINVAL. The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. All calls share the array: calls that overlap on the GPU (different
+ * streams, threads or plans) race and must be serialised by the caller. Every
+ * location the Legendre kernel reads is written by the Fourier kernel of the same
+ * call, so nothing needs clearing between calls.
+ * flags: SHT_ADD. */
+SHT_API int sht_analyze_static_scratch(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, int64_t ldc,
+                                       int K, unsigned flags, void* stream);
+
 /* Synchronises the device and returns (then clears) the plan's device status word:
  * 0 = no kernel gave up waiting; otherwise the code of the first bounded wait in a
  * tensor-core kernel that expired (1 s limit), whose outputs are then incomplete.

@@ -411,3 +411,15 @@ cudaError_t fft_set_smem(int bytes) {
 }
 
 }  // namespace sht
+
+namespace sht {
+// The analysis Fourier kernel writing FP32 coefficients into a caller-chosen scratch
+// (used by the static-scratch analysis entry point).
+cudaError_t launch_fft_analysis_to(const Plan& p, const float* grid, int64_t ldg, int K, float2* scratch,
+                                   cudaStream_t s) {
+    dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);
+    const TcImage none{};
+    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_rings, p.d_twiddle, grid, ldg, scratch, K, none);
+    return cudaGetLastError();
+}
+}  // namespace sht

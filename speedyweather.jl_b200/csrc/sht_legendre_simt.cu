@@ -239,3 +239,17 @@ cudaError_t launch_legendre_analysis_fp32(const Plan& p, float2* coeffs, int64_t
 }
 
 }  // namespace sht
+
+namespace sht {
+// The FP32 Legendre analysis reading the Fourier coefficients from a caller-chosen
+// scratch (used by the static-scratch analysis entry point).
+cudaError_t launch_legendre_analysis_fp32_from(const Plan& p, const float2* scratch, float2* coeffs, int64_t ldc,
+                                               int K, bool add, cudaStream_t s) {
+    if (p.n_ana_items == 0) return cudaSuccess;
+    dim3 g(p.n_ana_items, (2 * K + BN - 1) / BN, 2);
+    legendre_analysis_fp32_kernel<<<g, NT, 0, s>>>(p.d_ana_items, p.d_lam, p.d_lam_off, p.d_rows, p.d_j0, p.d_lm_off,
+                                                   p.d_rings, p.nh, p.nh_pad, p.lmax, scratch, coeffs, ldc, K,
+                                                   add ? 1 : 0);
+    return cudaGetLastError();
+}
+}  // namespace sht

@@ -645,3 +645,9 @@ int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p_, int64_t
 }
 
 }  // extern "C"
+
+namespace sht {
+// Accessors for entry points defined in other files of the library.
+const Plan* plan_impl(const sht_plan* plan) { return plan ? &plan->p : nullptr; }
+int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace sht

@@ -51,6 +51,7 @@ SIGNATURES = {
     "sht_laplace": (C.c_int, [_P, _P, _P, _I64, C.c_int, C.c_uint, C.c_double, _P]),
     "sht_gradient": (C.c_int, [_P, _P, _P, _P, _I64, C.c_int, C.c_double, _P]),
     "sht_device_status": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "sht_analyze_static_scratch": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
     "sht_last_error": (C.c_char_p, []),
     "sht_version": (C.c_char_p, []),
 }
