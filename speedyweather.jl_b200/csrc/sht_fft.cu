@@ -36,6 +36,17 @@ template <bool INV>
 __device__ __forceinline__ float2 twmul(float2 v, float2 w) {
     return INV ? cmulc(v, w) : cmul(v, w);
 }
+// Exact quotient x / d for 0 <= x < 2^22 and d >= 1 through a float reciprocal:
+// (x + 0.5) / d is at least 0.5 / d away from an integer and the two roundings
+// err by less than 1.2e-7 (x + 0.5) / d, so truncation gives floor(x / d). A few
+// instructions instead of the integer division sequence, in every index loop.
+struct Div {
+    int d;
+    float r;
+};
+__device__ __forceinline__ Div mkdiv(int d) { return Div{d, 1.0f / (float)d}; }
+__device__ __forceinline__ int quo(int x, Div v) { return (int)(((float)x + 0.5f) * v.r); }
+
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
@@ -92,10 +103,11 @@ __device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y
                             const float2* __restrict__ W) {
     const int nb = n / P;
     const int tstride = n / (Ns * P);
+    const Div dnb = mkdiv(nb), dns = mkdiv(Ns);
     for (int w = threadIdx.x; w < C * nb; w += blockDim.x) {
-        const int c = w / nb;
+        const int c = quo(w, dnb);
         const int b = w - c * nb;
-        const int k = b % Ns;
+        const int k = b - quo(b, dns) * Ns;
         const float2* x = X + (size_t)c * n + b;
         float2 v[P];
 #pragma unroll
@@ -126,13 +138,14 @@ __device__ void stage_generic(float2* __restrict__ X, float2* __restrict__ Y, fl
     const int nb = n / p;
     const int tstride = n / (Ns * p);
     const int cols = C * nb;
+    const Div dcols = mkdiv(cols), dnb = mkdiv(nb), dns = mkdiv(Ns);
     for (int t = threadIdx.x; t < p; t += blockDim.x) Wp[t] = W[t * nb];
     for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
-        const int col = w % cols;
-        const int r = w / cols;
-        const int c = col / nb;
+        const int r = quo(w, dcols);
+        const int col = w - r * cols;
+        const int c = quo(col, dnb);
         const int b = col - c * nb;
-        const int k = b % Ns;
+        const int k = b - quo(b, dns) * Ns;
         if (r > 0 && k > 0) {
             float2* xp = X + (size_t)c * n + b + r * nb;
             *xp = twmul<INV>(*xp, W[r * k * tstride]);
@@ -142,11 +155,12 @@ __device__ void stage_generic(float2* __restrict__ X, float2* __restrict__ Y, fl
     const int h = (p - 1) / 2;
     const int ngroups = (h + GR) / GR;          // r in [0, h]
     for (int w = threadIdx.x; w < cols * ngroups; w += blockDim.x) {
-        const int col = w % cols;
-        const int r0 = (w / cols) * GR;
-        const int c = col / nb;
+        const int g = quo(w, dcols);
+        const int col = w - g * cols;
+        const int r0 = g * GR;
+        const int c = quo(col, dnb);
         const int b = col - c * nb;
-        const int k = b % Ns;
+        const int k = b - quo(b, dns) * Ns;
         const float2* x = X + (size_t)c * n + b;
         const float2 x0 = x[0];
         float ar[GR], ai[GR], br[GR], bi[GR];
@@ -217,10 +231,112 @@ __device__ float2* run_fft(float2* X, float2* Y, float2* Wp, int n, int C, const
 }
 
 __device__ __forceinline__ int smem_tw_len(int n) { return (n + 1) & ~1; }
+
+// Global <-> shared copies with four independent accesses in flight per thread (the
+// CTA is latency-bound otherwise: one ring of C layers is loaded, transformed and
+// stored in sequence).
+__device__ __forceinline__ void load_twiddles(float2* W, const float2* __restrict__ tw, int n) {
+    for (int t0 = threadIdx.x; t0 < n; t0 += 4 * blockDim.x) {
+        float2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < n) v[u] = __ldg(tw + t);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < n) W[t] = v[u];
+        }
+    }
+}
+
+// X[c n + i] = (north ring value, south ring value) of layer k0 + c. Rings start at
+// multiples of 4 points on these grids, so 16-byte vectors are used when the layer
+// stride and base allow.
+__device__ __forceinline__ void load_rings(float2* X, const float* __restrict__ grid, int64_t ldg, int64_t off_n,
+                                           int64_t off_s, int k0, int C, int n, Div dn) {
+    const bool vec = ((ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(grid) & 15) == 0) && ((off_n & 3) == 0) &&
+                     ((off_s & 3) == 0) && ((n & 3) == 0);
+    if (vec) {
+        const int n4 = n >> 2, tot = C * n4;
+        const Div dn4 = mkdiv(n4);
+        for (int w0 = threadIdx.x; w0 < tot; w0 += 4 * blockDim.x) {
+            float4 a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int w = w0 + u * blockDim.x;
+                if (w < tot) {
+                    const int c = quo(w, dn4), i4 = w - c * n4;
+                    const float* g = grid + (int64_t)(k0 + c) * ldg;
+                    a[u] = __ldg(reinterpret_cast<const float4*>(g + off_n) + i4);
+                    b[u] = __ldg(reinterpret_cast<const float4*>(g + off_s) + i4);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int w = w0 + u * blockDim.x;
+                if (w < tot) {
+                    const int c = quo(w, dn4), i4 = w - c * n4;
+                    float4* x = reinterpret_cast<float4*>(X + (size_t)c * n + 4 * i4);
+                    x[0] = make_float4(a[u].x, b[u].x, a[u].y, b[u].y);
+                    x[1] = make_float4(a[u].z, b[u].z, a[u].w, b[u].w);
+                }
+            }
+        }
+        return;
+    }
+    for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
+        const int c = quo(w, dn);
+        const int i = w - c * n;
+        const float* g = grid + (int64_t)(k0 + c) * ldg;
+        X[w] = make_float2(g[off_n + i], g[off_s + i]);
+    }
+}
+
+// grid rings of layer k0 + c (=, or += with add) <- (Re z, Im z)
+__device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ldg, int64_t off_n, int64_t off_s, int k0,
+                                            int C, int n, Div dn, const float2* z, int add) {
+    const bool vec = ((ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(grid) & 15) == 0) && ((off_n & 3) == 0) &&
+                     ((off_s & 3) == 0) && ((n & 3) == 0);
+    if (vec) {
+        const int n4 = n >> 2, tot = C * n4;
+        const Div dn4 = mkdiv(n4);
+        for (int w = threadIdx.x; w < tot; w += blockDim.x) {
+            const int c = quo(w, dn4), i4 = w - c * n4;
+            const float4* zz = reinterpret_cast<const float4*>(z + (size_t)c * n + 4 * i4);
+            const float4 p0 = zz[0], p1 = zz[1];
+            float4 a = make_float4(p0.x, p0.z, p1.x, p1.z), b = make_float4(p0.y, p0.w, p1.y, p1.w);
+            float4* gn = reinterpret_cast<float4*>(grid + (int64_t)(k0 + c) * ldg + off_n) + i4;
+            float4* gs = reinterpret_cast<float4*>(grid + (int64_t)(k0 + c) * ldg + off_s) + i4;
+            if (add) {
+                const float4 on = *gn, os = *gs;
+                a = make_float4(a.x + on.x, a.y + on.y, a.z + on.z, a.w + on.w);
+                b = make_float4(b.x + os.x, b.y + os.y, b.z + os.z, b.w + os.w);
+            }
+            *gn = a;
+            *gs = b;
+        }
+        return;
+    }
+    for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
+        const int c = quo(w, dn);
+        const int i = w - c * n;
+        float* g = grid + (int64_t)(k0 + c) * ldg;
+        const float2 v = z[w];
+        if (add) {
+            g[off_n + i] += v.x;
+            g[off_s + i] += v.y;
+        } else {
+            g[off_n + i] = v.x;
+            g[off_s + i] = v.y;
+        }
+    }
+}
 // shared memory: W (n twiddles) | Wp (n, per-stage DFT table) | X (C n) | Y (C n)
 
 // grid -> Fourier scratch (E/O combinations weighted by the solid angle)
-__global__ void __launch_bounds__(1024) fft_analysis_kernel(const RingDesc* __restrict__ rings,
+__global__ void __launch_bounds__(512, 2) fft_analysis_kernel(const RingDesc* __restrict__ rings,
                                                            const float2* __restrict__ twiddle,
                                                            const float* __restrict__ grid, int64_t ldg,
                                                            float2* __restrict__ four, int K, const TcImage img) {
@@ -230,17 +346,13 @@ __global__ void __launch_bounds__(1024) fft_analysis_kernel(const RingDesc* __re
     if (k0 >= K) return;
     const int C = min(rd.chunk, K - k0);
     const int n = rd.n;
+    const Div dn = mkdiv(n), dC = mkdiv(C);
     float2* W = sm;
     float2* Wp = sm + smem_tw_len(n);
     float2* X = Wp + rd.wp_len;
     float2* Y = X + (size_t)C * n;
-    for (int t = threadIdx.x; t < n; t += blockDim.x) W[t] = twiddle[rd.tw_off + t];
-    for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
-        const int c = w / n;
-        const int i = w - c * n;
-        const float* g = grid + (int64_t)(k0 + c) * ldg;
-        X[w] = make_float2(g[rd.off_north + i], g[rd.off_south + i]);
-    }
+    load_twiddles(W, twiddle + rd.tw_off, n);
+    load_rings(X, grid, ldg, rd.off_north, rd.off_south, k0, C, n, dn);
     __syncthreads();
     const float2* Z = run_fft<false>(X, Y, Wp, n, C, rd, W);
     const float half_domega = 0.5f * rd.domega;
@@ -251,10 +363,11 @@ __global__ void __launch_bounds__(1024) fft_analysis_kernel(const RingDesc* __re
         // row j - j0(m); 8 real columns (4 layers) form one 16-byte chunk
         const int cbeg = 2 * k0, cend = 2 * (k0 + C);
         const int gbeg = cbeg / 8, ngr = (cend + 7) / 8 - gbeg;
+        const Div dngr = mkdiv(ngr);
         const int j = blockIdx.x;
         for (int w = threadIdx.x; w < ngr * nm; w += blockDim.x) {
-            const int g = gbeg + w % ngr;
-            const int m = w / ngr;
+            const int m = quo(w, dngr);
+            const int g = gbeg + (w - m * ngr);
             float ev[8], ov[8];
             bool have[8];
 #pragma unroll
@@ -315,8 +428,8 @@ __global__ void __launch_bounds__(1024) fft_analysis_kernel(const RingDesc* __re
         return;
     }
     for (int w = threadIdx.x; w < C * nm; w += blockDim.x) {
-        const int c = w % C;
-        const int m = w / C;
+        const int m = quo(w, dC);
+        const int c = w - m * C;
         const float2 a = Z[(size_t)c * n + m];
         const float2 b = Z[(size_t)c * n + (m == 0 ? 0 : n - m)];
         // F_N = (a + conj b)/2, F_S = (a - conj b)/(2i)
@@ -331,7 +444,7 @@ __global__ void __launch_bounds__(1024) fft_analysis_kernel(const RingDesc* __re
 }
 
 // Fourier scratch -> grid
-__global__ void __launch_bounds__(1024) fft_synthesis_kernel(const RingDesc* __restrict__ rings,
+__global__ void __launch_bounds__(512, 2) fft_synthesis_kernel(const RingDesc* __restrict__ rings,
                                                             const float2* __restrict__ twiddle,
                                                             const float2* __restrict__ four, float* __restrict__ grid,
                                                             int64_t ldg, int K, int unscale, int add) {
@@ -341,16 +454,17 @@ __global__ void __launch_bounds__(1024) fft_synthesis_kernel(const RingDesc* __r
     if (k0 >= K) return;
     const int C = min(rd.chunk, K - k0);
     const int n = rd.n;
+    const Div dn = mkdiv(n), dC = mkdiv(C);
     float2* W = sm;
     float2* Wp = sm + smem_tw_len(n);
     float2* X = Wp + rd.wp_len;
     float2* Y = X + (size_t)C * n;
-    for (int t = threadIdx.x; t < n; t += blockDim.x) W[t] = twiddle[rd.tw_off + t];
+    load_twiddles(W, twiddle + rd.tw_off, n);
     const float scale = unscale ? rd.coslat_inv : 1.0f;
     const int nhalf = n / 2;   // highest source frequency
     for (int w = threadIdx.x; w < C * (nhalf + 1); w += blockDim.x) {
-        const int c = w % C;
-        const int m = w / C;
+        const int m = quo(w, dC);
+        const int c = w - m * C;
         float2 gn = make_float2(0.f, 0.f), gs = make_float2(0.f, 0.f);
         if (m <= rd.mt) {
             const int64_t row = (rd.gofs + m) * 2;
@@ -369,24 +483,12 @@ __global__ void __launch_bounds__(1024) fft_synthesis_kernel(const RingDesc* __r
     }
     __syncthreads();
     const float2* z = run_fft<true>(X, Y, Wp, n, C, rd, W);
-    for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
-        const int c = w / n;
-        const int i = w - c * n;
-        float* g = grid + (int64_t)(k0 + c) * ldg;
-        const float2 v = z[w];
-        if (add) {
-            g[rd.off_north + i] += v.x;
-            g[rd.off_south + i] += v.y;
-        } else {
-            g[rd.off_north + i] = v.x;
-            g[rd.off_south + i] = v.y;
-        }
-    }
+    store_rings(grid, ldg, rd.off_north, rd.off_south, k0, C, n, dn, z, add);
 }
 
 }  // namespace
 
-static int fft_threads(const Plan&) { return 1024; }
+static int fft_threads(const Plan&) { return 512; }
 
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, bool to_image) {
     dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);

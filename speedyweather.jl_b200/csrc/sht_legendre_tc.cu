@@ -385,52 +385,50 @@ __device__ __forceinline__ void split_bf16(float x, uint16_t* out, int npieces) 
     }
 }
 
-__global__ void syn_image_kernel(const TcDev t, const float2* __restrict__ coeffs, int64_t ldc, int K) {
+// One CTA per (m, 64-row block kt): the block's 128 consecutive packed coefficients
+// (both parities) of up to 32 layers at a time are staged in shared memory with
+// coalesced loads, then every thread assembles 16-byte chunks (8 rows of one parity
+// and one real column) of the swizzled tiles.
+constexpr int SYN_KCHUNK = 32;
+__global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const float2* __restrict__ coeffs,
+                                                        int64_t ldc, int K) {
+    __shared__ float2 sc[SYN_KCHUNK][2 * BLK + 1];
     const int m = blockIdx.x;
     const int kt = blockIdx.y;
     if (kt >= t.nkt[m]) return;
-    const int rows_m = t.rows[m];
     const int64_t lmo = t.lm_off[m];
+    const int lmrem = t.lmax - m - 2 * BLK * kt;      // coefficients of this order left from the block start
     uint8_t* img = reinterpret_cast<uint8_t*>(const_cast<uint16_t*>(t.syn_img));
-    for (int w = threadIdx.x; w < K * 8; w += blockDim.x) {
-        const int ib8 = w % 8;
-        const int k = w / 8;
-        // 8 parity rows [64 kt + 8 ib8, +8) of both parities = 16 consecutive lm
-        float re[2][8], im[2][8];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int par = q & 1, ii = q >> 1;
-            const int i = kt * BLK + ib8 * 8 + ii;
-            const int l = m + 2 * i + par;
-            float2 v = make_float2(0.f, 0.f);
-            if (i < rows_m && l < t.lmax) v = coeffs[(int64_t)k * ldc + lmo + 2 * i + par];
-            re[par][ii] = v.x;
-            im[par][ii] = v.y;
+    const int64_t tile0 = t.syn_tile_base[m] + kt, tile1 = t.syn_tile_base[m] + t.nkt[m] + kt;
+    for (int k0 = 0; k0 < K; k0 += SYN_KCHUNK) {
+        const int kc = min(SYN_KCHUNK, K - k0);
+        __syncthreads();
+        for (int w = threadIdx.x; w < kc * 2 * BLK; w += blockDim.x) {
+            const int kk = w / (2 * BLK), q = w % (2 * BLK);
+            sc[kk][q] = q < lmrem ? coeffs[(int64_t)(k0 + kk) * ldc + lmo + 2 * BLK * kt + q] : make_float2(0.f, 0.f);
         }
+        __syncthreads();
+        // items: (layer kk, 8-row chunk ib8, parity, re/im)
+        for (int w = threadIdx.x; w < kc * 32; w += blockDim.x) {
+            const int ib8 = w & 7, par = (w >> 3) & 1, ri = (w >> 4) & 1, kk = w >> 5;
+            const int c = 2 * (k0 + kk) + ri;
+            uint16_t pc[3][8];
 #pragma unroll
-        for (int par = 0; par < 2; ++par) {
-            const int64_t tile = t.syn_tile_base[m] + (int64_t)par * t.nkt[m] + kt;
-#pragma unroll
-            for (int ri = 0; ri < 2; ++ri) {
-                const int c = 2 * k + ri;
-                const float* src = ri ? im[par] : re[par];
-                uint16_t pc[3][8];
-#pragma unroll
-                for (int ii = 0; ii < 8; ++ii) {
-                    uint16_t tmp[3];
-                    split_bf16(src[ii], tmp, t.npb);
-                    for (int q = 0; q < t.npb; ++q) pc[q][ii] = tmp[q];
-                }
-                const int64_t off = (int64_t)(c / 8) * 1024 + (c % 8) * 128 + ((ib8 ^ (c % 8)) * 16);
-                for (int q = 0; q < t.npb; ++q) {
-                    uint8_t* dst = img + (tile * t.npb + q) * t.syn_tile_bytes + off;
-                    uint4 u;
-                    u.x = (uint32_t)pc[q][0] | ((uint32_t)pc[q][1] << 16);
-                    u.y = (uint32_t)pc[q][2] | ((uint32_t)pc[q][3] << 16);
-                    u.z = (uint32_t)pc[q][4] | ((uint32_t)pc[q][5] << 16);
-                    u.w = (uint32_t)pc[q][6] | ((uint32_t)pc[q][7] << 16);
-                    *reinterpret_cast<uint4*>(dst) = u;
-                }
+            for (int ii = 0; ii < 8; ++ii) {
+                const float2 v = sc[kk][2 * (8 * ib8 + ii) + par];
+                uint16_t tmp[3];
+                split_bf16(ri ? v.y : v.x, tmp, t.npb);
+                for (int q = 0; q < t.npb; ++q) pc[q][ii] = tmp[q];
+            }
+            const int64_t off = (int64_t)(c / 8) * 1024 + (c % 8) * 128 + ((ib8 ^ (c % 8)) * 16);
+            const int64_t tile = par ? tile1 : tile0;
+            for (int q = 0; q < t.npb; ++q) {
+                uint4 u;
+                u.x = (uint32_t)pc[q][0] | ((uint32_t)pc[q][1] << 16);
+                u.y = (uint32_t)pc[q][2] | ((uint32_t)pc[q][3] << 16);
+                u.z = (uint32_t)pc[q][4] | ((uint32_t)pc[q][5] << 16);
+                u.w = (uint32_t)pc[q][6] | ((uint32_t)pc[q][7] << 16);
+                *reinterpret_cast<uint4*>(img + (tile * t.npb + q) * t.syn_tile_bytes + off) = u;
             }
         }
     }

@@ -266,7 +266,7 @@ int build_plan(Plan& p) {
     std::vector<RingDesc> rings(nh);
     std::vector<float2> tw;
     int64_t gofs = 0;
-    const int smem_budget = 224 * 1024;
+    const int smem_budget = 113 * 1024;     // two CTAs per SM
     int max_smem = 0;
     p.min_chunk = 1 << 30;
     for (int j = 0; j < nh; ++j) {
