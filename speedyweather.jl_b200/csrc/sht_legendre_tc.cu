@@ -23,9 +23,10 @@
 //   coefficients for the synthesis, the FFT kernel for the analysis) directly as
 //   swizzled shared-memory images in global memory and loaded with 1-D bulk copies.
 //
-// One CTA computes one 128 x N output tile (N <= 256 real columns): warp 0 issues
-// the copies, warp 1 owns the tensor memory and one of its threads issues the
-// MMAs, warps 2-5 read the accumulator (tcgen05.ld) and store. Every wait is
+// A persistent CTA per SM computes a sequence of 128 x N output tiles (N <= 256 real
+// columns): warp 0 issues the copies, warp 1 owns the tensor memory (two
+// accumulators) and one of its threads issues the MMAs, warps 2-5 read the
+// accumulator (tcgen05.ld) and store while the next tile accumulates. Every wait is
 // bounded by a one-second global-timer limit; on expiry the CTA records an error
 // in the plan's status word, drains, frees its tensor memory and returns.
 #include <cuda.h>
@@ -92,6 +93,7 @@ struct TcState {
     TcItem* d_ana_items = nullptr;
     int n_ana_items = 0;
     int max_smem = 0;
+    int nsm = 148;                 // SMs of the device (persistent grid)
 };
 
 // ---------------------------------------------------------------- PTX wrappers
@@ -188,54 +190,101 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 // ---------------------------------------------------------------- the GEMM kernel
 // SYN: A = Lam^T (MN-major), B = synthesis image (K-major), D -> Fourier scratch.
 // ANA: A = Lam (K-major), B = analysis image (MN-major), D -> coefficients.
+// Persistent: CTA b of the grid's x dimension computes the items b, b + gridDim.x, ...
+// of its column tile (grid y). The copy warp runs ahead through a ring of shared
+// memory stages across items; the MMA thread alternates two accumulators in tensor
+// memory so that the epilogue of one item overlaps the MMAs of the next.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <bool SYN>
+__device__ __forceinline__ int item_steps(const TcDev& t, const TcItem& it) {
+    return SYN ? t.nkt[it.m] : t.njt[it.m];
+}
+
+template <bool SYN>
+__device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_cols, int K, uint32_t taddr, int r,
+                               float2* four, float2* coeffs, int64_t ldc, int add, bool good) {
+    const int m = it.m, par = it.par, tile = it.tile;
+    if (SYN) {
+        const int j = t.j0[m] + tile * 128 + r;
+        const bool valid = good && j < t.nh && m <= t.rings[j].mt;
+        float2* dst = valid ? four + ((t.rings[j].gofs + m) * 2 + par) * K : nullptr;
+        for (int c0 = 0; c0 < nt_cols; c0 += 32) {
+            float v[32];
+            tmem_ld32(taddr + c0, v);
+            if (!valid) continue;
+#pragma unroll
+            for (int q = 0; q < 16; q += 2) {
+                const int k = (ct * 256 + c0) / 2 + q;
+                if (k + 1 < K && (K % 2) == 0) {    // 16-byte aligned: row * K and k even
+                    *reinterpret_cast<float4*>(dst + k) = make_float4(v[2 * q], v[2 * q + 1], v[2 * q + 2], v[2 * q + 3]);
+                } else {
+                    if (k < K) dst[k] = make_float2(v[2 * q], v[2 * q + 1]);
+                    if (k + 1 < K) dst[k + 1] = make_float2(v[2 * q + 2], v[2 * q + 3]);
+                }
+            }
+        }
+    } else {
+        const int i = tile * 128 + r;
+        const bool valid = good && i < t.rows[m] && m + 2 * i + par < t.lmax;
+        const int64_t lmo = t.lm_off[m];
+        for (int c0 = 0; c0 < nt_cols; c0 += 32) {
+            float v[32];
+            tmem_ld32(taddr + c0, v);
+            if (!valid) continue;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int k = (ct * 256 + c0) / 2 + q;
+                if (k >= K) break;
+                float2* d = coeffs + (int64_t)k * ldc + lmo + 2 * i + par;
+                float2 val = make_float2(v[2 * q], v[2 * q + 1]);
+                if (add) {
+                    const float2 o = *d;
+                    val.x += o.x;
+                    val.y += o.y;
+                }
+                *d = val;
+            }
+        }
+    }
+}
+
 template <bool SYN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    legendre_tc_kernel(const TcDev t, const TcItem* __restrict__ items, int K, int nt_cols, int stages,
-                       uint32_t tmem_cols, float2* __restrict__ four, float2* __restrict__ coeffs, int64_t ldc,
+    legendre_tc_kernel(const TcDev t, const TcItem* __restrict__ items, int nitems, int K, int nt_cols, int stages,
+                       uint32_t acc_cols, float2* __restrict__ four, float2* __restrict__ coeffs, int64_t ldc,
                        int add) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const TcItem it = items[blockIdx.x];
-    const int m = it.m, par = it.par, tile = it.tile;
     const int ct = blockIdx.y;                       // column tile (256 columns)
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int nsteps = SYN ? t.nkt[m] : t.njt[m];
     const int a_bytes = t.npa * A_PIECE_BYTES;
     const int b_piece_bytes = nt_cols * 128;
     const int stage_bytes = a_bytes + t.npb * b_piece_bytes;
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + (size_t)stages * stage_bytes);
     uint64_t* empty_bar = full_bar + stages;
-    uint64_t* acc_bar = empty_bar + stages;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_bar + 1);
+    uint64_t* accf = empty_bar + stages;             // accumulator a ready   (tcgen05.commit)
+    uint64_t* acce = accf + 2;                       // accumulator a drained (128 epilogue threads)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + 2);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-
-    const int rows_m = t.rows[m];
-    const int j0 = t.j0[m];
-    const int64_t lmo = t.lm_off[m];
-
-    if (nsteps == 0) {          // analysis of an order no ring carries: coefficients are zero
-        if (!SYN && !add && warp >= 2) {
-            const int r = (warp % 4) * 32 + lane;
-            const int i = tile * 128 + r;
-            if (i < rows_m && m + 2 * i + par < t.lmax)
-                for (int c = 0; c < nt_cols && ct * 256 + c < 2 * K; c += 2)
-                    coeffs[(int64_t)((ct * 256 + c) / 2) * ldc + lmo + 2 * i + par] = make_float2(0.f, 0.f);
-        }
-        return;
-    }
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; ++s) {
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
-        mbar_init(acc_bar, 1);
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&accf[a], 1);
+            mbar_init(&acce[a], 128);
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(tmem_cols)
+                     "r"(2 * acc_cols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -244,130 +293,140 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    const CUtensorMap* map = t.maps + (2 * m + par);
     if (warp == 0 && lane == 0) {
         // ------------------------------------------------ producer
-        const int64_t tb = SYN ? t.syn_tile_base[m] + (int64_t)par * t.nkt[m] : t.ana_tile_base[m] + (int64_t)par * t.njt[m];
         const int64_t img_tile_bytes = SYN ? t.syn_tile_bytes : t.ana_tile_bytes;
         const uint8_t* img = reinterpret_cast<const uint8_t*>(SYN ? t.syn_img : t.ana_img);
         const int64_t col_off = SYN ? (int64_t)ct * 256 * 128 : (int64_t)ct * 4 * BOX_BYTES;
-        for (int ks = 0; ks < nsteps; ++ks) {
-            const int s = ks % stages;
-            if (ks >= stages && !mbar_wait(&empty_bar[s], ((ks / stages) - 1) & 1)) {
-                *abort_flag = 1;
-                atomicExch(t.err, 1);
-                break;
-            }
-            if (*abort_flag) break;
-            uint8_t* st = smem + (size_t)s * stage_bytes;
-            mbar_expect_tx(&full_bar[s], (uint32_t)stage_bytes);
-            for (int pa = 0; pa < t.npa; ++pa) {
-                uint8_t* a = st + pa * A_PIECE_BYTES;
-                if (SYN) {   // rings [128 tile, +128) of rows [64 ks, +64)
-                    tma_load_3d(a, map, tile * 128, ks * BLK, pa, &full_bar[s]);
-                    tma_load_3d(a + BOX_BYTES, map, tile * 128 + BLK, ks * BLK, pa, &full_bar[s]);
-                } else {     // rows [128 tile, +128) of rings [64 ks, +64)
-                    tma_load_3d(a, map, ks * BLK, tile * 128, pa, &full_bar[s]);
-                    tma_load_3d(a + BOX_BYTES, map, ks * BLK, tile * 128 + BLK, pa, &full_bar[s]);
+        int g = 0;
+        bool ok = true;
+        for (int ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ix += gridDim.x) {
+            const TcItem it = items[ix];
+            const int m = it.m, par = it.par, tile = it.tile;
+            const int nsteps = item_steps<SYN>(t, it);
+            const CUtensorMap* map = t.maps + (2 * m + par);
+            const int64_t tb = SYN ? t.syn_tile_base[m] + (int64_t)par * t.nkt[m]
+                                   : t.ana_tile_base[m] + (int64_t)par * t.njt[m];
+            for (int ks = 0; ks < nsteps; ++ks, ++g) {
+                const int s = g % stages;
+                if (g >= stages && !mbar_wait(&empty_bar[s], ((g / stages) - 1) & 1)) {
+                    *abort_flag = 1;
+                    atomicExch(t.err, 1);
+                    ok = false;
+                    break;
+                }
+                uint8_t* st = smem + (size_t)s * stage_bytes;
+                mbar_expect_tx(&full_bar[s], (uint32_t)stage_bytes);
+                for (int pa = 0; pa < t.npa; ++pa) {
+                    uint8_t* a = st + pa * A_PIECE_BYTES;
+                    if (SYN) {   // rings [128 tile, +128) of rows [64 ks, +64)
+                        tma_load_3d(a, map, tile * 128, ks * BLK, pa, &full_bar[s]);
+                        tma_load_3d(a + BOX_BYTES, map, tile * 128 + BLK, ks * BLK, pa, &full_bar[s]);
+                    } else {     // rows [128 tile, +128) of rings [64 ks, +64)
+                        tma_load_3d(a, map, ks * BLK, tile * 128, pa, &full_bar[s]);
+                        tma_load_3d(a + BOX_BYTES, map, ks * BLK, tile * 128 + BLK, pa, &full_bar[s]);
+                    }
+                }
+                for (int pb = 0; pb < t.npb; ++pb) {
+                    const uint8_t* src = img + ((tb + ks) * t.npb + pb) * img_tile_bytes + col_off;
+                    bulk_load(st + a_bytes + pb * b_piece_bytes, src, (uint32_t)b_piece_bytes, &full_bar[s]);
                 }
             }
-            for (int pb = 0; pb < t.npb; ++pb) {
-                const uint8_t* src = img + ((tb + ks) * t.npb + pb) * img_tile_bytes + col_off;
-                bulk_load(st + a_bytes + pb * b_piece_bytes, src, (uint32_t)b_piece_bytes, &full_bar[s]);
-            }
         }
+        // No copy may still be landing in shared memory when the CTA exits: wait for the
+        // last fill of every stage (already complete unless the MMA thread gave up).
+        for (int u = g - 1; u >= 0 && u >= g - stages; --u)
+            if (!mbar_wait(&full_bar[u % stages], (u / stages) & 1)) atomicExch(t.err, 5);
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------ MMA issuer
         const uint32_t idesc = idesc_f16(1u, SYN ? 1u : 0u, SYN ? 0u : 1u, (uint32_t)nt_cols);
+        int g = 0, ti = 0;
         bool ok = true;
-        for (int ks = 0; ks < nsteps && ok; ++ks) {
-            const int s = ks % stages;
-            if (!mbar_wait(&full_bar[s], (ks / stages) & 1)) {
+        for (int ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ix += gridDim.x) {
+            const TcItem it = items[ix];
+            const int nsteps = item_steps<SYN>(t, it);
+            if (nsteps == 0) continue;
+            const int a = ti & 1;
+            if (ti >= 2 && !mbar_wait(&acce[a], ((ti / 2) - 1) & 1)) {
                 *abort_flag = 1;
-                atomicExch(t.err, 2);
-                ok = false;
+                atomicExch(t.err, 4);
                 break;
             }
             tc_fence_after();
-            const uint32_t st = smem_u32(smem + (size_t)s * stage_bytes);
-            for (int kk = 0; kk < BLK / 16; ++kk) {
-                for (int q = 0; q < t.nprod; ++q) {
-                    const int pa = (t.prod >> (4 * q)) & 3, pb = (t.prod >> (4 * q + 2)) & 3;
-                    const uint32_t a = st + pa * A_PIECE_BYTES;
-                    const uint32_t b = st + a_bytes + pb * b_piece_bytes;
-                    uint64_t da, db;
-                    if (SYN) {
-                        da = sdesc(a + kk * 2048, BOX_BYTES, 1024);     // MN-major: 16 rows per step
-                        db = sdesc(b + kk * 32, 16, 1024);              // K-major: 32 B per step
-                    } else {
-                        da = sdesc(a + kk * 32, 16, 1024);
-                        db = sdesc(b + kk * 2048, BOX_BYTES, 1024);
-                    }
-                    umma_f16(tmem, da, db, idesc, (ks | kk | q) ? 1u : 0u);
+            const uint32_t dacc = tmem + (uint32_t)(a * acc_cols);
+            for (int ks = 0; ks < nsteps; ++ks, ++g) {
+                const int s = g % stages;
+                if (!mbar_wait(&full_bar[s], (g / stages) & 1)) {
+                    *abort_flag = 1;
+                    atomicExch(t.err, 2);
+                    ok = false;
+                    break;
                 }
+                tc_fence_after();
+                const uint32_t st = smem_u32(smem + (size_t)s * stage_bytes);
+                for (int kk = 0; kk < BLK / 16; ++kk) {
+                    for (int q = 0; q < t.nprod; ++q) {
+                        const int pa = (t.prod >> (4 * q)) & 3, pb = (t.prod >> (4 * q + 2)) & 3;
+                        const uint32_t aa = st + pa * A_PIECE_BYTES;
+                        const uint32_t bb = st + a_bytes + pb * b_piece_bytes;
+                        uint64_t da, db;
+                        if (SYN) {
+                            da = sdesc(aa + kk * 2048, BOX_BYTES, 1024);     // MN-major: 16 rows per step
+                            db = sdesc(bb + kk * 32, 16, 1024);              // K-major: 32 B per step
+                        } else {
+                            da = sdesc(aa + kk * 32, 16, 1024);
+                            db = sdesc(bb + kk * 2048, BOX_BYTES, 1024);
+                        }
+                        umma_f16(dacc, da, db, idesc, (ks | kk | q) ? 1u : 0u);
+                    }
+                }
+                umma_commit(&empty_bar[s]);      // frees the stage once these MMAs complete
             }
-            umma_commit(&empty_bar[s]);      // frees the stage once these MMAs complete
+            umma_commit(&accf[a]);               // accumulator ready (or drained after an abort)
+            ++ti;
         }
-        umma_commit(acc_bar);                // accumulator ready (or drained after an abort)
+        // Every MMA must have completed before the tensor memory is released.
+        if (ti > 0 && !mbar_wait(&accf[(ti - 1) & 1], ((ti - 1) / 2) & 1)) atomicExch(t.err, 6);
     } else if (warp >= 2) {
         // ------------------------------------------------ epilogue
-        const bool ok = mbar_wait(acc_bar, 0);
-        if (!ok) {
-            *abort_flag = 1;
-            atomicExch(t.err, 3);
-        }
-        tc_fence_after();
         const int quarter = warp % 4;
         const int r = quarter * 32 + lane;
-        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
-        const bool good = ok && !*abort_flag;
-        if (SYN) {
-            const int j = j0 + tile * 128 + r;
-            const bool valid = good && j < t.nh && m <= t.rings[j].mt;
-            float2* dst = valid ? four + ((t.rings[j].gofs + m) * 2 + par) * K : nullptr;
-            for (int c0 = 0; c0 < nt_cols; c0 += 32) {
-                float v[32];
-                tmem_ld32(taddr + c0, v);
-                if (!valid) continue;
-#pragma unroll
-                for (int q = 0; q < 16; q += 2) {
-                    const int k = (ct * 256 + c0) / 2 + q;
-                    if (k + 1 < K && (K % 2) == 0) {    // 16-byte aligned: row * K and k even
-                        *reinterpret_cast<float4*>(dst + k) = make_float4(v[2 * q], v[2 * q + 1], v[2 * q + 2], v[2 * q + 3]);
-                    } else {
-                        if (k < K) dst[k] = make_float2(v[2 * q], v[2 * q + 1]);
-                        if (k + 1 < K) dst[k + 1] = make_float2(v[2 * q + 2], v[2 * q + 3]);
-                    }
+        int ti = 0;
+        for (int ix = blockIdx.x; ix < nitems; ix += gridDim.x) {
+            const TcItem it = items[ix];
+            if (item_steps<SYN>(t, it) == 0) {      // analysis of an order no ring carries: zeros
+                if (!SYN && !add && !*abort_flag) {
+                    const int i = it.tile * 128 + r;
+                    if (i < t.rows[it.m] && it.m + 2 * i + it.par < t.lmax)
+                        for (int c = 0; c < nt_cols && ct * 256 + c < 2 * K; c += 2)
+                            coeffs[(int64_t)((ct * 256 + c) / 2) * ldc + t.lm_off[it.m] + 2 * i + it.par] =
+                                make_float2(0.f, 0.f);
                 }
+                continue;
             }
-        } else {
-            const int i = tile * 128 + r;
-            const bool valid = good && i < rows_m && m + 2 * i + par < t.lmax;
-            for (int c0 = 0; c0 < nt_cols; c0 += 32) {
-                float v[32];
-                tmem_ld32(taddr + c0, v);
-                if (!valid) continue;
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int k = (ct * 256 + c0) / 2 + q;
-                    if (k >= K) break;
-                    float2* d = coeffs + (int64_t)k * ldc + lmo + 2 * i + par;
-                    float2 val = make_float2(v[2 * q], v[2 * q + 1]);
-                    if (add) {
-                        const float2 o = *d;
-                        val.x += o.x;
-                        val.y += o.y;
-                    }
-                    *d = val;
-                }
+            const int a = ti & 1;
+            // warp-uniform outcome: tcgen05.ld below is a warp-collective instruction
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&accf[a], (ti / 2) & 1));
+            if (!ok) {
+                *abort_flag = 1;
+                atomicExch(t.err, 3);
             }
+            tc_fence_after();
+            const uint32_t taddr = tmem + (uint32_t)(a * acc_cols) + ((uint32_t)(quarter * 32) << 16);
+            epilogue_store<SYN>(t, it, ct, nt_cols, K, taddr, r, four, coeffs, ldc, add, ok && !*abort_flag);
+            tc_fence_before();
+            mbar_arrive(&acce[a]);
+            ++ti;
+            if (!ok) break;
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
+        __syncwarp();
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * acc_cols)
+                     : "memory");
     }
 }
 
@@ -647,6 +706,12 @@ cudaError_t tc_prepare(Plan& p) {
     p.ana_img.fp16 = 0;
 
     s->max_smem = 227 * 1024;
+    {
+        int dev = 0, nsm = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
+            s->nsm = nsm;
+    }
     if ((e = cudaFuncSetAttribute(legendre_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   s->max_smem)) != cudaSuccess)
         return e;
@@ -681,8 +746,8 @@ cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, in
     const int nt_cols = std::min(256, (ncols + 63) / 64 * 64);
     int stages;
     const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
-    legendre_tc_kernel<true><<<dim3(s.n_syn_items, nct), TC_THREADS, smem, st>>>(
-        t, s.d_syn_items, K, nt_cols, stages, tmem_cols_for(nt_cols), p.d_four, nullptr, 0, 0);
+    legendre_tc_kernel<true><<<dim3(std::min(s.n_syn_items, s.nsm), nct), TC_THREADS, smem, st>>>(
+        t, s.d_syn_items, s.n_syn_items, K, nt_cols, stages, tmem_cols_for(nt_cols), p.d_four, nullptr, 0, 0);
     return cudaGetLastError();
 }
 
@@ -695,8 +760,9 @@ cudaError_t launch_legendre_analysis_tc(const Plan& p, float2* coeffs, int64_t l
     const int nt_cols = std::min(256, (ncols + 63) / 64 * 64);
     int stages;
     const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
-    legendre_tc_kernel<false><<<dim3(s.n_ana_items, nct), TC_THREADS, smem, st>>>(
-        t, s.d_ana_items, K, nt_cols, stages, tmem_cols_for(nt_cols), nullptr, coeffs, ldc, add ? 1 : 0);
+    legendre_tc_kernel<false><<<dim3(std::min(s.n_ana_items, s.nsm), nct), TC_THREADS, smem, st>>>(
+        t, s.d_ana_items, s.n_ana_items, K, nt_cols, stages, tmem_cols_for(nt_cols), nullptr, coeffs, ldc,
+        add ? 1 : 0);
     return cudaGetLastError();
 }
 
