@@ -50,22 +50,58 @@ __device__ __forceinline__ int quo(int x, Div v) { return (int)(((float)x + 0.5f
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
-// y = DFT_P(v) (forward: exp(-2 pi i rs/P); inverse: exp(+...)). W is the ring's
-// table exp(-2 pi i t / n); W_P^t = W[t * (n / P)].
+// cos and sin of 2 pi t / P for the odd radices (t <= (P - 1) / 2)
+__host__ __device__ constexpr float rot_cos(int P, int t) {
+    return P == 3 ? -0.5f
+         : P == 5 ? (t == 1 ? 0.30901699437494745f : -0.8090169943749473f)
+                  : (t == 1 ? 0.6234898018587336f : t == 2 ? -0.22252093395631434f : -0.900968867902419f);
+}
+__host__ __device__ constexpr float rot_sin(int P, int t) {
+    return P == 3 ? 0.8660254037844387f
+         : P == 5 ? (t == 1 ? 0.9510565162951535f : 0.5877852522924732f)
+                  : (t == 1 ? 0.7818314824680298f : t == 2 ? 0.9749279121818236f : 0.43388373911755823f);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2 a, float2 b, float2 c, float2 d, float2& y0, float2& y1, float2& y2,
+                                     float2& y3) {
+    const float2 s02 = cadd(a, c), d02 = csub(a, c);
+    const float2 s13 = cadd(b, d), d13 = csub(b, d);
+    // forward: y1 = d02 - i d13, y3 = d02 + i d13
+    const float2 jd = INV ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);
+    y0 = cadd(s02, s13);
+    y2 = csub(s02, s13);
+    y1 = cadd(d02, jd);
+    y3 = csub(d02, jd);
+}
+
+// y = DFT_P(v) (forward: exp(-2 pi i rs/P); inverse: exp(+...)), P in {2, 3, 4, 5, 7, 8}.
 template <int P, bool INV>
-__device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P], const float2* W, int pstride) {
+__device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P]) {
     if constexpr (P == 2) {
         y[0] = cadd(v[0], v[1]);
         y[1] = csub(v[0], v[1]);
     } else if constexpr (P == 4) {
-        const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-        const float2 s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
-        // forward: y1 = d02 - i d13, y3 = d02 + i d13
-        const float2 jd = INV ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);
-        y[0] = cadd(s02, s13);
-        y[2] = csub(s02, s13);
-        y[1] = cadd(d02, jd);
-        y[3] = csub(d02, jd);
+        dft4<INV>(v[0], v[1], v[2], v[3], y[0], y[1], y[2], y[3]);
+    } else if constexpr (P == 8) {
+        // two DFT_4 of the even and odd points, combined with exp(-+ i pi r / 4)
+        float2 e[4], o[4];
+        dft4<INV>(v[0], v[2], v[4], v[6], e[0], e[1], e[2], e[3]);
+        dft4<INV>(v[1], v[3], v[5], v[7], o[0], o[1], o[2], o[3]);
+        constexpr float h = 0.7071067811865476f;
+        const float2 o1 = INV ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                              : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+        const float2 o2 = INV ? make_float2(-o[2].y, o[2].x) : make_float2(o[2].y, -o[2].x);
+        const float2 o3 = INV ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                              : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+        y[0] = cadd(e[0], o[0]);
+        y[4] = csub(e[0], o[0]);
+        y[1] = cadd(e[1], o1);
+        y[5] = csub(e[1], o1);
+        y[2] = cadd(e[2], o2);
+        y[6] = csub(e[2], o2);
+        y[3] = cadd(e[3], o3);
+        y[7] = csub(e[3], o3);
     } else {
         // odd P: symmetric direct DFT, y_r and y_{P-r} share the sums
         constexpr int H = (P - 1) / 2;
@@ -78,8 +114,9 @@ __device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P], 
             float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
 #pragma unroll
             for (int q = 1; q <= H; ++q) {
-                const float2 w = W[((r * q) % P) * pstride];
-                const float cs = w.x, sn = -w.y;
+                const int t = (r * q) % P;
+                const float cs = rot_cos(P, t <= H ? t : P - t);
+                const float sn = t <= H ? rot_sin(P, t) : -rot_sin(P, P - t);
                 const float2 a = cadd(v[q], v[P - q]);
                 const float2 b = csub(v[q], v[P - q]);
                 A.x = fmaf(a.x, cs, A.x); A.y = fmaf(a.y, cs, A.y);
@@ -97,104 +134,167 @@ __device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P], 
 }
 
 // One Stockham stage of radix P over C vectors of length n; Ns = product of the
-// radices of earlier stages. Output in natural order after the last stage.
-template <int P, bool INV>
+// radices of earlier stages. Output in natural order after the last stage. A work
+// item is one butterfly position b for CT layers: its index arithmetic and twiddles
+// are shared by the layers. The first stage (Ns = 1) has no twiddles.
+constexpr int CT = 2;
+
+template <int P, bool INV, bool FIRST>
 __device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y, int n, int C, int Ns,
                             const float2* __restrict__ W) {
     const int nb = n / P;
     const int tstride = n / (Ns * P);
+    const int ncg = (C + CT - 1) / CT;
+    const Div dnb = mkdiv(nb), dns = mkdiv(Ns);
+    for (int w = threadIdx.x; w < ncg * nb; w += blockDim.x) {
+        const int cg = quo(w, dnb);
+        const int b = w - cg * nb;
+        const int k = FIRST ? 0 : b - quo(b, dns) * Ns;
+        float2 tw[P];
+        if (!FIRST) {
+            const int kt = k * tstride;
+#pragma unroll
+            for (int r = 1; r < P; ++r) tw[r] = W[r * kt];
+        }
+#pragma unroll
+        for (int t = 0; t < CT; ++t) {
+            const int c = cg * CT + t;
+            if (c >= C) break;
+            const float2* x = X + (size_t)c * n + b;
+            float2 v[P];
+#pragma unroll
+            for (int r = 0; r < P; ++r) v[r] = (FIRST || r == 0) ? x[r * nb] : twmul<INV>(x[r * nb], tw[r]);
+            float2 y[P];
+            dft_small<P, INV>(v, y);
+            float2* yo = Y + (size_t)c * n + (b - k) * P + k;
+#pragma unroll
+            for (int r = 0; r < P; ++r) yo[r * Ns] = y[r];
+        }
+    }
+}
+
+// Twiddles of a prime stage that is not the first one, applied in place:
+// x[c n + b + r nb] *= W^(r k tstride), k = b mod Ns.
+template <bool INV>
+__device__ void twiddle_pass(float2* __restrict__ X, int n, int C, int Ns, int p, const float2* __restrict__ W) {
+    const int nb = n / p;
+    const int tstride = n / (Ns * p);
     const Div dnb = mkdiv(nb), dns = mkdiv(Ns);
     for (int w = threadIdx.x; w < C * nb; w += blockDim.x) {
         const int c = quo(w, dnb);
         const int b = w - c * nb;
         const int k = b - quo(b, dns) * Ns;
-        const float2* x = X + (size_t)c * n + b;
-        float2 v[P];
-#pragma unroll
-        for (int r = 0; r < P; ++r) {
-            float2 t = x[r * nb];
-            if (r > 0) t = twmul<INV>(t, W[r * k * tstride]);
-            v[r] = t;
-        }
-        float2 y[P];
-        dft_small<P, INV>(v, y, W, nb);
-        float2* yo = Y + (size_t)c * n + (b - k) * P + k;
-#pragma unroll
-        for (int r = 0; r < P; ++r) yo[r * Ns] = y[r];
+        if (k == 0) continue;
+        float2* x = X + (size_t)c * n + b;
+        const int kt = k * tstride;
+        for (int r = 1; r < p; ++r) x[r * nb] = twmul<INV>(x[r * nb], W[r * kt]);
     }
 }
 
-// Stage of a large odd prime radix p: twiddle in place, then the symmetric direct DFT
-//   u_q = x_q + x_{p-q}, v_q = x_q - x_{p-q},  A_r = sum_q u_q cos(2 pi r q / p),
-//   B_r = sum_q v_q sin(2 pi r q / p),  y_r = x_0 + A_r -+ i B_r,  y_{p-r} = x_0 + A_r +- i B_r.
-// Work items are (column, group of GR outputs r) with the column index fastest, so the
-// lanes of a warp share r (the DFT-table reads broadcast) and read consecutive x.
-// Wp is a contiguous copy of exp(-2 pi i t / p), t < p.
-constexpr int GR = 8;
+// Stage of an odd prime radix p > 8 as a symmetric direct DFT in Rader's ordering.
+// With g a primitive root of p and h = (p - 1) / 2, the input pairs {q, p - q} are
+// enumerated as q_b = g^-b and the output pairs {r, p - r} as r_a = g^a (a, b < h);
+// every nonzero residue appears once since g^h = -1. Then r_a q_b = g^(a - b) and
+//   A_a = sum_b (x_qb + x_-qb) cos(2 pi g^(a-b) / p),  B_a = sum_b (x_qb - x_-qb) sin(...)
+//   y_ra = x_0 + A_a -+ i B_a,  y_-ra = x_0 + A_a +- i B_a       (forward / inverse)
+// The weight depends on a - b only: a thread owning the GR outputs a0 .. a0 + GR - 1
+// reads, for GR consecutive b, one window of 2 GR consecutive table entries
+// T[a - b + hpad - 1] (16-byte loads shared by the warp) and does 4 GR FMAs per b.
+// Table block of the prime (float2 units, hpad = h rounded up to GR):
+//   T [2 hpad] | q_b [hpad int32] | r_a [hpad int32]
+constexpr int GR = kPrimeGroup;
 
-template <bool INV>
-__device__ void stage_generic(float2* __restrict__ X, float2* __restrict__ Y, float2* __restrict__ Wp, int n, int C,
-                              int Ns, int p, const float2* __restrict__ W) {
-    const int nb = n / p;
-    const int tstride = n / (Ns * p);
-    const int cols = C * nb;
-    const Div dcols = mkdiv(cols), dnb = mkdiv(nb), dns = mkdiv(Ns);
-    for (int t = threadIdx.x; t < p; t += blockDim.x) Wp[t] = W[t * nb];
-    for (int w = threadIdx.x; w < C * n; w += blockDim.x) {
-        const int r = quo(w, dcols);
-        const int col = w - r * cols;
-        const int c = quo(col, dnb);
-        const int b = col - c * nb;
-        const int k = b - quo(b, dns) * Ns;
-        if (r > 0 && k > 0) {
-            float2* xp = X + (size_t)c * n + b + r * nb;
-            *xp = twmul<INV>(*xp, W[r * k * tstride]);
+__host__ __device__ inline int prime_hpad(int p) { return ((p - 1) / 2 + GR - 1) / GR * GR; }
+
+template <bool TAIL>
+__device__ __forceinline__ void prime_block(float (&ar)[GR], float (&ai)[GR], float (&br)[GR], float (&bi)[GR],
+                                            const float2* __restrict__ x, int nb, int n,
+                                            const float2* __restrict__ T, const int* __restrict__ qb, int h, int B0,
+                                            int tbase) {
+    float2 wv[2 * GR];
+    const float4* t4 = reinterpret_cast<const float4*>(T + tbase);
+#pragma unroll
+    for (int e = 0; e < GR; ++e) {
+        const float4 f = t4[e];
+        wv[2 * e] = make_float2(f.x, f.y);
+        wv[2 * e + 1] = make_float2(f.z, f.w);
+    }
+    int qv[GR];
+    const int4* q4 = reinterpret_cast<const int4*>(qb + B0);
+#pragma unroll
+    for (int e = 0; e < GR / 4; ++e) {
+        const int4 qq = q4[e];
+        qv[4 * e] = qq.x;
+        qv[4 * e + 1] = qq.y;
+        qv[4 * e + 2] = qq.z;
+        qv[4 * e + 3] = qq.w;
+    }
+#pragma unroll
+    for (int s = 0; s < GR; ++s) {
+        float2 u = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f);
+        if (!TAIL || B0 + s < h) {
+            const int qn = qv[s] * nb;
+            const float2 xq = x[qn], xm = x[n - qn];
+            u = cadd(xq, xm);
+            v = csub(xq, xm);
+        }
+#pragma unroll
+        for (int i = 0; i < GR; ++i) {
+            const float2 wt = wv[i - s + GR - 1];
+            ar[i] = fmaf(u.x, wt.x, ar[i]);
+            ai[i] = fmaf(u.y, wt.x, ai[i]);
+            br[i] = fmaf(v.x, wt.y, br[i]);
+            bi[i] = fmaf(v.y, wt.y, bi[i]);
         }
     }
-    __syncthreads();
+}
+
+template <bool INV>
+__device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y, int n, int C, int Ns, int p,
+                            const float2* __restrict__ G) {
+    const int nb = n / p;
     const int h = (p - 1) / 2;
-    const int ngroups = (h + GR) / GR;          // r in [0, h]
-    for (int w = threadIdx.x; w < cols * ngroups; w += blockDim.x) {
-        const int g = quo(w, dcols);
-        const int col = w - g * cols;
-        const int r0 = g * GR;
+    const int hpad = prime_hpad(p);
+    const float2* T = G;
+    const int* qb = reinterpret_cast<const int*>(G + 2 * hpad);
+    const int* ra = qb + hpad;
+    const int cols = C * nb;
+    const Div dnb = mkdiv(nb), dns = mkdiv(Ns), dcols = mkdiv(cols);
+    // y_0 = sum of the column
+    for (int col = threadIdx.x; col < cols; col += blockDim.x) {
         const int c = quo(col, dnb);
         const int b = col - c * nb;
         const int k = b - quo(b, dns) * Ns;
         const float2* x = X + (size_t)c * n + b;
-        const float2 x0 = x[0];
+        float2 s0 = x[0], s1 = make_float2(0.f, 0.f);
+        for (int q = 1; q + 1 < p; q += 2) {
+            s0 = cadd(s0, x[q * nb]);
+            s1 = cadd(s1, x[(q + 1) * nb]);
+        }
+        Y[(size_t)c * n + (b - k) * p + k] = cadd(s0, s1);
+    }
+    const int ng = hpad / GR;
+    for (int w = threadIdx.x; w < cols * ng; w += blockDim.x) {
+        const int g = quo(w, dcols);
+        const int col = w - g * cols;
+        const int c = quo(col, dnb);
+        const int b = col - c * nb;
+        const int k = b - quo(b, dns) * Ns;
+        const float2* x = X + (size_t)c * n + b;
+        const int a0 = g * GR;
         float ar[GR], ai[GR], br[GR], bi[GR];
-        int idx[GR];
 #pragma unroll
-        for (int i = 0; i < GR; ++i) {
-            ar[i] = ai[i] = br[i] = bi[i] = 0.f;
-            idx[i] = 0;
-        }
-        for (int q = 1; q <= h; ++q) {
-            const float2 xq = x[q * nb], xm = x[(p - q) * nb];
-            const float ur = xq.x + xm.x, ui = xq.y + xm.y;
-            const float vr = xq.x - xm.x, vi = xq.y - xm.y;
-#pragma unroll
-            for (int i = 0; i < GR; ++i) {
-                idx[i] += r0 + i;
-                if (idx[i] >= p) idx[i] -= p;
-                const float2 wv = Wp[idx[i]];
-                const float cs = wv.x, sn = -wv.y;
-                ar[i] = fmaf(ur, cs, ar[i]);
-                ai[i] = fmaf(ui, cs, ai[i]);
-                br[i] = fmaf(vr, sn, br[i]);
-                bi[i] = fmaf(vi, sn, bi[i]);
-            }
-        }
+        for (int i = 0; i < GR; ++i) ar[i] = ai[i] = br[i] = bi[i] = 0.f;
+        int B0 = 0;
+        for (; B0 + GR <= h; B0 += GR) prime_block<false>(ar, ai, br, bi, x, nb, n, T, qb, h, B0, a0 - B0 + hpad - GR);
+        if (B0 < h) prime_block<true>(ar, ai, br, bi, x, nb, n, T, qb, h, B0, a0 - B0 + hpad - GR);
+        const float2 x0 = x[0];
         float2* yo = Y + (size_t)c * n + (b - k) * p + k;
 #pragma unroll
         for (int i = 0; i < GR; ++i) {
-            const int r = r0 + i;
-            if (r > h) break;
-            if (r == 0) {
-                yo[0] = make_float2(x0.x + ar[0], x0.y + ai[0]);
-                continue;
-            }
+            const int a = a0 + i;
+            if (a >= h) break;
+            const int r = ra[a];
             float2 yr, ypr;
             if (!INV) {
                 yr = make_float2(x0.x + ar[i] + bi[i], x0.y + ai[i] - br[i]);
@@ -209,19 +309,37 @@ __device__ void stage_generic(float2* __restrict__ X, float2* __restrict__ Y, fl
     }
 }
 
-// Runs all stages; returns the buffer holding the result.
+// Runs all stages; returns the buffer holding the result. G: the ring's prime tables.
 template <bool INV>
-__device__ float2* run_fft(float2* X, float2* Y, float2* Wp, int n, int C, const RingDesc& rd, const float2* W) {
+__device__ float2* run_fft(float2* X, float2* Y, int n, int C, const RingDesc& rd, const float2* W, const float2* G) {
     int Ns = 1;
     for (int s = 0; s < rd.nfac; ++s) {
         const int p = rd.fac[s];
-        switch (p) {
-            case 2: stage_small<2, INV>(X, Y, n, C, Ns, W); break;
-            case 3: stage_small<3, INV>(X, Y, n, C, Ns, W); break;
-            case 4: stage_small<4, INV>(X, Y, n, C, Ns, W); break;
-            case 5: stage_small<5, INV>(X, Y, n, C, Ns, W); break;
-            case 7: stage_small<7, INV>(X, Y, n, C, Ns, W); break;
-            default: stage_generic<INV>(X, Y, Wp, n, C, Ns, p, W); break;
+        if (p > 8) {
+            if (Ns > 1) {
+                twiddle_pass<INV>(X, n, C, Ns, p, W);
+                __syncthreads();
+            }
+            stage_prime<INV>(X, Y, n, C, Ns, p, G);
+            G += 3 * prime_hpad(p);
+        } else if (Ns == 1) {
+            switch (p) {
+                case 2: stage_small<2, INV, true>(X, Y, n, C, Ns, W); break;
+                case 3: stage_small<3, INV, true>(X, Y, n, C, Ns, W); break;
+                case 4: stage_small<4, INV, true>(X, Y, n, C, Ns, W); break;
+                case 5: stage_small<5, INV, true>(X, Y, n, C, Ns, W); break;
+                case 7: stage_small<7, INV, true>(X, Y, n, C, Ns, W); break;
+                default: stage_small<8, INV, true>(X, Y, n, C, Ns, W); break;
+            }
+        } else {
+            switch (p) {
+                case 2: stage_small<2, INV, false>(X, Y, n, C, Ns, W); break;
+                case 3: stage_small<3, INV, false>(X, Y, n, C, Ns, W); break;
+                case 4: stage_small<4, INV, false>(X, Y, n, C, Ns, W); break;
+                case 5: stage_small<5, INV, false>(X, Y, n, C, Ns, W); break;
+                case 7: stage_small<7, INV, false>(X, Y, n, C, Ns, W); break;
+                default: stage_small<8, INV, false>(X, Y, n, C, Ns, W); break;
+            }
         }
         __syncthreads();
         float2* t = X; X = Y; Y = t;
@@ -333,10 +451,10 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
         }
     }
 }
-// shared memory: W (n twiddles) | Wp (n, per-stage DFT table) | X (C n) | Y (C n)
+// shared memory: W (n twiddles, padded to even) | G (prime tables) | X (C n) | Y (C n)
 
 // grid -> Fourier scratch (E/O combinations weighted by the solid angle)
-__global__ void __launch_bounds__(512, 2) fft_analysis_kernel(const RingDesc* __restrict__ rings,
+__global__ void __launch_bounds__(256, 2) fft_analysis_kernel(const RingDesc* __restrict__ rings,
                                                            const float2* __restrict__ twiddle,
                                                            const float* __restrict__ grid, int64_t ldg,
                                                            float2* __restrict__ four, int K, const TcImage img) {
@@ -348,13 +466,13 @@ __global__ void __launch_bounds__(512, 2) fft_analysis_kernel(const RingDesc* __
     const int n = rd.n;
     const Div dn = mkdiv(n), dC = mkdiv(C);
     float2* W = sm;
-    float2* Wp = sm + smem_tw_len(n);
-    float2* X = Wp + rd.wp_len;
+    float2* G = sm + smem_tw_len(n);
+    float2* X = G + rd.gen_len;
     float2* Y = X + (size_t)C * n;
-    load_twiddles(W, twiddle + rd.tw_off, n);
+    load_twiddles(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
     load_rings(X, grid, ldg, rd.off_north, rd.off_south, k0, C, n, dn);
     __syncthreads();
-    const float2* Z = run_fft<false>(X, Y, Wp, n, C, rd, W);
+    const float2* Z = run_fft<false>(X, Y, n, C, rd, W, G);
     const float half_domega = 0.5f * rd.domega;
     const int nm = rd.mt + 1;
     if (img.base != nullptr) {
@@ -444,7 +562,7 @@ __global__ void __launch_bounds__(512, 2) fft_analysis_kernel(const RingDesc* __
 }
 
 // Fourier scratch -> grid
-__global__ void __launch_bounds__(512, 2) fft_synthesis_kernel(const RingDesc* __restrict__ rings,
+__global__ void __launch_bounds__(256, 2) fft_synthesis_kernel(const RingDesc* __restrict__ rings,
                                                             const float2* __restrict__ twiddle,
                                                             const float2* __restrict__ four, float* __restrict__ grid,
                                                             int64_t ldg, int K, int unscale, int add) {
@@ -456,10 +574,10 @@ __global__ void __launch_bounds__(512, 2) fft_synthesis_kernel(const RingDesc* _
     const int n = rd.n;
     const Div dn = mkdiv(n), dC = mkdiv(C);
     float2* W = sm;
-    float2* Wp = sm + smem_tw_len(n);
-    float2* X = Wp + rd.wp_len;
+    float2* G = sm + smem_tw_len(n);
+    float2* X = G + rd.gen_len;
     float2* Y = X + (size_t)C * n;
-    load_twiddles(W, twiddle + rd.tw_off, n);
+    load_twiddles(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
     const float scale = unscale ? rd.coslat_inv : 1.0f;
     const int nhalf = n / 2;   // highest source frequency
     for (int w = threadIdx.x; w < C * (nhalf + 1); w += blockDim.x) {
@@ -482,13 +600,13 @@ __global__ void __launch_bounds__(512, 2) fft_synthesis_kernel(const RingDesc* _
         }
     }
     __syncthreads();
-    const float2* z = run_fft<true>(X, Y, Wp, n, C, rd, W);
+    const float2* z = run_fft<true>(X, Y, n, C, rd, W, G);
     store_rings(grid, ldg, rd.off_north, rd.off_south, k0, C, n, dn, z, add);
 }
 
 }  // namespace
 
-static int fft_threads(const Plan&) { return 512; }
+static int fft_threads(const Plan&) { return 256; }
 
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, bool to_image) {
     dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);

@@ -12,6 +12,7 @@
 namespace sht {
 
 constexpr int kMaxFactors = 24;      // radices per ring FFT (n <= 2^24)
+constexpr int kPrimeGroup = 8;       // outputs per thread of a prime FFT stage
 
 // Per-ring real-FFT description, indexed by the northern ring j (0-based).
 // The southern mirror ring has the same length.
@@ -20,11 +21,11 @@ struct RingDesc {
     int32_t mt;           // mmax_truncation (0-based highest order kept)
     int32_t nfac;         // number of Stockham stages
     int32_t chunk;        // layers per CTA in the FFT kernels
-    int32_t wp_len;       // shared-memory entries of the per-stage DFT table (even, >= largest radix)
+    int32_t gen_len;      // float2 entries of the prime-stage tables after the twiddles (even)
     int64_t off_north;    // first grid point of the northern ring
     int64_t off_south;    // first grid point of the southern ring
     int64_t gofs;         // first Fourier-scratch row (m = 0) of this ring
-    int64_t tw_off;       // offset of this ring's twiddle table (n entries)
+    int64_t tw_off;       // offset of this ring's twiddles ((n + 1) & ~1 entries) and prime tables
     float domega;         // solid angle w_j 2pi / n_j
     float coslat_inv;     // 1 / cos(latitude)
     int32_t fac[kMaxFactors];

@@ -86,7 +86,9 @@ void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
     if (n % 2 == 1) x[n / 2] = 0.0;
 }
 
-// Prime factorisation into Stockham radices: 4s first, then 2, 3, 5, 7, larger primes.
+// Prime factorisation into Stockham radices, in stage order: primes above 8 first
+// (largest first; the first stage needs no twiddles), then 7, 5, 3, then the power of
+// two as radix-8 stages with one radix-4 or radix-2 (or two radix-4) for the rest.
 int factorize(int n, int32_t* fac) {
     std::vector<int> f;
     int m = n;
@@ -96,15 +98,72 @@ int factorize(int n, int32_t* fac) {
             m /= p;
         }
     if (m > 1) f.push_back(m);
-    const int twos = (int)std::count(f.begin(), f.end(), 2);
     std::vector<int> out;
-    for (int i = 0; i < twos / 2; ++i) out.push_back(4);
-    if (twos % 2) out.push_back(2);
-    for (int q : f)
-        if (q != 2) out.push_back(q);
+    for (auto it = f.rbegin(); it != f.rend(); ++it)
+        if (*it > 8) out.push_back(*it);
+    for (int q : {7, 5, 3})
+        for (int x : f)
+            if (x == q) out.push_back(q);
+    int twos = (int)std::count(f.begin(), f.end(), 2);
+    if (twos % 3 == 1 && twos >= 4) {
+        out.push_back(4);
+        out.push_back(4);
+        twos -= 4;
+    }
+    for (; twos >= 3; twos -= 3) out.push_back(8);
+    if (twos == 2) out.push_back(4);
+    if (twos == 1) out.push_back(2);
     if ((int)out.size() > kMaxFactors) return -1;
     for (size_t i = 0; i < out.size(); ++i) fac[i] = out[i];
     return (int)out.size();
+}
+
+// Table block of a prime stage p > 8 (layout and use in sht_fft.cu, stage_prime):
+// T[e] = (cos, sin)(2 pi g^(e - hpad + 1) / p) for e < 2 hpad, q_b = g^-b, r_a = g^a.
+static int primitive_root(int p) {
+    std::vector<int> qs;
+    int m = p - 1;
+    for (int d = 2; d * d <= m; ++d)
+        if (m % d == 0) {
+            qs.push_back(d);
+            while (m % d == 0) m /= d;
+        }
+    if (m > 1) qs.push_back(m);
+    auto pw = [p](int64_t b, int64_t e) {
+        int64_t r = 1;
+        b %= p;
+        for (; e > 0; e >>= 1, b = b * b % p)
+            if (e & 1) r = r * b % p;
+        return r;
+    };
+    for (int g = 2; g < p; ++g) {
+        bool ok = true;
+        for (int q : qs) ok = ok && pw(g, (p - 1) / q) != 1;
+        if (ok) return g;
+    }
+    return 1;
+}
+
+static void prime_table(int p, std::vector<float2>& out) {
+    const int h = (p - 1) / 2, hpad = (h + kPrimeGroup - 1) / kPrimeGroup * kPrimeGroup;
+    const int g = primitive_root(p);
+    std::vector<int64_t> gp(p - 1);           // g^t mod p, t < p - 1
+    gp[0] = 1;
+    for (int t = 1; t < p - 1; ++t) gp[t] = gp[t - 1] * g % p;
+    auto gpow = [&](int64_t t) { return gp[((t % (p - 1)) + (p - 1)) % (p - 1)]; };
+    for (int e = 0; e < 2 * hpad; ++e) {
+        const double a = 2.0 * M_PI * (double)gpow(e - hpad + 1) / p;
+        out.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+    }
+    std::vector<int32_t> idx(2 * hpad, 0);    // q_b | r_a
+    for (int b = 0; b < h; ++b) idx[b] = (int32_t)gpow(-b);
+    for (int a = 0; a < h; ++a) idx[hpad + a] = (int32_t)gpow(a);
+    for (int e = 0; e < hpad; ++e) {
+        float2 v;
+        std::memcpy(&v.x, &idx[2 * e], 4);
+        std::memcpy(&v.y, &idx[2 * e + 1], 4);
+        out.push_back(v);
+    }
 }
 
 int shortcut_mt(int kind, int nlon, double latd) {
@@ -285,14 +344,15 @@ int build_plan(Plan& p) {
             const double a = -2.0 * M_PI * t / r.n;
             tw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
         }
+        if (r.n % 2) tw.push_back(make_float2(0.f, 0.f));
+        for (int s = 0; s < r.nfac; ++s)
+            if (r.fac[s] > 8) prime_table(r.fac[s], tw);
+        r.gen_len = (int32_t)((int64_t)tw.size() - r.tw_off - ((r.n + 1) & ~1));
         r.domega = (float)(p.weights[j] * (2.0 * M_PI / r.n));                  // quadrature_weights.jl:48-49
         r.coslat_inv = (float)(1.0 / std::cos(p.latd[j] * M_PI / 180.0));       // spectral_transform.jl:150-151
-        // shared memory of the FFT kernels: twiddles (n), the per-stage DFT table of the
-        // largest prime (<= n/4 + 1 for these grids) and two buffers of chunk x n complex
-        int pmax = 2;
-        for (int s = 0; s < r.nfac; ++s) pmax = std::max(pmax, (int)r.fac[s]);
-        r.wp_len = (pmax + 1) & ~1;
-        const int tw_bytes = (((r.n + 1) & ~1) + r.wp_len) * 8;
+        // shared memory of the FFT kernels: twiddles, prime tables and two buffers of
+        // chunk x n complex
+        const int tw_bytes = (((r.n + 1) & ~1) + r.gen_len) * 8;
         int chunk = 1;
         while (chunk * 2 <= 32 && tw_bytes + 2 * (chunk * 2) * r.n * 8 <= smem_budget) chunk *= 2;
         r.chunk = chunk;
