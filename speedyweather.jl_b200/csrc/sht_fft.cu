@@ -454,13 +454,14 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
 // shared memory: W (n twiddles, padded to even) | G (prime tables) | X (C n) | Y (C n)
 
 // grid -> Fourier scratch (E/O combinations weighted by the solid angle)
-__global__ void __launch_bounds__(256, 2) fft_analysis_kernel(const RingDesc* __restrict__ rings,
+__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kernel(const int2* __restrict__ items, const RingDesc* __restrict__ rings,
                                                            const float2* __restrict__ twiddle,
                                                            const float* __restrict__ grid, int64_t ldg,
                                                            float2* __restrict__ four, int K, const TcImage img) {
     extern __shared__ float2 sm[];
-    const RingDesc& rd = rings[blockIdx.x];
-    const int k0 = blockIdx.y * rd.chunk;
+    const int2 item = items[blockIdx.x];
+    const RingDesc& rd = rings[item.x];
+    const int k0 = item.y * rd.chunk;
     if (k0 >= K) return;
     const int C = min(rd.chunk, K - k0);
     const int n = rd.n;
@@ -482,7 +483,7 @@ __global__ void __launch_bounds__(256, 2) fft_analysis_kernel(const RingDesc* __
         const int cbeg = 2 * k0, cend = 2 * (k0 + C);
         const int gbeg = cbeg / 8, ngr = (cend + 7) / 8 - gbeg;
         const Div dngr = mkdiv(ngr);
-        const int j = blockIdx.x;
+        const int j = item.x;
         for (int w = threadIdx.x; w < ngr * nm; w += blockDim.x) {
             const int m = quo(w, dngr);
             const int g = gbeg + (w - m * ngr);
@@ -562,13 +563,14 @@ __global__ void __launch_bounds__(256, 2) fft_analysis_kernel(const RingDesc* __
 }
 
 // Fourier scratch -> grid
-__global__ void __launch_bounds__(256, 2) fft_synthesis_kernel(const RingDesc* __restrict__ rings,
+__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kernel(const int2* __restrict__ items, const RingDesc* __restrict__ rings,
                                                             const float2* __restrict__ twiddle,
                                                             const float2* __restrict__ four, float* __restrict__ grid,
                                                             int64_t ldg, int K, int unscale, int add) {
     extern __shared__ float2 sm[];
-    const RingDesc& rd = rings[blockIdx.x];
-    const int k0 = blockIdx.y * rd.chunk;
+    const int2 item = items[blockIdx.x];
+    const RingDesc& rd = rings[item.x];
+    const int k0 = item.y * rd.chunk;
     if (k0 >= K) return;
     const int C = min(rd.chunk, K - k0);
     const int n = rd.n;
@@ -580,23 +582,37 @@ __global__ void __launch_bounds__(256, 2) fft_synthesis_kernel(const RingDesc* _
     load_twiddles(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
     const float scale = unscale ? rd.coslat_inv : 1.0f;
     const int nhalf = n / 2;   // highest source frequency
-    for (int w = threadIdx.x; w < C * (nhalf + 1); w += blockDim.x) {
-        const int m = quo(w, dC);
-        const int c = w - m * C;
-        float2 gn = make_float2(0.f, 0.f), gs = make_float2(0.f, 0.f);
-        if (m <= rd.mt) {
-            const int64_t row = (rd.gofs + m) * 2;
-            const float2 e = four[row * K + k0 + c];
-            const float2 o = four[(row + 1) * K + k0 + c];
-            gn = make_float2(scale * (e.x + o.x), scale * (e.y + o.y));
-            gs = make_float2(scale * (e.x - o.x), scale * (e.y - o.y));
+    // four (order, layer) items per thread in flight: the scratch reads are the latency
+    const int tot = C * (nhalf + 1);
+    for (int w0 = threadIdx.x; w0 < tot; w0 += 4 * blockDim.x) {
+        float2 e[4], o[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int w = w0 + u * blockDim.x;
+            const int m = quo(w, dC);
+            const int c = w - m * C;
+            e[u] = o[u] = make_float2(0.f, 0.f);
+            if (w < tot && m <= rd.mt) {
+                const int64_t row = (rd.gofs + m) * 2;
+                e[u] = four[row * K + k0 + c];
+                o[u] = four[(row + 1) * K + k0 + c];
+            }
         }
-        const bool selfconj = (m == 0) || (2 * m == n);
-        if (selfconj) {
-            X[(size_t)c * n + m] = make_float2(gn.x, gs.x);
-        } else {
-            X[(size_t)c * n + m] = make_float2(gn.x - gs.y, gn.y + gs.x);
-            X[(size_t)c * n + (n - m)] = make_float2(gn.x + gs.y, gs.x - gn.y);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int w = w0 + u * blockDim.x;
+            if (w >= tot) break;
+            const int m = quo(w, dC);
+            const int c = w - m * C;
+            const float2 gn = make_float2(scale * (e[u].x + o[u].x), scale * (e[u].y + o[u].y));
+            const float2 gs = make_float2(scale * (e[u].x - o[u].x), scale * (e[u].y - o[u].y));
+            const bool selfconj = (m == 0) || (2 * m == n);
+            if (selfconj) {
+                X[(size_t)c * n + m] = make_float2(gn.x, gs.x);
+            } else {
+                X[(size_t)c * n + m] = make_float2(gn.x - gs.y, gn.y + gs.x);
+                X[(size_t)c * n + (n - m)] = make_float2(gn.x + gs.y, gs.x - gn.y);
+            }
         }
     }
     __syncthreads();
@@ -606,19 +622,19 @@ __global__ void __launch_bounds__(256, 2) fft_synthesis_kernel(const RingDesc* _
 
 }  // namespace
 
-static int fft_threads(const Plan&) { return 256; }
+static int fft_threads(const Plan&) { return kFftThreads; }
 
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, bool to_image) {
-    dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);
+    const dim3 g(p.n_fft_items);
     const TcImage none{};
-    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_rings, p.d_twiddle, grid, ldg, p.d_four, K,
+    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, p.d_rings, p.d_twiddle, grid, ldg, p.d_four, K,
                                                               (to_image || p.tc) ? p.ana_img : none);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags, cudaStream_t s) {
-    dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);
-    fft_synthesis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_rings, p.d_twiddle, p.d_four, grid, ldg, K,
+    const dim3 g(p.n_fft_items);
+    fft_synthesis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, p.d_rings, p.d_twiddle, p.d_four, grid, ldg, K,
                                                                (flags & SHT_UNSCALE_COSLAT) ? 1 : 0,
                                                                (flags & SHT_ADD) ? 1 : 0);
     return cudaGetLastError();
@@ -637,9 +653,9 @@ namespace sht {
 // (used by the static-scratch analysis entry point).
 cudaError_t launch_fft_analysis_to(const Plan& p, const float* grid, int64_t ldg, int K, float2* scratch,
                                    cudaStream_t s) {
-    dim3 g(p.nh, (K + p.min_chunk - 1) / p.min_chunk);
+    const dim3 g(p.n_fft_items);
     const TcImage none{};
-    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_rings, p.d_twiddle, grid, ldg, scratch, K, none);
+    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, p.d_rings, p.d_twiddle, grid, ldg, scratch, K, none);
     return cudaGetLastError();
 }
 }  // namespace sht

@@ -14,6 +14,18 @@ namespace sht {
 constexpr int kMaxFactors = 24;      // radices per ring FFT (n <= 2^24)
 constexpr int kPrimeGroup = 8;       // outputs per thread of a prime FFT stage
 
+// Launch shape of the FFT kernels: threads per CTA, CTAs per SM, and the shared
+// memory one CTA may use (which bounds the layers per CTA).
+#ifndef SHT_FFT_THREADS
+#define SHT_FFT_THREADS 256
+#endif
+#ifndef SHT_FFT_CTAS_PER_SM
+#define SHT_FFT_CTAS_PER_SM 2
+#endif
+constexpr int kFftThreads = SHT_FFT_THREADS;
+constexpr int kFftCtasPerSm = SHT_FFT_CTAS_PER_SM;
+constexpr int kFftSmemBudget = (227 * 1024) / SHT_FFT_CTAS_PER_SM - 1024;
+
 // Per-ring real-FFT description, indexed by the northern ring j (0-based).
 // The southern mirror ring has the same length.
 struct RingDesc {
@@ -98,8 +110,9 @@ struct Plan {
     void* tc = nullptr;                 // tensor-core Legendre state (sht_legendre_tc.cu)
     TcImage ana_img;                    // analysis data image written by the FFT (tensor-core plans)
     int smem_fft = 0;                   // dynamic shared memory of the FFT kernels
-    int max_chunk_groups = 0;           // grid.y upper bound factor for FFT launch
     int min_chunk = 1;
+    int2* d_fft_items = nullptr;        // FFT work list: (ring, layer chunk), costliest first
+    int n_fft_items = 0;
 };
 
 enum GradIdx {

@@ -197,7 +197,7 @@ void release(Plan& p) {
     tc_release(p);
     void* ptrs[] = {p.d_rings, p.d_twiddle, p.d_lam, p.d_lam_off, p.d_j0, p.d_rows, p.d_lm_off, p.d_syn_items,
                     p.d_ana_items, p.d_mt, p.d_gofs, p.d_grad, p.d_l_of, p.d_m_of, p.d_eig, p.d_eig_inv, p.d_four,
-                    p.d_err};
+                    p.d_err, p.d_fft_items};
     for (void* q : ptrs)
         if (q) cudaFree(q);
 }
@@ -325,7 +325,7 @@ int build_plan(Plan& p) {
     std::vector<RingDesc> rings(nh);
     std::vector<float2> tw;
     int64_t gofs = 0;
-    const int smem_budget = 113 * 1024;     // two CTAs per SM
+    const int smem_budget = kFftSmemBudget;
     int max_smem = 0;
     p.min_chunk = 1 << 30;
     for (int j = 0; j < nh; ++j) {
@@ -361,6 +361,27 @@ int build_plan(Plan& p) {
     }
     p.scratch_rows = gofs;
     p.smem_fft = max_smem;
+
+    // --- FFT work list: one CTA per (ring, chunk of layers), issued costliest first so
+    // that the last wave holds the cheapest CTAs. Cost per layer: FMAs of the prime
+    // stages (2 n hpad each) plus ~3 n per small-radix stage and ~4 n of copies.
+    std::vector<std::pair<double, int2>> fitems;
+    const int kmax = std::max(1, d.nlayers);
+    for (int j = 0; j < nh; ++j) {
+        const RingDesc& r = rings[j];
+        double per_layer = 4.0 * r.n;
+        for (int s2 = 0; s2 < r.nfac; ++s2)
+            per_layer += r.fac[s2] > 8 ? 2.0 * r.n * ((r.fac[s2] - 1) / 2 + kPrimeGroup - 1) / kPrimeGroup * kPrimeGroup
+                                       : 3.0 * r.n;
+        for (int ci = 0; ci * r.chunk < kmax; ++ci) {
+            const int c = std::min(r.chunk, kmax - ci * r.chunk);
+            fitems.push_back({c * per_layer, make_int2(j, ci)});
+        }
+    }
+    std::stable_sort(fitems.begin(), fitems.end(),
+                     [](const std::pair<double, int2>& a, const std::pair<double, int2>& b) { return a.first > b.first; });
+    std::vector<int2> fft_items;
+    for (auto& f : fitems) fft_items.push_back(f.second);
 
     // --- work lists of the Legendre kernels (64-row tiles, heavy orders first) ---
     std::vector<LegItem> syn, ana;
@@ -416,6 +437,7 @@ int build_plan(Plan& p) {
     UP(p.d_lm_off, p.lm_off);
     UP(p.d_syn_items, syn);
     UP(p.d_ana_items, ana);
+    UP(p.d_fft_items, fft_items);
     UP(p.d_mt, p.mt);
     UP(p.d_grad, grad);
     UP(p.d_l_of, l_of);
@@ -428,6 +450,7 @@ int build_plan(Plan& p) {
     if ((e = upload(&p.d_gofs, gofs_v, tb)) != cudaSuccess) return cuda_fail(e, "sht_plan_create upload gofs");
     p.n_syn_items = (int)syn.size();
     p.n_ana_items = (int)ana.size();
+    p.n_fft_items = (int)fft_items.size();
     p.table_bytes = tb;
 
     p.four_elems = p.scratch_rows * 2 * std::max(1, d.nlayers);
