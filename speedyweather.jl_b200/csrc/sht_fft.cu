@@ -140,7 +140,7 @@ __device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P]) 
 constexpr int CT = 2;
 
 template <int P, bool INV, bool FIRST>
-__device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y, int n, int C, int Ns,
+__device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y, int n, int ldx, int C, int Ns,
                             const float2* __restrict__ W) {
     const int nb = n / P;
     const int tstride = n / (Ns * P);
@@ -160,13 +160,13 @@ __device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y
         for (int t = 0; t < CT; ++t) {
             const int c = cg * CT + t;
             if (c >= C) break;
-            const float2* x = X + (size_t)c * n + b;
+            const float2* x = X + c * ldx + b;
             float2 v[P];
 #pragma unroll
             for (int r = 0; r < P; ++r) v[r] = (FIRST || r == 0) ? x[r * nb] : twmul<INV>(x[r * nb], tw[r]);
             float2 y[P];
             dft_small<P, INV>(v, y);
-            float2* yo = Y + (size_t)c * n + (b - k) * P + k;
+            float2* yo = Y + c * ldx + (b - k) * P + k;
 #pragma unroll
             for (int r = 0; r < P; ++r) yo[r * Ns] = y[r];
         }
@@ -176,7 +176,7 @@ __device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y
 // Twiddles of a prime stage that is not the first one, applied in place:
 // x[c n + b + r nb] *= W^(r k tstride), k = b mod Ns.
 template <bool INV>
-__device__ void twiddle_pass(float2* __restrict__ X, int n, int C, int Ns, int p, const float2* __restrict__ W) {
+__device__ void twiddle_pass(float2* __restrict__ X, int n, int ldx, int C, int Ns, int p, const float2* __restrict__ W) {
     const int nb = n / p;
     const int tstride = n / (Ns * p);
     const Div dnb = mkdiv(nb), dns = mkdiv(Ns);
@@ -185,7 +185,7 @@ __device__ void twiddle_pass(float2* __restrict__ X, int n, int C, int Ns, int p
         const int b = w - c * nb;
         const int k = b - quo(b, dns) * Ns;
         if (k == 0) continue;
-        float2* x = X + (size_t)c * n + b;
+        float2* x = X + c * ldx + b;
         const int kt = k * tstride;
         for (int r = 1; r < p; ++r) x[r * nb] = twmul<INV>(x[r * nb], W[r * kt]);
     }
@@ -250,7 +250,7 @@ __device__ __forceinline__ void prime_block(float (&ar)[GR], float (&ai)[GR], fl
 }
 
 template <bool INV>
-__device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y, int n, int C, int Ns, int p,
+__device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y, int n, int ldx, int C, int Ns, int p,
                             const float2* __restrict__ G) {
     const int nb = n / p;
     const int h = (p - 1) / 2;
@@ -265,13 +265,13 @@ __device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y
         const int c = quo(col, dnb);
         const int b = col - c * nb;
         const int k = b - quo(b, dns) * Ns;
-        const float2* x = X + (size_t)c * n + b;
+        const float2* x = X + c * ldx + b;
         float2 s0 = x[0], s1 = make_float2(0.f, 0.f);
         for (int q = 1; q + 1 < p; q += 2) {
             s0 = cadd(s0, x[q * nb]);
             s1 = cadd(s1, x[(q + 1) * nb]);
         }
-        Y[(size_t)c * n + (b - k) * p + k] = cadd(s0, s1);
+        Y[c * ldx + (b - k) * p + k] = cadd(s0, s1);
     }
     const int ng = hpad / GR;
     for (int w = threadIdx.x; w < cols * ng; w += blockDim.x) {
@@ -280,7 +280,7 @@ __device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y
         const int c = quo(col, dnb);
         const int b = col - c * nb;
         const int k = b - quo(b, dns) * Ns;
-        const float2* x = X + (size_t)c * n + b;
+        const float2* x = X + c * ldx + b;
         const int a0 = g * GR;
         float ar[GR], ai[GR], br[GR], bi[GR];
 #pragma unroll
@@ -289,7 +289,7 @@ __device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y
         for (; B0 + GR <= h; B0 += GR) prime_block<false>(ar, ai, br, bi, x, nb, n, T, qb, h, B0, a0 - B0 + hpad - GR);
         if (B0 < h) prime_block<true>(ar, ai, br, bi, x, nb, n, T, qb, h, B0, a0 - B0 + hpad - GR);
         const float2 x0 = x[0];
-        float2* yo = Y + (size_t)c * n + (b - k) * p + k;
+        float2* yo = Y + c * ldx + (b - k) * p + k;
 #pragma unroll
         for (int i = 0; i < GR; ++i) {
             const int a = a0 + i;
@@ -311,34 +311,35 @@ __device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y
 
 // Runs all stages; returns the buffer holding the result. G: the ring's prime tables.
 template <bool INV>
-__device__ float2* run_fft(float2* X, float2* Y, int n, int C, const RingDesc& rd, const float2* W, const float2* G) {
+__device__ float2* run_fft(float2* X, float2* Y, int n, int ldx, int C, const RingDesc& rd, const float2* W,
+                           const float2* G) {
     int Ns = 1;
     for (int s = 0; s < rd.nfac; ++s) {
         const int p = rd.fac[s];
         if (p > 8) {
             if (Ns > 1) {
-                twiddle_pass<INV>(X, n, C, Ns, p, W);
+                twiddle_pass<INV>(X, n, ldx, C, Ns, p, W);
                 __syncthreads();
             }
-            stage_prime<INV>(X, Y, n, C, Ns, p, G);
+            stage_prime<INV>(X, Y, n, ldx, C, Ns, p, G);
             G += 3 * prime_hpad(p);
         } else if (Ns == 1) {
             switch (p) {
-                case 2: stage_small<2, INV, true>(X, Y, n, C, Ns, W); break;
-                case 3: stage_small<3, INV, true>(X, Y, n, C, Ns, W); break;
-                case 4: stage_small<4, INV, true>(X, Y, n, C, Ns, W); break;
-                case 5: stage_small<5, INV, true>(X, Y, n, C, Ns, W); break;
-                case 7: stage_small<7, INV, true>(X, Y, n, C, Ns, W); break;
-                default: stage_small<8, INV, true>(X, Y, n, C, Ns, W); break;
+                case 2: stage_small<2, INV, true>(X, Y, n, ldx, C, Ns, W); break;
+                case 3: stage_small<3, INV, true>(X, Y, n, ldx, C, Ns, W); break;
+                case 4: stage_small<4, INV, true>(X, Y, n, ldx, C, Ns, W); break;
+                case 5: stage_small<5, INV, true>(X, Y, n, ldx, C, Ns, W); break;
+                case 7: stage_small<7, INV, true>(X, Y, n, ldx, C, Ns, W); break;
+                default: stage_small<8, INV, true>(X, Y, n, ldx, C, Ns, W); break;
             }
         } else {
             switch (p) {
-                case 2: stage_small<2, INV, false>(X, Y, n, C, Ns, W); break;
-                case 3: stage_small<3, INV, false>(X, Y, n, C, Ns, W); break;
-                case 4: stage_small<4, INV, false>(X, Y, n, C, Ns, W); break;
-                case 5: stage_small<5, INV, false>(X, Y, n, C, Ns, W); break;
-                case 7: stage_small<7, INV, false>(X, Y, n, C, Ns, W); break;
-                default: stage_small<8, INV, false>(X, Y, n, C, Ns, W); break;
+                case 2: stage_small<2, INV, false>(X, Y, n, ldx, C, Ns, W); break;
+                case 3: stage_small<3, INV, false>(X, Y, n, ldx, C, Ns, W); break;
+                case 4: stage_small<4, INV, false>(X, Y, n, ldx, C, Ns, W); break;
+                case 5: stage_small<5, INV, false>(X, Y, n, ldx, C, Ns, W); break;
+                case 7: stage_small<7, INV, false>(X, Y, n, ldx, C, Ns, W); break;
+                default: stage_small<8, INV, false>(X, Y, n, ldx, C, Ns, W); break;
             }
         }
         __syncthreads();
@@ -369,11 +370,11 @@ __device__ __forceinline__ void load_twiddles(float2* W, const float2* __restric
     }
 }
 
-// X[c n + i] = (north ring value, south ring value) of layer k0 + c. Rings start at
+// X[c ldx + i] = (north ring value, south ring value) of layer k0 + c. Rings start at
 // multiples of 4 points on these grids, so 16-byte vectors are used when the layer
 // stride and base allow.
 __device__ __forceinline__ void load_rings(float2* X, const float* __restrict__ grid, int64_t ldg, int64_t off_n,
-                                           int64_t off_s, int k0, int C, int n, Div dn) {
+                                           int64_t off_s, int k0, int C, int n, int ldx, Div dn) {
     const bool vec = ((ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(grid) & 15) == 0) && ((off_n & 3) == 0) &&
                      ((off_s & 3) == 0) && ((n & 3) == 0);
     if (vec) {
@@ -396,7 +397,7 @@ __device__ __forceinline__ void load_rings(float2* X, const float* __restrict__ 
                 const int w = w0 + u * blockDim.x;
                 if (w < tot) {
                     const int c = quo(w, dn4), i4 = w - c * n4;
-                    float4* x = reinterpret_cast<float4*>(X + (size_t)c * n + 4 * i4);
+                    float4* x = reinterpret_cast<float4*>(X + c * ldx + 4 * i4);
                     x[0] = make_float4(a[u].x, b[u].x, a[u].y, b[u].y);
                     x[1] = make_float4(a[u].z, b[u].z, a[u].w, b[u].w);
                 }
@@ -408,13 +409,13 @@ __device__ __forceinline__ void load_rings(float2* X, const float* __restrict__ 
         const int c = quo(w, dn);
         const int i = w - c * n;
         const float* g = grid + (int64_t)(k0 + c) * ldg;
-        X[w] = make_float2(g[off_n + i], g[off_s + i]);
+        X[c * ldx + i] = make_float2(g[off_n + i], g[off_s + i]);
     }
 }
 
 // grid rings of layer k0 + c (=, or += with add) <- (Re z, Im z)
 __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ldg, int64_t off_n, int64_t off_s, int k0,
-                                            int C, int n, Div dn, const float2* z, int add) {
+                                            int C, int n, int ldx, Div dn, const float2* z, int add) {
     const bool vec = ((ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(grid) & 15) == 0) && ((off_n & 3) == 0) &&
                      ((off_s & 3) == 0) && ((n & 3) == 0);
     if (vec) {
@@ -422,7 +423,7 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
         const Div dn4 = mkdiv(n4);
         for (int w = threadIdx.x; w < tot; w += blockDim.x) {
             const int c = quo(w, dn4), i4 = w - c * n4;
-            const float4* zz = reinterpret_cast<const float4*>(z + (size_t)c * n + 4 * i4);
+            const float4* zz = reinterpret_cast<const float4*>(z + c * ldx + 4 * i4);
             const float4 p0 = zz[0], p1 = zz[1];
             float4 a = make_float4(p0.x, p0.z, p1.x, p1.z), b = make_float4(p0.y, p0.w, p1.y, p1.w);
             float4* gn = reinterpret_cast<float4*>(grid + (int64_t)(k0 + c) * ldg + off_n) + i4;
@@ -441,7 +442,7 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
         const int c = quo(w, dn);
         const int i = w - c * n;
         float* g = grid + (int64_t)(k0 + c) * ldg;
-        const float2 v = z[w];
+        const float2 v = z[c * ldx + i];
         if (add) {
             g[off_n + i] += v.x;
             g[off_s + i] += v.y;
@@ -451,7 +452,8 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
         }
     }
 }
-// shared memory: W (n twiddles, padded to even) | G (prime tables) | X (C n) | Y (C n)
+// shared memory: W (n twiddles, padded to even) | G (prime tables) | X (C ldx) | Y (C ldx);
+// ldx >= n is the padded layer stride
 
 // grid -> Fourier scratch (E/O combinations weighted by the solid angle)
 __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kernel(const int2* __restrict__ items, const RingDesc* __restrict__ rings,
@@ -465,15 +467,16 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
     if (k0 >= K) return;
     const int C = min(rd.chunk, K - k0);
     const int n = rd.n;
-    const Div dn = mkdiv(n), dC = mkdiv(C);
+    const int ldx = rd.ldx;
+    const Div dn = mkdiv(n);
     float2* W = sm;
     float2* G = sm + smem_tw_len(n);
     float2* X = G + rd.gen_len;
-    float2* Y = X + (size_t)C * n;
+    float2* Y = X + C * ldx;
     load_twiddles(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
-    load_rings(X, grid, ldg, rd.off_north, rd.off_south, k0, C, n, dn);
+    load_rings(X, grid, ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn);
     __syncthreads();
-    const float2* Z = run_fft<false>(X, Y, n, C, rd, W, G);
+    const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G);
     const float half_domega = 0.5f * rd.domega;
     const int nm = rd.mt + 1;
     if (img.base != nullptr) {
@@ -496,8 +499,8 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
                 ev[q] = ov[q] = 0.f;
                 if (!have[q]) continue;
                 const int cl = c / 2 - k0;
-                const float2 a = Z[(size_t)cl * n + m];
-                const float2 b = Z[(size_t)cl * n + (m == 0 ? 0 : n - m)];
+                const float2 a = Z[cl * ldx + m];
+                const float2 b = Z[cl * ldx + (m == 0 ? 0 : n - m)];
                 const float2 fn = make_float2(a.x + b.x, a.y - b.y);
                 const float2 fs = make_float2(a.y + b.y, b.x - a.x);
                 if (c % 2 == 0) {
@@ -546,11 +549,14 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
         }
         return;
     }
+    // layer fastest across the lanes: a warp writes whole runs of C layers of a scratch
+    // row; the padded layer stride of shared memory keeps the lanes' reads in distinct banks
+    const Div dC = mkdiv(C);
     for (int w = threadIdx.x; w < C * nm; w += blockDim.x) {
         const int m = quo(w, dC);
         const int c = w - m * C;
-        const float2 a = Z[(size_t)c * n + m];
-        const float2 b = Z[(size_t)c * n + (m == 0 ? 0 : n - m)];
+        const float2 a = Z[c * ldx + m];
+        const float2 b = Z[c * ldx + (m == 0 ? 0 : n - m)];
         // F_N = (a + conj b)/2, F_S = (a - conj b)/(2i)
         const float2 fn = make_float2(a.x + b.x, a.y - b.y);
         const float2 fs = make_float2(a.y + b.y, b.x - a.x);
@@ -574,16 +580,19 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kern
     if (k0 >= K) return;
     const int C = min(rd.chunk, K - k0);
     const int n = rd.n;
-    const Div dn = mkdiv(n), dC = mkdiv(C);
+    const int ldx = rd.ldx;
+    const Div dn = mkdiv(n);
     float2* W = sm;
     float2* G = sm + smem_tw_len(n);
     float2* X = G + rd.gen_len;
-    float2* Y = X + (size_t)C * n;
+    float2* Y = X + C * ldx;
     load_twiddles(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
     const float scale = unscale ? rd.coslat_inv : 1.0f;
     const int nhalf = n / 2;   // highest source frequency
-    // four (order, layer) items per thread in flight: the scratch reads are the latency
+    // layer fastest across the lanes (a warp reads whole runs of C layers of a scratch
+    // row), four items per thread in flight: the scratch reads are the latency
     const int tot = C * (nhalf + 1);
+    const Div dC = mkdiv(C);
     for (int w0 = threadIdx.x; w0 < tot; w0 += 4 * blockDim.x) {
         float2 e[4], o[4];
 #pragma unroll
@@ -608,16 +617,16 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kern
             const float2 gs = make_float2(scale * (e[u].x - o[u].x), scale * (e[u].y - o[u].y));
             const bool selfconj = (m == 0) || (2 * m == n);
             if (selfconj) {
-                X[(size_t)c * n + m] = make_float2(gn.x, gs.x);
+                X[c * ldx + m] = make_float2(gn.x, gs.x);
             } else {
-                X[(size_t)c * n + m] = make_float2(gn.x - gs.y, gn.y + gs.x);
-                X[(size_t)c * n + (n - m)] = make_float2(gn.x + gs.y, gs.x - gn.y);
+                X[c * ldx + m] = make_float2(gn.x - gs.y, gn.y + gs.x);
+                X[c * ldx + (n - m)] = make_float2(gn.x + gs.y, gs.x - gn.y);
             }
         }
     }
     __syncthreads();
-    const float2* z = run_fft<true>(X, Y, n, C, rd, W, G);
-    store_rings(grid, ldg, rd.off_north, rd.off_south, k0, C, n, dn, z, add);
+    const float2* z = run_fft<true>(X, Y, n, ldx, C, rd, W, G);
+    store_rings(grid, ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn, z, add);
 }
 
 }  // namespace

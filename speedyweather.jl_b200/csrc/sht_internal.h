@@ -34,6 +34,7 @@ struct RingDesc {
     int32_t nfac;         // number of Stockham stages
     int32_t chunk;        // layers per CTA in the FFT kernels
     int32_t gen_len;      // float2 entries of the prime-stage tables after the twiddles (even)
+    int32_t ldx;          // layer stride of the FFT's shared-memory buffers (>= n, even)
     int64_t off_north;    // first grid point of the northern ring
     int64_t off_south;    // first grid point of the southern ring
     int64_t gofs;         // first Fourier-scratch row (m = 0) of this ring

@@ -353,11 +353,19 @@ int build_plan(Plan& p) {
         // shared memory of the FFT kernels: twiddles, prime tables and two buffers of
         // chunk x n complex
         const int tw_bytes = (((r.n + 1) & ~1) + r.gen_len) * 8;
+        // layer stride ldx = n + pad with ldx = 16 / chunk (mod 16) in float2 units (2 for
+        // chunks of 8 or more): the chunk's layers of one order then fall in distinct
+        // shared-memory banks when the lanes run over the layers
+        auto stride = [&](int c) {
+            const int want = c >= 8 ? 2 : 16 / c;
+            return r.n + (((want - r.n) % 16) + 16) % 16;
+        };
         int chunk = 1;
-        while (chunk * 2 <= 32 && tw_bytes + 2 * (chunk * 2) * r.n * 8 <= smem_budget) chunk *= 2;
+        while (chunk * 2 <= 32 && tw_bytes + 2 * (chunk * 2) * stride(chunk * 2) * 8 <= smem_budget) chunk *= 2;
         r.chunk = chunk;
+        r.ldx = stride(chunk);
         p.min_chunk = std::min(p.min_chunk, chunk);
-        max_smem = std::max(max_smem, tw_bytes + 2 * chunk * r.n * 8);
+        max_smem = std::max(max_smem, tw_bytes + 2 * chunk * r.ldx * 8);
     }
     p.scratch_rows = gofs;
     p.smem_fft = max_smem;
