@@ -433,62 +433,62 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // ---------------------------------------------------------------- synthesis data image
 // coefficients [k][lm] complex FP32 -> per (m, p, kt, piece) K-major SWIZZLE_128B tiles
 // of nmax rows (columns c = 2k + re/im) x 64 parity rows (128 B).
-__device__ __forceinline__ void split_bf16(float x, uint16_t* out, int npieces) {
-    float r = x;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        if (q >= npieces) break;
-        const __nv_bfloat16 h = __float2bfloat16_rn(r);
-        out[q] = __bfloat16_as_ushort(h);
-        r -= __bfloat162float(h);
-    }
-}
 
-// One CTA per (m, 64-row block kt): the block's 128 consecutive packed coefficients
-// (both parities) of up to 32 layers at a time are staged in shared memory with
-// coalesced loads, then every thread assembles 16-byte chunks (8 rows of one parity
-// and one real column) of the swizzled tiles.
-constexpr int SYN_KCHUNK = 32;
+// Synthesis data image. One thread per (order m, 64-row block kt, 8-row chunk ib8,
+// layer k): it loads the 16 packed coefficients of its 8 rows (both parities, four
+// 16-byte loads; the 8 threads of a layer read 512 consecutive bytes) and writes, per
+// parity, real/imaginary column and piece, one whole 16-byte chunk of the swizzled
+// K-major tile: rows 8 ib8 .. 8 ib8 + 7 of column c = 2 k + ri. CTA: 8 chunks x 32
+// layers. Rows past the order's last coefficient are written as zeros.
+template <int NPB>
 __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const float2* __restrict__ coeffs,
                                                         int64_t ldc, int K) {
-    __shared__ float2 sc[SYN_KCHUNK][2 * BLK + 1];
     const int m = blockIdx.x;
     const int kt = blockIdx.y;
     if (kt >= t.nkt[m]) return;
-    const int64_t lmo = t.lm_off[m];
-    const int lmrem = t.lmax - m - 2 * BLK * kt;      // coefficients of this order left from the block start
-    uint8_t* img = reinterpret_cast<uint8_t*>(const_cast<uint16_t*>(t.syn_img));
-    const int64_t tile0 = t.syn_tile_base[m] + kt, tile1 = t.syn_tile_base[m] + t.nkt[m] + kt;
-    for (int k0 = 0; k0 < K; k0 += SYN_KCHUNK) {
-        const int kc = min(SYN_KCHUNK, K - k0);
-        __syncthreads();
-        for (int w = threadIdx.x; w < kc * 2 * BLK; w += blockDim.x) {
-            const int kk = w / (2 * BLK), q = w % (2 * BLK);
-            sc[kk][q] = q < lmrem ? coeffs[(int64_t)(k0 + kk) * ldc + lmo + 2 * BLK * kt + q] : make_float2(0.f, 0.f);
-        }
-        __syncthreads();
-        // items: (layer kk, 8-row chunk ib8, parity, re/im)
-        for (int w = threadIdx.x; w < kc * 32; w += blockDim.x) {
-            const int ib8 = w & 7, par = (w >> 3) & 1, ri = (w >> 4) & 1, kk = w >> 5;
-            const int c = 2 * (k0 + kk) + ri;
-            uint16_t pc[3][8];
+    const int ib8 = threadIdx.x & 7;
+    const int k = blockIdx.z * 32 + (threadIdx.x >> 3);
+    if (k >= K) return;
+    const int lmrem = t.lmax - m - 2 * BLK * kt - 16 * ib8;   // packed coefficients left from this chunk
+    const float2* src = coeffs + (int64_t)k * ldc + t.lm_off[m] + 2 * BLK * kt + 16 * ib8;
+    float2 v[16];
+    const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && lmrem >= 16;
+    if (vec) {
 #pragma unroll
-            for (int ii = 0; ii < 8; ++ii) {
-                const float2 v = sc[kk][2 * (8 * ib8 + ii) + par];
-                uint16_t tmp[3];
-                split_bf16(ri ? v.y : v.x, tmp, t.npb);
-                for (int q = 0; q < t.npb; ++q) pc[q][ii] = tmp[q];
+        for (int q = 0; q < 8; ++q) {
+            const float4 f = __ldg(reinterpret_cast<const float4*>(src) + q);
+            v[2 * q] = make_float2(f.x, f.y);
+            v[2 * q + 1] = make_float2(f.z, f.w);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = q < lmrem ? __ldg(src + q) : make_float2(0.f, 0.f);
+    }
+    uint8_t* img = reinterpret_cast<uint8_t*>(const_cast<uint16_t*>(t.syn_img));
+#pragma unroll
+    for (int par = 0; par < 2; ++par) {
+        const int64_t tile = t.syn_tile_base[m] + (int64_t)par * t.nkt[m] + kt;
+#pragma unroll
+        for (int ri = 0; ri < 2; ++ri) {
+            const int c = 2 * k + ri;
+            uint32_t w[NPB][4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                float r0 = ri ? v[2 * (2 * h) + par].y : v[2 * (2 * h) + par].x;
+                float r1 = ri ? v[2 * (2 * h + 1) + par].y : v[2 * (2 * h + 1) + par].x;
+#pragma unroll
+                for (int q = 0; q < NPB; ++q) {
+                    const __nv_bfloat16 h0 = __float2bfloat16_rn(r0), h1 = __float2bfloat16_rn(r1);
+                    w[q][h] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+                    r0 -= __bfloat162float(h0);
+                    r1 -= __bfloat162float(h1);
+                }
             }
             const int64_t off = (int64_t)(c / 8) * 1024 + (c % 8) * 128 + ((ib8 ^ (c % 8)) * 16);
-            const int64_t tile = par ? tile1 : tile0;
-            for (int q = 0; q < t.npb; ++q) {
-                uint4 u;
-                u.x = (uint32_t)pc[q][0] | ((uint32_t)pc[q][1] << 16);
-                u.y = (uint32_t)pc[q][2] | ((uint32_t)pc[q][3] << 16);
-                u.z = (uint32_t)pc[q][4] | ((uint32_t)pc[q][5] << 16);
-                u.w = (uint32_t)pc[q][6] | ((uint32_t)pc[q][7] << 16);
-                *reinterpret_cast<uint4*>(img + (tile * t.npb + q) * t.syn_tile_bytes + off) = u;
-            }
+#pragma unroll
+            for (int q = 0; q < NPB; ++q)
+                *reinterpret_cast<uint4*>(img + (tile * NPB + q) * t.syn_tile_bytes + off) =
+                    make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
         }
     }
 }
@@ -738,7 +738,11 @@ static uint32_t tmem_cols_for(int n) {
 cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, int64_t ldc, int K, cudaStream_t st) {
     const TcState& s = *static_cast<const TcState*>(p.tc);
     const TcDev t = make_dev(p);
-    syn_image_kernel<<<dim3(p.mmax, (p.rows[0] + BLK - 1) / BLK), 256, 0, st>>>(t, coeffs, ldc, K);
+    const dim3 ig(p.mmax, (p.rows[0] + BLK - 1) / BLK, (K + 31) / 32);
+    if (s.npb == 2)
+        syn_image_kernel<2><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
+    else
+        syn_image_kernel<3><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || s.n_syn_items == 0) return e;
     const int ncols = 2 * K;
