@@ -452,6 +452,35 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
         }
     }
 }
+// Writes the 16-bit pieces of 8 reals as one 16-byte chunk per piece (pieces a tile
+// apart); a partial chunk (mask of valid reals) is written element by element.
+template <int NP>
+__device__ __forceinline__ void put_pieces(uint8_t* dst, int64_t piece_stride, const float (&v)[8], unsigned mask) {
+    uint32_t w[NP][4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+        float r0 = v[2 * h], r1 = v[2 * h + 1];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            const __nv_bfloat16 h0 = __float2bfloat16_rn(r0), h1 = __float2bfloat16_rn(r1);
+            w[q][h] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+            r0 -= __bfloat162float(h0);
+            r1 -= __bfloat162float(h1);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+        uint8_t* d = dst + q * piece_stride;
+        if (mask == 0xffu) {
+            *reinterpret_cast<uint4*>(d) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                if (mask >> e & 1u) reinterpret_cast<uint16_t*>(d)[e] = (uint16_t)(w[q][e / 2] >> (16 * (e & 1)));
+        }
+    }
+}
+
 // shared memory: W (n twiddles, padded to even) | G (prime tables) | X (C ldx) | Y (C ldx);
 // ldx >= n is the padded layer stride
 
@@ -490,61 +519,38 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
         for (int w = threadIdx.x; w < ngr * nm; w += blockDim.x) {
             const int m = quo(w, dngr);
             const int g = gbeg + (w - m * ngr);
+            const int mm = m == 0 ? 0 : n - m;
+            // layers 4 g .. 4 g + 3: real columns 8 g + 2 t (re) and 8 g + 2 t + 1 (im)
             float ev[8], ov[8];
-            bool have[8];
+            unsigned mask = 0;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int c = 8 * g + q;
-                have[q] = c >= cbeg && c < cend;
-                ev[q] = ov[q] = 0.f;
-                if (!have[q]) continue;
-                const int cl = c / 2 - k0;
-                const float2 a = Z[cl * ldx + m];
-                const float2 b = Z[cl * ldx + (m == 0 ? 0 : n - m)];
-                const float2 fn = make_float2(a.x + b.x, a.y - b.y);
-                const float2 fs = make_float2(a.y + b.y, b.x - a.x);
-                if (c % 2 == 0) {
-                    ev[q] = half_domega * (fn.x + fs.x);
-                    ov[q] = half_domega * (fn.x - fs.x);
-                } else {
-                    ev[q] = half_domega * (fn.y + fs.y);
-                    ov[q] = half_domega * (fn.y - fs.y);
+            for (int t = 0; t < 4; ++t) {
+                const int kl = 4 * g + t - k0;
+                ev[2 * t] = ev[2 * t + 1] = ov[2 * t] = ov[2 * t + 1] = 0.f;
+                if (kl >= 0 && kl < C) {
+                    const float2 a = Z[kl * ldx + m];
+                    const float2 b = Z[kl * ldx + mm];
+                    const float2 fn = make_float2(a.x + b.x, a.y - b.y);
+                    const float2 fs = make_float2(a.y + b.y, b.x - a.x);
+                    ev[2 * t] = half_domega * (fn.x + fs.x);
+                    ev[2 * t + 1] = half_domega * (fn.y + fs.y);
+                    ov[2 * t] = half_domega * (fn.x - fs.x);
+                    ov[2 * t + 1] = half_domega * (fn.y - fs.y);
+                    mask |= 3u << (2 * t);
                 }
             }
-            const bool full = have[0] && have[7];
             const int jj = j - img.j0[m];
             const int r = jj % 64;
             // column block of 64 (8 KB apart), 8-row group, row, swizzled 16-byte chunk
             const int64_t row_off = (int64_t)(g / 8) * 8192 + (r / 8) * 1024 + (r % 8) * 128 + (((g % 8) ^ (r % 8)) * 16);
-            for (int par = 0; par < 2; ++par) {
-                const float* v = par ? ov : ev;
-                const int64_t tile = img.tile_base[m] + (int64_t)par * img.njt[m] + jj / 64;
-                uint16_t pc[3][8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    float x = v[q];
-#pragma unroll
-                    for (int pp = 0; pp < 3; ++pp) {
-                        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-                        pc[pp][q] = __bfloat16_as_ushort(h);
-                        x -= __bfloat162float(h);
-                    }
-                }
-                for (int pp = 0; pp < img.npieces; ++pp) {
-                    uint8_t* dst = reinterpret_cast<uint8_t*>(img.base) + (tile * img.npieces + pp) * img.tile_bytes + row_off;
-                    if (full) {
-                        uint4 u;
-                        u.x = (uint32_t)pc[pp][0] | ((uint32_t)pc[pp][1] << 16);
-                        u.y = (uint32_t)pc[pp][2] | ((uint32_t)pc[pp][3] << 16);
-                        u.z = (uint32_t)pc[pp][4] | ((uint32_t)pc[pp][5] << 16);
-                        u.w = (uint32_t)pc[pp][6] | ((uint32_t)pc[pp][7] << 16);
-                        *reinterpret_cast<uint4*>(dst) = u;
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 8; ++q)
-                            if (have[q]) reinterpret_cast<uint16_t*>(dst)[q] = pc[pp][q];
-                    }
-                }
+            uint8_t* base = reinterpret_cast<uint8_t*>(img.base) + row_off;
+            const int64_t t0 = img.tile_base[m] + jj / 64;
+            if (img.npieces == 2) {
+                put_pieces<2>(base + t0 * 2 * img.tile_bytes, img.tile_bytes, ev, mask);
+                put_pieces<2>(base + (t0 + img.njt[m]) * 2 * img.tile_bytes, img.tile_bytes, ov, mask);
+            } else {
+                put_pieces<3>(base + t0 * 3 * img.tile_bytes, img.tile_bytes, ev, mask);
+                put_pieces<3>(base + (t0 + img.njt[m]) * 3 * img.tile_bytes, img.tile_bytes, ov, mask);
             }
         }
         return;
