@@ -351,23 +351,18 @@ __device__ float2* run_fft(float2* X, float2* Y, int n, int ldx, int C, const Ri
 
 __device__ __forceinline__ int smem_tw_len(int n) { return (n + 1) & ~1; }
 
-// Global <-> shared copies with four independent accesses in flight per thread (the
-// CTA is latency-bound otherwise: one ring of C layers is loaded, transformed and
-// stored in sequence).
-__device__ __forceinline__ void load_twiddles(float2* W, const float2* __restrict__ tw, int n) {
-    for (int t0 = threadIdx.x; t0 < n; t0 += 4 * blockDim.x) {
-        float2 v[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int t = t0 + u * blockDim.x;
-            if (t < n) v[u] = __ldg(tw + t);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int t = t0 + u * blockDim.x;
-            if (t < n) W[t] = v[u];
-        }
-    }
+// 16-byte asynchronous global -> shared copies (no register staging): a CTA issues
+// all copies of its inputs at once, so its load phase is one memory round trip.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+// twiddles and prime tables (len float2, even; source 16-byte aligned)
+__device__ __forceinline__ void copy_twiddles_async(float2* W, const float2* __restrict__ tw, int len) {
+    for (int t = threadIdx.x; t < len / 2; t += blockDim.x) cp_async16(W + 2 * t, tw + 2 * t);
 }
 
 // X[c ldx + i] = (north ring value, south ring value) of layer k0 + c. Rings start at
@@ -502,8 +497,41 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
     float2* G = sm + smem_tw_len(n);
     float2* X = G + rd.gen_len;
     float2* Y = X + C * ldx;
-    load_twiddles(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
-    load_rings(X, grid, ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn);
+    // Ring values of the C layers land raw in Y (layer c at Y + c ldx: n northern, then
+    // n southern floats) by asynchronous copies issued together with the twiddles,
+    // then are interleaved into X. Unaligned layouts take the register path.
+    const bool avec = ((ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(grid) & 15) == 0) &&
+                      ((rd.off_north & 3) == 0) && ((rd.off_south & 3) == 0) && ((n & 3) == 0);
+    copy_twiddles_async(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
+    const int n4 = n >> 2;
+    if (avec) {
+        const Div d2n4 = mkdiv(2 * n4);
+        for (int w = threadIdx.x; w < C * 2 * n4; w += blockDim.x) {
+            const int c = quo(w, d2n4);
+            const int r = w - c * 2 * n4;
+            const int hs = r >= n4 ? 1 : 0;
+            const int i4 = r - hs * n4;
+            const float* src = grid + (int64_t)(k0 + c) * ldg + (hs ? rd.off_south : rd.off_north) + 4 * i4;
+            cp_async16(reinterpret_cast<float*>(Y + c * ldx) + hs * n + 4 * i4, src);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (avec) {
+        const Div dn4 = mkdiv(n4);
+        for (int w = threadIdx.x; w < C * n4; w += blockDim.x) {
+            const int c = quo(w, dn4);
+            const int i4 = w - c * n4;
+            const float* raw = reinterpret_cast<const float*>(Y + c * ldx);
+            const float4 a = reinterpret_cast<const float4*>(raw)[i4];
+            const float4 b = reinterpret_cast<const float4*>(raw + n)[i4];
+            float4* x = reinterpret_cast<float4*>(X + c * ldx + 4 * i4);
+            x[0] = make_float4(a.x, b.x, a.y, b.y);
+            x[1] = make_float4(a.z, b.z, a.w, b.w);
+        }
+    } else {
+        load_rings(X, grid, ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn);
+    }
     __syncthreads();
     const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G);
     const float half_domega = 0.5f * rd.domega;
@@ -592,7 +620,24 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kern
     float2* G = sm + smem_tw_len(n);
     float2* X = G + rd.gen_len;
     float2* Y = X + C * ldx;
-    load_twiddles(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
+    // The scratch rows r = 2 m + eo (m <= mt) of the C layers land in Y as [r][c] by
+    // asynchronous copies issued together with the twiddles (2 (mt + 1) <= ldx). Odd
+    // layer counts or offsets read the scratch directly.
+    const bool svec = ((K & 1) == 0) && ((k0 & 1) == 0) && ((C & 1) == 0) &&
+                      ((reinterpret_cast<uintptr_t>(four) & 15) == 0);
+    copy_twiddles_async(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
+    if (svec) {
+        const int half = C / 2, nrow = 2 * (rd.mt + 1);
+        const Div dh = mkdiv(half);
+        const float2* src0 = four + 2 * rd.gofs * K + k0;
+        for (int w = threadIdx.x; w < nrow * half; w += blockDim.x) {
+            const int r = quo(w, dh);
+            const int h = w - r * half;
+            cp_async16(Y + r * C + 2 * h, src0 + (int64_t)r * K + 2 * h);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
     const float scale = unscale ? rd.coslat_inv : 1.0f;
     const int nhalf = n / 2;   // highest source frequency
     // layer fastest across the lanes (a warp reads whole runs of C layers of a scratch
@@ -608,9 +653,14 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kern
             const int c = w - m * C;
             e[u] = o[u] = make_float2(0.f, 0.f);
             if (w < tot && m <= rd.mt) {
-                const int64_t row = (rd.gofs + m) * 2;
-                e[u] = four[row * K + k0 + c];
-                o[u] = four[(row + 1) * K + k0 + c];
+                if (svec) {
+                    e[u] = Y[2 * m * C + c];
+                    o[u] = Y[(2 * m + 1) * C + c];
+                } else {
+                    const int64_t row = (rd.gofs + m) * 2;
+                    e[u] = four[row * K + k0 + c];
+                    o[u] = four[(row + 1) * K + k0 + c];
+                }
             }
         }
 #pragma unroll

@@ -356,9 +356,11 @@ int build_plan(Plan& p) {
         // layer stride ldx = n + pad with ldx = 16 / chunk (mod 16) in float2 units (2 for
         // chunks of 8 or more): the chunk's layers of one order then fall in distinct
         // shared-memory banks when the lanes run over the layers
+        // (and ldx >= 2 (mt + 1): the synthesis stages the ring's scratch rows in one buffer)
         auto stride = [&](int c) {
             const int want = c >= 8 ? 2 : 16 / c;
-            return r.n + (((want - r.n) % 16) + 16) % 16;
+            const int base = std::max(r.n, 2 * (r.mt + 1));
+            return base + (((want - base) % 16) + 16) % 16;
         };
         int chunk = 1;
         while (chunk * 2 <= 32 && tw_bytes + 2 * (chunk * 2) * stride(chunk * 2) * 8 <= smem_budget) chunk *= 2;
