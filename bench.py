@@ -276,7 +276,7 @@ def run_ours(args):
     field = st.Field.zeros(grid, LAYERS, device=device)
     out = st.LowerTriangularArray.zeros(spec, LAYERS, device=device)
 
-    precisions = [args.precision] if args.precision != "auto" else ["fp32", "bf16x3", "bf16x5"]
+    precisions = [args.precision] if args.precision != "auto" else ["fp32", "bf16x3", "fp16x3", "bf16x5"]
     variants = {}
     transforms = {}
     for prec in precisions:
@@ -415,7 +415,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3", "bf16x5"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3", "fp16x3", "bf16x5"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample-layers", type=int, default=16)

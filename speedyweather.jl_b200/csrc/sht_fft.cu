@@ -19,6 +19,7 @@
 // FFTW's conventions are kept: r2c and c2r are unnormalised and c2r ignores the
 // imaginary parts of the DC and Nyquist bins.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "sht_internal.h"
 
@@ -195,11 +196,15 @@ __device__ void twiddle_pass(float2* __restrict__ X, int n, int ldx, int C, int 
 // With g a primitive root of p and h = (p - 1) / 2, the input pairs {q, p - q} are
 // enumerated as q_b = g^-b and the output pairs {r, p - r} as r_a = g^a (a, b < h);
 // every nonzero residue appears once since g^h = -1. Then r_a q_b = g^(a - b) and
-//   A_a = sum_b (x_qb + x_-qb) cos(2 pi g^(a-b) / p),  B_a = sum_b (x_qb - x_-qb) sin(...)
+//   A_a = sum_b u_b cos(2 pi g^(a-b) / p),  B_a = sum_b v_b sin(...),
+//   u_b = x_qb + x_-qb,  v_b = x_qb - x_-qb,
 //   y_ra = x_0 + A_a -+ i B_a,  y_-ra = x_0 + A_a +- i B_a       (forward / inverse)
 // The weight depends on a - b only: a thread owning the GR outputs a0 .. a0 + GR - 1
 // reads, for GR consecutive b, one window of 2 GR consecutive table entries
 // T[a - b + hpad - 1] (16-byte loads shared by the warp) and does 4 GR FMAs per b.
+// A first pass stores u_b, v_b (and x_0) of every column in Y, [b][column] with the
+// column fastest; the main pass reads them with one 16-byte load per b and writes
+// its outputs into X, which holds the stage's result.
 // Table block of the prime (float2 units, hpad = h rounded up to GR):
 //   T [2 hpad] | q_b [hpad int32] | r_a [hpad int32]
 constexpr int GR = kPrimeGroup;
@@ -208,9 +213,8 @@ __host__ __device__ inline int prime_hpad(int p) { return ((p - 1) / 2 + GR - 1)
 
 template <bool TAIL>
 __device__ __forceinline__ void prime_block(float (&ar)[GR], float (&ai)[GR], float (&br)[GR], float (&bi)[GR],
-                                            const float2* __restrict__ x, int nb, int n,
-                                            const float2* __restrict__ T, const int* __restrict__ qb, int h, int B0,
-                                            int tbase) {
+                                            const float4* __restrict__ uv, int cols, const float2* __restrict__ T,
+                                            int h, int B0, int tbase) {
     float2 wv[2 * GR];
     const float4* t4 = reinterpret_cast<const float4*>(T + tbase);
 #pragma unroll
@@ -219,38 +223,23 @@ __device__ __forceinline__ void prime_block(float (&ar)[GR], float (&ai)[GR], fl
         wv[2 * e] = make_float2(f.x, f.y);
         wv[2 * e + 1] = make_float2(f.z, f.w);
     }
-    int qv[GR];
-    const int4* q4 = reinterpret_cast<const int4*>(qb + B0);
-#pragma unroll
-    for (int e = 0; e < GR / 4; ++e) {
-        const int4 qq = q4[e];
-        qv[4 * e] = qq.x;
-        qv[4 * e + 1] = qq.y;
-        qv[4 * e + 2] = qq.z;
-        qv[4 * e + 3] = qq.w;
-    }
 #pragma unroll
     for (int s = 0; s < GR; ++s) {
-        float2 u = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f);
-        if (!TAIL || B0 + s < h) {
-            const int qn = qv[s] * nb;
-            const float2 xq = x[qn], xm = x[n - qn];
-            u = cadd(xq, xm);
-            v = csub(xq, xm);
-        }
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!TAIL || B0 + s < h) q = uv[(B0 + s) * cols];
 #pragma unroll
         for (int i = 0; i < GR; ++i) {
             const float2 wt = wv[i - s + GR - 1];
-            ar[i] = fmaf(u.x, wt.x, ar[i]);
-            ai[i] = fmaf(u.y, wt.x, ai[i]);
-            br[i] = fmaf(v.x, wt.y, br[i]);
-            bi[i] = fmaf(v.y, wt.y, bi[i]);
+            ar[i] = fmaf(q.x, wt.x, ar[i]);
+            ai[i] = fmaf(q.y, wt.x, ai[i]);
+            br[i] = fmaf(q.z, wt.y, br[i]);
+            bi[i] = fmaf(q.w, wt.y, bi[i]);
         }
     }
 }
 
 template <bool INV>
-__device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y, int n, int ldx, int C, int Ns, int p,
+__device__ void stage_prime(float2* __restrict__ X, float2* __restrict__ Y, int n, int ldx, int C, int Ns, int p,
                             const float2* __restrict__ G) {
     const int nb = n / p;
     const int h = (p - 1) / 2;
@@ -260,18 +249,39 @@ __device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y
     const int* ra = qb + hpad;
     const int cols = C * nb;
     const Div dnb = mkdiv(nb), dns = mkdiv(Ns), dcols = mkdiv(cols);
-    // y_0 = sum of the column
+    float4* UV = reinterpret_cast<float4*>(Y);      // [b < h][column]
+    float2* X0 = Y + 2 * h * cols;                  // [column]; cols (2 h + 1) = C n <= C ldx
+    for (int w = threadIdx.x; w < (h + 1) * cols; w += blockDim.x) {
+        const int b = quo(w, dcols);
+        const int col = w - b * cols;
+        const int c = quo(col, dnb);
+        const float2* x = X + c * ldx + (col - c * nb);
+        if (b < h) {
+            const int qn = qb[b] * nb;
+            const float2 xq = x[qn], xm = x[n - qn];
+            UV[b * cols + col] = make_float4(xq.x + xm.x, xq.y + xm.y, xq.x - xm.x, xq.y - xm.y);
+        } else {
+            X0[col] = x[0];
+        }
+    }
+    __syncthreads();
+    // y_0 = x_0 + sum_b u_b
     for (int col = threadIdx.x; col < cols; col += blockDim.x) {
         const int c = quo(col, dnb);
         const int b = col - c * nb;
         const int k = b - quo(b, dns) * Ns;
-        const float2* x = X + c * ldx + b;
-        float2 s0 = x[0], s1 = make_float2(0.f, 0.f);
-        for (int q = 1; q + 1 < p; q += 2) {
-            s0 = cadd(s0, x[q * nb]);
-            s1 = cadd(s1, x[(q + 1) * nb]);
+        float2 s0 = X0[col], s1 = make_float2(0.f, 0.f);
+        int q = 0;
+        for (; q + 1 < h; q += 2) {
+            const float4 a = UV[q * cols + col], e = UV[(q + 1) * cols + col];
+            s0 = make_float2(s0.x + a.x, s0.y + a.y);
+            s1 = make_float2(s1.x + e.x, s1.y + e.y);
         }
-        Y[c * ldx + (b - k) * p + k] = cadd(s0, s1);
+        if (q < h) {
+            const float4 a = UV[q * cols + col];
+            s0 = make_float2(s0.x + a.x, s0.y + a.y);
+        }
+        X[c * ldx + (b - k) * p + k] = cadd(s0, s1);
     }
     const int ng = hpad / GR;
     for (int w = threadIdx.x; w < cols * ng; w += blockDim.x) {
@@ -280,16 +290,16 @@ __device__ void stage_prime(const float2* __restrict__ X, float2* __restrict__ Y
         const int c = quo(col, dnb);
         const int b = col - c * nb;
         const int k = b - quo(b, dns) * Ns;
-        const float2* x = X + c * ldx + b;
         const int a0 = g * GR;
         float ar[GR], ai[GR], br[GR], bi[GR];
 #pragma unroll
         for (int i = 0; i < GR; ++i) ar[i] = ai[i] = br[i] = bi[i] = 0.f;
+        const float4* uv = UV + col;
         int B0 = 0;
-        for (; B0 + GR <= h; B0 += GR) prime_block<false>(ar, ai, br, bi, x, nb, n, T, qb, h, B0, a0 - B0 + hpad - GR);
-        if (B0 < h) prime_block<true>(ar, ai, br, bi, x, nb, n, T, qb, h, B0, a0 - B0 + hpad - GR);
-        const float2 x0 = x[0];
-        float2* yo = Y + c * ldx + (b - k) * p + k;
+        for (; B0 + GR <= h; B0 += GR) prime_block<false>(ar, ai, br, bi, uv, cols, T, h, B0, a0 - B0 + hpad - GR);
+        if (B0 < h) prime_block<true>(ar, ai, br, bi, uv, cols, T, h, B0, a0 - B0 + hpad - GR);
+        const float2 x0 = X0[col];
+        float2* yo = X + c * ldx + (b - k) * p + k;
 #pragma unroll
         for (int i = 0; i < GR; ++i) {
             const int a = a0 + i;
@@ -321,8 +331,11 @@ __device__ float2* run_fft(float2* X, float2* Y, int n, int ldx, int C, const Ri
                 twiddle_pass<INV>(X, n, ldx, C, Ns, p, W);
                 __syncthreads();
             }
-            stage_prime<INV>(X, Y, n, ldx, C, Ns, p, G);
+            stage_prime<INV>(X, Y, n, ldx, C, Ns, p, G);     // result in X
             G += 3 * prime_hpad(p);
+            __syncthreads();
+            Ns *= p;
+            continue;
         } else if (Ns == 1) {
             switch (p) {
                 case 2: stage_small<2, INV, true>(X, Y, n, ldx, C, Ns, W); break;
@@ -447,9 +460,29 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
         }
     }
 }
-// Writes the 16-bit pieces of 8 reals as one 16-byte chunk per piece (pieces a tile
-// apart); a partial chunk (mask of valid reals) is written element by element.
-template <int NP>
+// Exponent e with |bound| 2^-e < 1 (0 for a zero bound): the power-of-two data scale
+// of fp16 pieces.
+__device__ __forceinline__ int scale_exp(float bound) {
+    int e = 0;
+    if (bound > 0.f) frexpf(bound, &e);
+    return e;
+}
+template <bool F16>
+__device__ __forceinline__ uint32_t piece_bits(float& r) {
+    if (F16) {
+        const __half h = __float2half_rn(r);
+        r -= __half2float(h);
+        return __half_as_ushort(h);
+    }
+    const __nv_bfloat16 h = __float2bfloat16_rn(r);
+    r -= __bfloat162float(h);
+    return __bfloat16_as_ushort(h);
+}
+
+// Writes the 16-bit pieces (bf16 or fp16) of 8 reals as one 16-byte chunk per piece
+// (pieces a tile apart); a partial chunk (mask of valid reals) is written element by
+// element.
+template <int NP, bool F16>
 __device__ __forceinline__ void put_pieces(uint8_t* dst, int64_t piece_stride, const float (&v)[8], unsigned mask) {
     uint32_t w[NP][4];
 #pragma unroll
@@ -457,10 +490,8 @@ __device__ __forceinline__ void put_pieces(uint8_t* dst, int64_t piece_stride, c
         float r0 = v[2 * h], r1 = v[2 * h + 1];
 #pragma unroll
         for (int q = 0; q < NP; ++q) {
-            const __nv_bfloat16 h0 = __float2bfloat16_rn(r0), h1 = __float2bfloat16_rn(r1);
-            w[q][h] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-            r0 -= __bfloat162float(h0);
-            r1 -= __bfloat162float(h1);
+            const uint32_t b0 = piece_bits<F16>(r0);
+            w[q][h] = b0 | (piece_bits<F16>(r1) << 16);
         }
     }
 #pragma unroll
@@ -560,10 +591,13 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
                     const float2 b = Z[kl * ldx + mm];
                     const float2 fn = make_float2(a.x + b.x, a.y - b.y);
                     const float2 fs = make_float2(a.y + b.y, b.x - a.x);
-                    ev[2 * t] = half_domega * (fn.x + fs.x);
-                    ev[2 * t + 1] = half_domega * (fn.y + fs.y);
-                    ov[2 * t] = half_domega * (fn.x - fs.x);
-                    ov[2 * t + 1] = half_domega * (fn.y - fs.y);
+                    // fp16 pieces: the layer's data scale 2^(15 - e_k) folded into the weight
+                    const float hw = img.fp16 ? ldexpf(half_domega, 15 - scale_exp(img.absmax[k0 + kl] * img.absmax_mul))
+                                              : half_domega;
+                    ev[2 * t] = hw * (fn.x + fs.x);
+                    ev[2 * t + 1] = hw * (fn.y + fs.y);
+                    ov[2 * t] = hw * (fn.x - fs.x);
+                    ov[2 * t + 1] = hw * (fn.y - fs.y);
                     mask |= 3u << (2 * t);
                 }
             }
@@ -573,12 +607,15 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
             const int64_t row_off = (int64_t)(g / 8) * 8192 + (r / 8) * 1024 + (r % 8) * 128 + (((g % 8) ^ (r % 8)) * 16);
             uint8_t* base = reinterpret_cast<uint8_t*>(img.base) + row_off;
             const int64_t t0 = img.tile_base[m] + jj / 64;
-            if (img.npieces == 2) {
-                put_pieces<2>(base + t0 * 2 * img.tile_bytes, img.tile_bytes, ev, mask);
-                put_pieces<2>(base + (t0 + img.njt[m]) * 2 * img.tile_bytes, img.tile_bytes, ov, mask);
+            if (img.fp16) {
+                put_pieces<2, true>(base + t0 * 2 * img.tile_bytes, img.tile_bytes, ev, mask);
+                put_pieces<2, true>(base + (t0 + img.njt[m]) * 2 * img.tile_bytes, img.tile_bytes, ov, mask);
+            } else if (img.npieces == 2) {
+                put_pieces<2, false>(base + t0 * 2 * img.tile_bytes, img.tile_bytes, ev, mask);
+                put_pieces<2, false>(base + (t0 + img.njt[m]) * 2 * img.tile_bytes, img.tile_bytes, ov, mask);
             } else {
-                put_pieces<3>(base + t0 * 3 * img.tile_bytes, img.tile_bytes, ev, mask);
-                put_pieces<3>(base + (t0 + img.njt[m]) * 3 * img.tile_bytes, img.tile_bytes, ov, mask);
+                put_pieces<3, false>(base + t0 * 3 * img.tile_bytes, img.tile_bytes, ev, mask);
+                put_pieces<3, false>(base + (t0 + img.njt[m]) * 3 * img.tile_bytes, img.tile_bytes, ov, mask);
             }
         }
         return;
@@ -692,6 +729,10 @@ static int fft_threads(const Plan&) { return kFftThreads; }
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, bool to_image) {
     const dim3 g(p.n_fft_items);
     const TcImage none{};
+    if ((to_image || p.tc) && p.ana_img.fp16) {
+        const cudaError_t e = tc_analysis_scale(p, grid, ldg, K, s);
+        if (e != cudaSuccess) return e;
+    }
     fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, p.d_rings, p.d_twiddle, grid, ldg, p.d_four, K,
                                                               (to_image || p.tc) ? p.ana_img : none);
     return cudaGetLastError();

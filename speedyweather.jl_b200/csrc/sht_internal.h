@@ -61,8 +61,8 @@ struct TcImage {
     int32_t npieces = 0;
     int32_t tile_bytes = 0;             // bytes of one tile
     int32_t fp16 = 0;                   // 0: bf16 pieces, 1: fp16 pieces
-    const float* col_scale = nullptr;   // fp16: per layer scale of the data (device)
-    const float* ring_scale = nullptr;  // fp16: per (m, ring) 1 / scale of the Legendre table
+    const float* absmax = nullptr;      // fp16: per layer max |grid value| of the call (device)
+    float absmax_mul = 0.f;             // fp16: bound of |E|, |O| per unit grid value
 };
 
 struct Plan {
@@ -122,6 +122,7 @@ enum GradIdx {
 };
 
 // ---- launchers (return cudaError_t of the launch) ----------------------------------
+cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s);
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s,
                                 bool to_image = false);
 cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags,

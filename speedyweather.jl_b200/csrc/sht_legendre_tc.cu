@@ -12,6 +12,13 @@
 //   SHT_PREC_BF16X3: Lam in 2 bf16 pieces, data in 2: L0 B0 + L0 B1 + L1 B0
 //   SHT_PREC_BF16X5: Lam in 3 bf16 pieces (from FP64), data in 2:
 //                    L0 B0 + L0 B1 + L1 B0 + L1 B1 + L2 B0
+//   SHT_PREC_FP16X3: as BF16X3 with fp16 pieces (11-bit significands), Lam scaled by
+//                    2^(15 - e_m) per order and the data by 2^(15 - e_k) per layer
+//                    (e from a max-abs reduction of the call's input), so that the
+//                    largest values sit in [2^14, 2^15): both pieces stay normal fp16
+//                    numbers down to 2^-18 of the maximum, and the products stay far
+//                    inside FP32's range. The epilogue multiplies by 2^(e_m + e_k - 30),
+//                    which is exact.
 //
 // Operands in shared memory use the SWIZZLE_128B canonical layouts of tcgen05:
 // * Lam[m][p] is stored [piece][i][j - j0(m)] in global memory; one TMA tensor map
@@ -32,6 +39,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <cmath>
 #include <cstring>
@@ -75,6 +83,11 @@ struct TcDev {
     int64_t syn_tile_bytes;        // one (m, p, kt, piece) synthesis data tile at nmax columns
     int64_t ana_tile_bytes;        // one (m, p, jt, piece) analysis data tile
     int nmax;                      // columns of the data images (multiple of 64)
+    int fp16;                      // 1: fp16 pieces with power-of-two scaling
+    const int32_t* mexp;           // per m: e_m of the Legendre scaling
+    const float* absmax_syn;       // per layer: max |coefficient part| of the synthesis input
+    const float* absmax_ana;       // per layer: max |grid value| of the analysis input
+    float ana_mul;                 // bound of |E|, |O| per unit grid value: 4 pi max_j w_j
 };
 
 struct TcState {
@@ -94,6 +107,10 @@ struct TcState {
     int n_ana_items = 0;
     int max_smem = 0;
     int nsm = 148;                 // SMs of the device (persistent grid)
+    int fp16 = 0;
+    int32_t* d_mexp = nullptr;
+    float* d_absmax = nullptr;     // [2 nlayers]: synthesis, analysis
+    float ana_mul = 0.f;
 };
 
 // ---------------------------------------------------------------- PTX wrappers
@@ -187,6 +204,27 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+constexpr int F16_TOP = 15;        // fp16 data scaled to [2^14, 2^15) of its maximum
+
+// Exponent e with |bound| 2^-e < 1 (0 for a zero bound).
+__device__ __forceinline__ int scale_exp(float bound) {
+    int e = 0;
+    if (bound > 0.f) frexpf(bound, &e);
+    return e;
+}
+// 16-bit pieces of x (bf16 or fp16), x = sum of the pieces to ~8 or ~11 bits each.
+template <bool F16>
+__device__ __forceinline__ uint32_t piece_bits(float& r) {
+    if (F16) {
+        const __half h = __float2half_rn(r);
+        r -= __half2float(h);
+        return __half_as_ushort(h);
+    }
+    const __nv_bfloat16 h = __float2bfloat16_rn(r);
+    r -= __bfloat162float(h);
+    return __bfloat16_as_ushort(h);
+}
+
 // ---------------------------------------------------------------- the GEMM kernel
 // SYN: A = Lam^T (MN-major), B = synthesis image (K-major), D -> Fourier scratch.
 // ANA: A = Lam (K-major), B = analysis image (MN-major), D -> coefficients.
@@ -207,6 +245,7 @@ template <bool SYN>
 __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_cols, int K, uint32_t taddr, int r,
                                float2* four, float2* coeffs, int64_t ldc, int add, bool good) {
     const int m = it.m, par = it.par, tile = it.tile;
+    const int me = t.fp16 ? t.mexp[m] : 0;
     if (SYN) {
         const int j = t.j0[m] + tile * 128 + r;
         const bool valid = good && j < t.nh && m <= t.rings[j].mt;
@@ -215,6 +254,15 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
             float v[32];
             tmem_ld32(taddr + c0, v);
             if (!valid) continue;
+            if (t.fp16) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int k = min((ct * 256 + c0) / 2 + q, K - 1);
+                    const float f = ldexpf(1.f, me + scale_exp(t.absmax_syn[k]) - 2 * F16_TOP);
+                    v[2 * q] *= f;
+                    v[2 * q + 1] *= f;
+                }
+            }
 #pragma unroll
             for (int q = 0; q < 16; q += 2) {
                 const int k = (ct * 256 + c0) / 2 + q;
@@ -240,6 +288,11 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
                 if (k >= K) break;
                 float2* d = coeffs + (int64_t)k * ldc + lmo + 2 * i + par;
                 float2 val = make_float2(v[2 * q], v[2 * q + 1]);
+                if (t.fp16) {
+                    const float f = ldexpf(1.f, me + scale_exp(t.absmax_ana[k] * t.ana_mul) - 2 * F16_TOP);
+                    val.x *= f;
+                    val.y *= f;
+                }
                 if (add) {
                     const float2 o = *d;
                     val.x += o.x;
@@ -339,7 +392,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (!mbar_wait(&full_bar[u % stages], (u / stages) & 1)) atomicExch(t.err, 5);
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------ MMA issuer
-        const uint32_t idesc = idesc_f16(1u, SYN ? 1u : 0u, SYN ? 0u : 1u, (uint32_t)nt_cols);
+        const uint32_t idesc = idesc_f16(t.fp16 ? 0u : 1u, SYN ? 1u : 0u, SYN ? 0u : 1u, (uint32_t)nt_cols);
         int g = 0, ti = 0;
         bool ok = true;
         for (int ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ix += gridDim.x) {
@@ -440,7 +493,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // parity, real/imaginary column and piece, one whole 16-byte chunk of the swizzled
 // K-major tile: rows 8 ib8 .. 8 ib8 + 7 of column c = 2 k + ri. CTA: 8 chunks x 32
 // layers. Rows past the order's last coefficient are written as zeros.
-template <int NPB>
+template <int NPB, bool F16>
 __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const float2* __restrict__ coeffs,
                                                         int64_t ldc, int K) {
     const int m = blockIdx.x;
@@ -464,6 +517,11 @@ __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const flo
 #pragma unroll
         for (int q = 0; q < 16; ++q) v[q] = q < lmrem ? __ldg(src + q) : make_float2(0.f, 0.f);
     }
+    if (F16) {
+        const float sc = ldexpf(1.f, F16_TOP - scale_exp(t.absmax_syn[k]));
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = make_float2(v[q].x * sc, v[q].y * sc);
+    }
     uint8_t* img = reinterpret_cast<uint8_t*>(const_cast<uint16_t*>(t.syn_img));
 #pragma unroll
     for (int par = 0; par < 2; ++par) {
@@ -478,10 +536,8 @@ __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const flo
                 float r1 = ri ? v[2 * (2 * h + 1) + par].y : v[2 * (2 * h + 1) + par].x;
 #pragma unroll
                 for (int q = 0; q < NPB; ++q) {
-                    const __nv_bfloat16 h0 = __float2bfloat16_rn(r0), h1 = __float2bfloat16_rn(r1);
-                    w[q][h] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-                    r0 -= __bfloat162float(h0);
-                    r1 -= __bfloat162float(h1);
+                    const uint32_t b0 = piece_bits<F16>(r0);
+                    w[q][h] = b0 | (piece_bits<F16>(r1) << 16);
                 }
             }
             const int64_t off = (int64_t)(c / 8) * 1024 + (c % 8) * 128 + ((ib8 ^ (c % 8)) * 16);
@@ -491,6 +547,27 @@ __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const flo
                     make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
         }
     }
+}
+
+// Per-layer max-abs of the transform inputs (the fp16 data scaling): one atomic max
+// (on the bits of a non-negative float) per warp.
+__global__ void absmax_coeffs_kernel(const float2* __restrict__ c, int64_t ldc, int64_t nlm, float* __restrict__ out) {
+    const int k = blockIdx.y;
+    float mx = 0.f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nlm; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 v = c[(int64_t)k * ldc + i];
+        mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned int*>(out + k), __float_as_uint(mx));
+}
+__global__ void absmax_grid_kernel(const float* __restrict__ g, int64_t ldg, int64_t npts, float* __restrict__ out) {
+    const int k = blockIdx.y;
+    float mx = 0.f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x)
+        mx = fmaxf(mx, fabsf(g[(int64_t)k * ldg + i]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned int*>(out + k), __float_as_uint(mx));
 }
 
 // ---------------------------------------------------------------- host side
@@ -532,6 +609,11 @@ TcDev make_dev(const Plan& p) {
     t.syn_tile_bytes = s.syn_tile_bytes;
     t.ana_tile_bytes = s.ana_tile_bytes;
     t.nmax = s.nmax;
+    t.fp16 = s.fp16;
+    t.mexp = s.d_mexp;
+    t.absmax_syn = s.d_absmax;
+    t.absmax_ana = s.d_absmax ? s.d_absmax + p.d.nlayers : nullptr;
+    t.ana_mul = s.ana_mul;
     return t;
 }
 
@@ -551,6 +633,9 @@ cudaError_t tc_prepare(Plan& p) {
     p.tc = s;
     if (p.d.precision == SHT_PREC_BF16X3) {
         s->npa = 2; s->npb = 2; s->nprod = 3;
+        s->prod = (0u | (0u << 2)) | ((0u | (1u << 2)) << 4) | ((1u | (0u << 2)) << 8);
+    } else if (p.d.precision == SHT_PREC_FP16X3) {
+        s->npa = 2; s->npb = 2; s->nprod = 3; s->fp16 = 1;
         s->prod = (0u | (0u << 2)) | ((0u | (1u << 2)) << 4) | ((1u | (0u << 2)) << 8);
     } else if (p.d.precision == SHT_PREC_BF16X5) {
         s->npa = 3; s->npb = 2; s->nprod = 5;
@@ -578,45 +663,79 @@ cudaError_t tc_prepare(Plan& p) {
         }
     }
     std::vector<uint16_t> lam((size_t)total, 0);
+    std::vector<int32_t> mexp(mmax, 0);
     {
         const int nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        auto work = [&](int tid) {
-            std::vector<double> col(p.lmax);
-            for (int j = tid; j < nh; j += nthreads) {
-                const double colat = M_PI / 2 - p.latd[j] * M_PI / 180.0;
-                const double xc = std::cos(colat);
-                const double sn = std::sqrt(std::max(0.0, 1.0 - xc * xc));
-                double pmm = 1.0 / std::sqrt(4.0 * M_PI);
-                for (int m = 0; m <= p.mt[j]; ++m) {
-                    if (m > 0) pmm = -std::sqrt((2.0 * m + 1.0) / (2.0 * m)) * sn * pmm;
-                    const int L = p.lmax - m;
-                    col[0] = pmm;
-                    if (L >= 2) {
-                        double p0 = pmm, p1 = std::sqrt(2.0 * m + 3.0) * xc * pmm;
-                        col[1] = p1;
-                        double a_prev = std::sqrt((4.0 * (m + 1) * (m + 1) - 1.0) / ((m + 1.0) * (m + 1.0) - 1.0 * m * m));
-                        for (int l = m + 2; l < p.lmax; ++l) {
-                            const double a = std::sqrt((4.0 * l * l - 1.0) / (1.0 * l * l - 1.0 * m * m));
-                            const double p2 = a * (xc * p1 - p0 / a_prev);
-                            col[l - m] = p2;
-                            p0 = p1;
-                            p1 = p2;
-                            a_prev = a;
-                        }
-                    }
-                    const int jj = j - p.j0[m];
-                    for (int i = 0; i < L; ++i) {
-                        const int par = i & 1, row = i >> 1;
-                        double r = col[i];
-                        for (int q = 0; q < s->npa; ++q) {
-                            const __nv_bfloat16 h = __float2bfloat16_rn((float)r);
-                            lam[blk_off[2 * m + par] + ((int64_t)q * p.rows[m] + row) * pitch[m] + jj] =
-                                __bfloat16_as_ushort(h);
-                            r -= (double)__bfloat162float(h);
-                        }
+        // Lam(l, m) of ring j in FP64 for m <= mt(j): fn(m, column, L)
+        auto columns = [&](int j, std::vector<double>& col, auto&& fn) {
+            const double colat = M_PI / 2 - p.latd[j] * M_PI / 180.0;
+            const double xc = std::cos(colat);
+            const double sn = std::sqrt(std::max(0.0, 1.0 - xc * xc));
+            double pmm = 1.0 / std::sqrt(4.0 * M_PI);
+            for (int m = 0; m <= p.mt[j]; ++m) {
+                if (m > 0) pmm = -std::sqrt((2.0 * m + 1.0) / (2.0 * m)) * sn * pmm;
+                const int L = p.lmax - m;
+                col[0] = pmm;
+                if (L >= 2) {
+                    double p0 = pmm, p1 = std::sqrt(2.0 * m + 3.0) * xc * pmm;
+                    col[1] = p1;
+                    double a_prev = std::sqrt((4.0 * (m + 1) * (m + 1) - 1.0) / ((m + 1.0) * (m + 1.0) - 1.0 * m * m));
+                    for (int l = m + 2; l < p.lmax; ++l) {
+                        const double a = std::sqrt((4.0 * l * l - 1.0) / (1.0 * l * l - 1.0 * m * m));
+                        const double p2 = a * (xc * p1 - p0 / a_prev);
+                        col[l - m] = p2;
+                        p0 = p1;
+                        p1 = p2;
+                        a_prev = a;
                     }
                 }
+                fn(m, col, L);
             }
+        };
+        if (s->fp16) {   // pass 1: e_m from max |Lam| of every order
+            std::vector<std::vector<double>> mx(nthreads, std::vector<double>(mmax, 0.0));
+            auto work = [&](int tid) {
+                std::vector<double> col(p.lmax);
+                for (int j = tid; j < nh; j += nthreads)
+                    columns(j, col, [&](int m, const std::vector<double>& c, int L) {
+                        for (int i = 0; i < L; ++i) mx[tid][m] = std::max(mx[tid][m], std::fabs(c[i]));
+                    });
+            };
+            std::vector<std::thread> th;
+            for (int t = 0; t < nthreads; ++t) th.emplace_back(work, t);
+            for (auto& t : th) t.join();
+            for (int m = 0; m < mmax; ++m) {
+                double v = 0.0;
+                for (int t = 0; t < nthreads; ++t) v = std::max(v, mx[t][m]);
+                int ex = 0;
+                if (v > 0.0) std::frexp(v, &ex);
+                mexp[m] = ex;
+            }
+        }
+        auto work = [&](int tid) {
+            std::vector<double> col(p.lmax);
+            for (int j = tid; j < nh; j += nthreads)
+                columns(j, col, [&](int m, const std::vector<double>& c, int L) {
+                    const int jj = j - p.j0[m];
+                    const double sc = s->fp16 ? std::ldexp(1.0, F16_TOP - mexp[m]) : 1.0;
+                    for (int i = 0; i < L; ++i) {
+                        const int par = i & 1, row = i >> 1;
+                        double r = c[i] * sc;
+                        for (int q = 0; q < s->npa; ++q) {
+                            uint16_t bits;
+                            if (s->fp16) {
+                                const __half h = __float2half_rn((float)r);
+                                bits = __half_as_ushort(h);
+                                r -= (double)__half2float(h);
+                            } else {
+                                const __nv_bfloat16 h = __float2bfloat16_rn((float)r);
+                                bits = __bfloat16_as_ushort(h);
+                                r -= (double)__bfloat162float(h);
+                            }
+                            lam[blk_off[2 * m + par] + ((int64_t)q * p.rows[m] + row) * pitch[m] + jj] = bits;
+                        }
+                    }
+                });
         };
         std::vector<std::thread> th;
         for (int t = 0; t < nthreads; ++t) th.emplace_back(work, t);
@@ -639,7 +758,7 @@ cudaError_t tc_prepare(Plan& p) {
             cuuint64_t strides[2] = {(cuuint64_t)pitch[m] * 2, (cuuint64_t)pitch[m] * 2 * p.rows[m]};
             cuuint32_t box[3] = {BLK, BLK, 1};
             cuuint32_t estr[3] = {1, 1, 1};
-            CUresult r = enc(&maps[2 * m + par], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
+            CUresult r = enc(&maps[2 * m + par], s->fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
                              s->d_lam + blk_off[2 * m + par], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -703,7 +822,17 @@ cudaError_t tc_prepare(Plan& p) {
     p.ana_img.j0 = p.d_j0;
     p.ana_img.npieces = s->npb;
     p.ana_img.tile_bytes = (int32_t)s->ana_tile_bytes;
-    p.ana_img.fp16 = 0;
+    p.ana_img.fp16 = s->fp16;
+    if (s->fp16) {
+        if ((e = up32(&s->d_mexp, mexp)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&s->d_absmax, 2 * sizeof(float) * std::max(1, p.d.nlayers))) != cudaSuccess) return e;
+        if ((e = cudaMemset(s->d_absmax, 0, 2 * sizeof(float) * std::max(1, p.d.nlayers))) != cudaSuccess) return e;
+        double wmax = 0.0;
+        for (int j = 0; j < p.nlat; ++j) wmax = std::max(wmax, p.weights[j]);
+        s->ana_mul = (float)(4.0 * M_PI * wmax * 1.0000001);
+        p.ana_img.absmax = s->d_absmax + p.d.nlayers;
+        p.ana_img.absmax_mul = s->ana_mul;
+    }
 
     s->max_smem = 227 * 1024;
     {
@@ -722,7 +851,7 @@ void tc_release(Plan& p) {
     TcState* s = static_cast<TcState*>(p.tc);
     if (!s) return;
     void* ptrs[] = {s->d_maps, s->d_lam, s->d_nr, s->d_nkt, s->d_njt, s->d_syn_base, s->d_ana_base,
-                    s->d_syn_img, s->d_ana_img, s->d_syn_items, s->d_ana_items};
+                    s->d_syn_img, s->d_ana_img, s->d_syn_items, s->d_ana_items, s->d_mexp, s->d_absmax};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete s;
@@ -738,12 +867,19 @@ static uint32_t tmem_cols_for(int n) {
 cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, int64_t ldc, int K, cudaStream_t st) {
     const TcState& s = *static_cast<const TcState*>(p.tc);
     const TcDev t = make_dev(p);
+    cudaError_t e;
+    if (s.fp16 && K > 0) {
+        if ((e = cudaMemsetAsync(s.d_absmax, 0, sizeof(float) * K, st)) != cudaSuccess) return e;
+        absmax_coeffs_kernel<<<dim3(32, K), 256, 0, st>>>(coeffs, ldc, p.nlm, s.d_absmax);
+    }
     const dim3 ig(p.mmax, (p.rows[0] + BLK - 1) / BLK, (K + 31) / 32);
-    if (s.npb == 2)
-        syn_image_kernel<2><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
+    if (s.fp16)
+        syn_image_kernel<2, true><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
+    else if (s.npb == 2)
+        syn_image_kernel<2, false><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
     else
-        syn_image_kernel<3><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
-    cudaError_t e = cudaGetLastError();
+        syn_image_kernel<3, false><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
+    e = cudaGetLastError();
     if (e != cudaSuccess || s.n_syn_items == 0) return e;
     const int ncols = 2 * K;
     const int nct = (ncols + 255) / 256;
@@ -752,6 +888,16 @@ cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, in
     const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
     legendre_tc_kernel<true><<<dim3(std::min(s.n_syn_items, s.nsm), nct), TC_THREADS, smem, st>>>(
         t, s.d_syn_items, s.n_syn_items, K, nt_cols, stages, tmem_cols_for(nt_cols), p.d_four, nullptr, 0, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t st) {
+    const TcState* s = static_cast<const TcState*>(p.tc);
+    if (!s || !s->fp16 || K <= 0) return cudaSuccess;
+    float* out = s->d_absmax + p.d.nlayers;
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * K, st);
+    if (e != cudaSuccess) return e;
+    absmax_grid_kernel<<<dim3(64, K), 256, 0, st>>>(grid, ldg, p.npoints, out);
     return cudaGetLastError();
 }
 

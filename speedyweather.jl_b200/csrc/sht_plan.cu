@@ -534,8 +534,6 @@ int sht_plan_create(const sht_desc* desc, sht_plan** out) {
     if (d.nlayers < 1) return fail(SHT_EINVAL, "nlayers %d must be >= 1", d.nlayers);
     if (d.precision < SHT_PREC_FP32 || d.precision > SHT_PREC_BF16X5)
         return fail(SHT_EINVAL, "precision %d unknown", d.precision);
-    if (d.precision == SHT_PREC_FP16X3)
-        return fail(SHT_EUNSUPPORTED, "precision SHT_PREC_FP16X3 (scaled split FP16) is not built in this library");
     if (d.precision != SHT_PREC_FP32 && d.nlayers > 1024)
         return fail(SHT_EINVAL, "tensor-core precisions support nlayers <= 1024");
     DeviceGuard g(d.device);
