@@ -460,13 +460,6 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
         }
     }
 }
-// Exponent e with |bound| 2^-e < 1 (0 for a zero bound): the power-of-two data scale
-// of fp16 pieces.
-__device__ __forceinline__ int scale_exp(float bound) {
-    int e = 0;
-    if (bound > 0.f) frexpf(bound, &e);
-    return e;
-}
 template <bool F16>
 __device__ __forceinline__ uint32_t piece_bits(float& r) {
     if (F16) {
@@ -592,8 +585,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
                     const float2 fn = make_float2(a.x + b.x, a.y - b.y);
                     const float2 fs = make_float2(a.y + b.y, b.x - a.x);
                     // fp16 pieces: the layer's data scale 2^(15 - e_k) folded into the weight
-                    const float hw = img.fp16 ? ldexpf(half_domega, 15 - scale_exp(img.absmax[k0 + kl] * img.absmax_mul))
-                                              : half_domega;
+                    const float hw = img.fp16 ? half_domega * img.kscale[k0 + kl].y : half_domega;
                     ev[2 * t] = hw * (fn.x + fs.x);
                     ev[2 * t + 1] = hw * (fn.y + fs.y);
                     ov[2 * t] = hw * (fn.x - fs.x);

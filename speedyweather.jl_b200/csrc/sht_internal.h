@@ -61,8 +61,7 @@ struct TcImage {
     int32_t npieces = 0;
     int32_t tile_bytes = 0;             // bytes of one tile
     int32_t fp16 = 0;                   // 0: bf16 pieces, 1: fp16 pieces
-    const float* absmax = nullptr;      // fp16: per layer max |grid value| of the call (device)
-    float absmax_mul = 0.f;             // fp16: bound of |E|, |O| per unit grid value
+    const float2* kscale = nullptr;     // fp16: per layer (2^(e_k - 15), 2^(15 - e_k)) data scale
 };
 
 struct Plan {

@@ -85,9 +85,8 @@ struct TcDev {
     int nmax;                      // columns of the data images (multiple of 64)
     int fp16;                      // 1: fp16 pieces with power-of-two scaling
     const int32_t* mexp;           // per m: e_m of the Legendre scaling
-    const float* absmax_syn;       // per layer: max |coefficient part| of the synthesis input
-    const float* absmax_ana;       // per layer: max |grid value| of the analysis input
-    float ana_mul;                 // bound of |E|, |O| per unit grid value: 4 pi max_j w_j
+    const float2* kscale_syn;      // per layer: (2^(e_k - 15), 2^(15 - e_k)) of the synthesis input
+    const float2* kscale_ana;      // per layer: the same for the analysis data (E, O)
 };
 
 struct TcState {
@@ -109,7 +108,8 @@ struct TcState {
     int nsm = 148;                 // SMs of the device (persistent grid)
     int fp16 = 0;
     int32_t* d_mexp = nullptr;
-    float* d_absmax = nullptr;     // [2 nlayers]: synthesis, analysis
+    float* d_absmax = nullptr;     // [2 nlayers]: synthesis, analysis max-abs of the call's input
+    float2* d_kscale = nullptr;    // [2 nlayers]: (2^(e_k - 15), 2^(15 - e_k)) per layer
     float ana_mul = 0.f;
 };
 
@@ -245,7 +245,7 @@ template <bool SYN>
 __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_cols, int K, uint32_t taddr, int r,
                                float2* four, float2* coeffs, int64_t ldc, int add, bool good) {
     const int m = it.m, par = it.par, tile = it.tile;
-    const int me = t.fp16 ? t.mexp[m] : 0;
+    const float mscale = t.fp16 ? ldexpf(1.f, t.mexp[m] - F16_TOP) : 1.f;
     if (SYN) {
         const int j = t.j0[m] + tile * 128 + r;
         const bool valid = good && j < t.nh && m <= t.rings[j].mt;
@@ -257,10 +257,9 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
             if (t.fp16) {
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
-                    const int k = min((ct * 256 + c0) / 2 + q, K - 1);
-                    const float f = ldexpf(1.f, me + scale_exp(t.absmax_syn[k]) - 2 * F16_TOP);
-                    v[2 * q] *= f;
-                    v[2 * q + 1] *= f;
+                    const float f = t.kscale_syn[min((ct * 256 + c0) / 2 + q, K - 1)].x;
+                    v[2 * q] = v[2 * q] * mscale * f;
+                    v[2 * q + 1] = v[2 * q + 1] * mscale * f;
                 }
             }
 #pragma unroll
@@ -289,9 +288,9 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
                 float2* d = coeffs + (int64_t)k * ldc + lmo + 2 * i + par;
                 float2 val = make_float2(v[2 * q], v[2 * q + 1]);
                 if (t.fp16) {
-                    const float f = ldexpf(1.f, me + scale_exp(t.absmax_ana[k] * t.ana_mul) - 2 * F16_TOP);
-                    val.x *= f;
-                    val.y *= f;
+                    const float f = t.kscale_ana[k].x;
+                    val.x = val.x * mscale * f;
+                    val.y = val.y * mscale * f;
                 }
                 if (add) {
                     const float2 o = *d;
@@ -518,7 +517,7 @@ __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const flo
         for (int q = 0; q < 16; ++q) v[q] = q < lmrem ? __ldg(src + q) : make_float2(0.f, 0.f);
     }
     if (F16) {
-        const float sc = ldexpf(1.f, F16_TOP - scale_exp(t.absmax_syn[k]));
+        const float sc = t.kscale_syn[k].y;
 #pragma unroll
         for (int q = 0; q < 16; ++q) v[q] = make_float2(v[q].x * sc, v[q].y * sc);
     }
@@ -549,25 +548,36 @@ __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const flo
     }
 }
 
-// Per-layer max-abs of the transform inputs (the fp16 data scaling): one atomic max
-// (on the bits of a non-negative float) per warp.
-__global__ void absmax_coeffs_kernel(const float2* __restrict__ c, int64_t ldc, int64_t nlm, float* __restrict__ out) {
-    const int k = blockIdx.y;
-    float mx = 0.f;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nlm; i += (int64_t)gridDim.x * blockDim.x) {
-        const float2 v = c[(int64_t)k * ldc + i];
-        mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
-    }
+// Per-layer max-abs of the transform inputs (the fp16 data scaling): 16-byte loads
+// where aligned, one atomic max (on the bits of a non-negative float) per warp.
+__device__ __forceinline__ void warp_atomic_max(float* out, float mx) {
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned int*>(out + k), __float_as_uint(mx));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned int*>(out), __float_as_uint(mx));
 }
-__global__ void absmax_grid_kernel(const float* __restrict__ g, int64_t ldg, int64_t npts, float* __restrict__ out) {
+__global__ void absmax_kernel(const float* __restrict__ x, int64_t ld, int64_t n, float* __restrict__ out) {
     const int k = blockIdx.y;
+    const float* row = x + (int64_t)k * ld;
     float mx = 0.f;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x)
-        mx = fmaxf(mx, fabsf(g[(int64_t)k * ldg + i]));
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<unsigned int*>(out + k), __float_as_uint(mx));
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i0 = 0;
+    if ((reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+        const float4* r4 = reinterpret_cast<const float4*>(row);
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n / 4; i += stride) {
+            const float4 v = __ldg(r4 + i);
+            mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+        }
+        i0 = n / 4 * 4;
+    }
+    for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+        mx = fmaxf(mx, fabsf(__ldg(row + i)));
+    warp_atomic_max(out + k, mx);
+}
+// (2^(e - 15), 2^(15 - e)) with bound = mul * max-abs, |bound| 2^-e < 1
+__global__ void kscale_kernel(const float* __restrict__ absmax, float mul, int K, float2* __restrict__ out) {
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int e = scale_exp(absmax[k] * mul);
+        out[k] = make_float2(ldexpf(1.f, e - F16_TOP), ldexpf(1.f, F16_TOP - e));
+    }
 }
 
 // ---------------------------------------------------------------- host side
@@ -611,9 +621,8 @@ TcDev make_dev(const Plan& p) {
     t.nmax = s.nmax;
     t.fp16 = s.fp16;
     t.mexp = s.d_mexp;
-    t.absmax_syn = s.d_absmax;
-    t.absmax_ana = s.d_absmax ? s.d_absmax + p.d.nlayers : nullptr;
-    t.ana_mul = s.ana_mul;
+    t.kscale_syn = s.d_kscale;
+    t.kscale_ana = s.d_kscale ? s.d_kscale + p.d.nlayers : nullptr;
     return t;
 }
 
@@ -827,11 +836,11 @@ cudaError_t tc_prepare(Plan& p) {
         if ((e = up32(&s->d_mexp, mexp)) != cudaSuccess) return e;
         if ((e = cudaMalloc(&s->d_absmax, 2 * sizeof(float) * std::max(1, p.d.nlayers))) != cudaSuccess) return e;
         if ((e = cudaMemset(s->d_absmax, 0, 2 * sizeof(float) * std::max(1, p.d.nlayers))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&s->d_kscale, 2 * sizeof(float2) * std::max(1, p.d.nlayers))) != cudaSuccess) return e;
         double wmax = 0.0;
         for (int j = 0; j < p.nlat; ++j) wmax = std::max(wmax, p.weights[j]);
         s->ana_mul = (float)(4.0 * M_PI * wmax * 1.0000001);
-        p.ana_img.absmax = s->d_absmax + p.d.nlayers;
-        p.ana_img.absmax_mul = s->ana_mul;
+        p.ana_img.kscale = s->d_kscale + p.d.nlayers;
     }
 
     s->max_smem = 227 * 1024;
@@ -851,7 +860,8 @@ void tc_release(Plan& p) {
     TcState* s = static_cast<TcState*>(p.tc);
     if (!s) return;
     void* ptrs[] = {s->d_maps, s->d_lam, s->d_nr, s->d_nkt, s->d_njt, s->d_syn_base, s->d_ana_base,
-                    s->d_syn_img, s->d_ana_img, s->d_syn_items, s->d_ana_items, s->d_mexp, s->d_absmax};
+                    s->d_syn_img, s->d_ana_img, s->d_syn_items, s->d_ana_items, s->d_mexp, s->d_absmax,
+                    s->d_kscale};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete s;
@@ -870,7 +880,10 @@ cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, in
     cudaError_t e;
     if (s.fp16 && K > 0) {
         if ((e = cudaMemsetAsync(s.d_absmax, 0, sizeof(float) * K, st)) != cudaSuccess) return e;
-        absmax_coeffs_kernel<<<dim3(32, K), 256, 0, st>>>(coeffs, ldc, p.nlm, s.d_absmax);
+        // a complex layer is 2 nlm floats
+        absmax_kernel<<<dim3(std::max(1, 2 * s.nsm / std::max(1, K)) * 4, K), 256, 0, st>>>(
+            reinterpret_cast<const float*>(coeffs), 2 * ldc, 2 * p.nlm, s.d_absmax);
+        kscale_kernel<<<1, 256, 0, st>>>(s.d_absmax, 1.f, K, s.d_kscale);
     }
     const dim3 ig(p.mmax, (p.rows[0] + BLK - 1) / BLK, (K + 31) / 32);
     if (s.fp16)
@@ -897,7 +910,8 @@ cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int
     float* out = s->d_absmax + p.d.nlayers;
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * K, st);
     if (e != cudaSuccess) return e;
-    absmax_grid_kernel<<<dim3(64, K), 256, 0, st>>>(grid, ldg, p.npoints, out);
+    absmax_kernel<<<dim3(std::max(1, 2 * s->nsm / std::max(1, K)) * 4, K), 256, 0, st>>>(grid, ldg, p.npoints, out);
+    kscale_kernel<<<1, 256, 0, st>>>(out, s->ana_mul, K, s->d_kscale + p.d.nlayers);
     return cudaGetLastError();
 }
 
