@@ -254,6 +254,29 @@ def time_stages(S, lt, field, out, reps):
     return res
 
 
+def profile_run(args):
+    """W + K round trips of one precision at the benchmark workload and nothing else:
+    the command ncu wraps for the launch list and the per-kernel captures."""
+    import torch
+    import speedytransforms as st
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sht_oracle as O
+    prec = "bf16x3" if args.precision == "auto" else args.precision
+    device = torch.device("cuda", 0)
+    spec, grid = st.Spectrum(T, T), st.OctahedralGaussianGrid(NLAT_HALF)
+    c_np = O.random_coeffs(O.Spectrum(T, T), LAYERS, seed=2)
+    lt = st.LowerTriangularArray(torch.tensor(np.ascontiguousarray(c_np.T), dtype=torch.complex64).to(device), spec)
+    field = st.Field.zeros(grid, LAYERS, device=device)
+    out = st.LowerTriangularArray.zeros(spec, LAYERS, device=device)
+    S = st.SpectralTransform(spec, grid, nlayers=LAYERS, precision=prec, device=device)
+    for _ in range(args.warmup + args.steps):
+        st.transform_(field, lt, S)
+        st.transform_(out, field, S)
+    torch.cuda.synchronize()
+    print(f"profile run: {prec}, {args.warmup} + {args.steps} round trips, device status {S.device_status()}")
+    return 0
+
+
 def run_ours(args):
     import torch
     rank, local_rank, world = dist_env()
@@ -387,7 +410,9 @@ def run_ours(args):
         mult = 3 if head in ("bf16x3", "fp16x3") else 1
         roofline["legendre_tflops"] = alg[dom]["flops"] * mult / (stage_ms[dom] * 1e-3) / 1e12
 
-    launches_per_rt = 4
+    # this library's kernels per round trip: FFT x 2 and Legendre x 2, plus the tensor-core
+    # synthesis data image, plus for fp16 the two max-abs passes and their scale kernels
+    launches_per_rt = {"fp32": 4, "bf16x3": 5, "bf16x5": 5, "fp16x3": 9}[head]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": head, "data": "synthetic",
@@ -418,11 +443,15 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3", "fp16x3", "bf16x5"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only W + K round trips of one precision (default bf16x3), for profilers")
     ap.add_argument("--ref-sample-layers", type=int, default=16)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_run:
+        return profile_run(args)
     return run_ours(args)
 
 
