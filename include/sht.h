@@ -182,6 +182,54 @@ SHT_API int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p, 
 SHT_API int sht_analyze_static_scratch(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, int64_t ldc,
                                        int K, unsigned flags, void* stream);
 
+/* Autotuner of a plan's own launches: times the FP32 Legendre kernels of an
+ * SHT_PREC_FP32 plan at K layers for each tile width (32, 64, 128 real columns) on
+ * scratch buffers it allocates, keeps the fastest per direction for later calls, and
+ * reports them in tile_columns[2] (synthesis, analysis; may be NULL). Results are
+ * bitwise the same for every tile width. Tensor-core plans have nothing to tune and
+ * return SHT_OK with tile_columns = {0, 0}. No counterpart in the reference. */
+SHT_API int sht_plan_autotune(sht_plan* plan, int K, void* stream, int32_t* tile_columns);
+
+/* ---- batches: many transforms (different plans, truncations, layer counts) in one
+ * grouped launch per stage, optionally captured as one CUDA graph ---------------------
+ * replaces the per-transform launch sequences of a time step
+ * (SpeedyWeather/src/time_stepping/transform.jl:117-191) and the per-transform CUDA
+ * graphs the reference caches by field pointer (SpeedyTransforms/ext/gpu_graphs_common.jl:296-343).
+ * A batch runs all SHT_SYNTHESIS items, then all SHT_ANALYSIS items, as four persistent
+ * launches (Legendre synthesis, FFT synthesis, FFT analysis, Legendre analysis) over the
+ * union of the items' work lists; each item has its own Fourier scratch, allocated by
+ * sht_batch_create, so items may share a plan. Arrays are bound at creation: later runs
+ * read and write the same device buffers. Plans: SHT_PREC_FP32, one device. */
+#define SHT_SYNTHESIS 0          /* coeffs -> grid */
+#define SHT_ANALYSIS 1           /* grid -> coeffs */
+
+typedef struct {
+    sht_plan* plan;
+    int direction;               /* SHT_SYNTHESIS or SHT_ANALYSIS */
+    void* coeffs;                /* [nlayers][ldc] complex float */
+    int64_t ldc;
+    float* grid;                 /* [nlayers][ldg] float */
+    int64_t ldg;
+    int nlayers;                 /* 1 .. the plan's nlayers */
+    unsigned flags;              /* SHT_UNSCALE_COSLAT (synthesis), SHT_ADD */
+} sht_batch_item;
+
+typedef struct sht_batch sht_batch;
+
+SHT_API int sht_batch_create(const sht_batch_item* items, int nitems, sht_batch** out);
+/* the grouped launches, on stream */
+SHT_API int sht_batch_run(sht_batch* b, void* stream);
+/* the same transforms as one sht_synthesize / sht_analyze call each (the baseline) */
+SHT_API int sht_batch_run_each(sht_batch* b, void* stream);
+/* captures sht_batch_run into a CUDA graph (on stream, or on a stream of the batch when
+ * stream is NULL: the legacy stream cannot capture); sht_batch_launch replays it */
+SHT_API int sht_batch_capture(sht_batch* b, void* stream);
+SHT_API int sht_batch_launch(sht_batch* b, void* stream);
+/* times the grouped launches for each Legendre tile width (running the batch), keeps
+ * the fastest and reports it; drops a captured graph (capture again afterwards) */
+SHT_API int sht_batch_autotune(sht_batch* b, void* stream, int32_t* tile_columns);
+SHT_API int sht_batch_destroy(sht_batch* b);
+
 /* Synchronises the device and returns (then clears) the plan's device status word:
  * 0 = no kernel gave up waiting; otherwise the code of the first bounded wait in a
  * tensor-core kernel that expired (1 s limit), whose outputs are then incomplete.

@@ -21,6 +21,9 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <map>
+#include <mutex>
+
 #include "sht_internal.h"
 
 namespace sht {
@@ -503,13 +506,17 @@ __device__ __forceinline__ void put_pieces(uint8_t* dst, int64_t piece_stride, c
 // shared memory: W (n twiddles, padded to even) | G (prime tables) | X (C ldx) | Y (C ldx);
 // ldx >= n is the padded layer stride
 
-// grid -> Fourier scratch (E/O combinations weighted by the solid angle)
-__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kernel(const int2* __restrict__ items, const RingDesc* __restrict__ rings,
-                                                           const float2* __restrict__ twiddle,
-                                                           const float* __restrict__ grid, int64_t ldg,
-                                                           float2* __restrict__ four, int K, const TcImage img) {
-    extern __shared__ float2 sm[];
-    const int2 item = items[blockIdx.x];
+// grid -> Fourier scratch (E/O combinations weighted by the solid angle), one work
+// item (ring, layer chunk) of one transform
+__device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2* sm) {
+    const RingDesc* __restrict__ rings = v.rings;
+    const float2* __restrict__ twiddle = v.twiddle;
+    const float* __restrict__ grid = v.gin;
+    const int64_t ldg = v.ldg;
+    float2* __restrict__ four = v.four;
+    const int K = v.K;
+    const TcImage& img = v.img;
+    const int2 item = make_int2(ring, chunk);
     const RingDesc& rd = rings[item.x];
     const int k0 = item.y * rd.chunk;
     if (k0 >= K) return;
@@ -631,13 +638,15 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
     }
 }
 
-// Fourier scratch -> grid
-__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kernel(const int2* __restrict__ items, const RingDesc* __restrict__ rings,
-                                                            const float2* __restrict__ twiddle,
-                                                            const float2* __restrict__ four, float* __restrict__ grid,
-                                                            int64_t ldg, int K, int unscale, int add) {
-    extern __shared__ float2 sm[];
-    const int2 item = items[blockIdx.x];
+// Fourier scratch -> grid, one work item (ring, layer chunk) of one transform
+__device__ void fft_synthesis_body(const FftView& v, int ring, int chunk, float2* sm) {
+    const RingDesc* __restrict__ rings = v.rings;
+    const float2* __restrict__ twiddle = v.twiddle;
+    const float2* __restrict__ four = v.four;
+    float* __restrict__ grid = v.gout;
+    const int64_t ldg = v.ldg;
+    const int K = v.K, unscale = v.unscale, add = v.add;
+    const int2 item = make_int2(ring, chunk);
     const RingDesc& rd = rings[item.x];
     const int k0 = item.y * rd.chunk;
     if (k0 >= K) return;
@@ -714,9 +723,63 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kern
     store_rings(grid, ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn, z, add);
 }
 
+__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kernel(const int2* __restrict__ items,
+                                                                                  const FftView v) {
+    extern __shared__ float2 sm[];
+    const int2 it = items[blockIdx.x];
+    fft_analysis_body(v, it.x, it.y, sm);
+}
+
+__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kernel(const int2* __restrict__ items,
+                                                                                   const FftView v) {
+    extern __shared__ float2 sm[];
+    const int2 it = items[blockIdx.x];
+    fft_synthesis_body(v, it.x, it.y, sm);
+}
+
+// Persistent grouped launch over the (ring, chunk) items of many transforms: CTA b
+// takes the items b, b + gridDim.x, ... of the batch's list (task, ring, chunk).
+__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_grouped_kernel(const FftView* __restrict__ views,
+                                                                                 const GroupItem* __restrict__ items,
+                                                                                 int nitems, int synthesis) {
+    extern __shared__ float2 sm[];
+    for (int ix = blockIdx.x; ix < nitems; ix += gridDim.x) {
+        const GroupItem it = items[ix];
+        __syncthreads();                  // the previous item is done with shared memory
+        if (synthesis)
+            fft_synthesis_body(views[it.task], it.a, it.b, sm);
+        else
+            fft_analysis_body(views[it.task], it.a, it.b, sm);
+    }
+}
+
 }  // namespace
 
 static int fft_threads(const Plan&) { return kFftThreads; }
+
+FftView fft_view(const Plan& p, const float* gin, float* gout, int64_t ldg, float2* four, int K, unsigned flags,
+                 bool image) {
+    FftView v{};
+    v.rings = p.d_rings;
+    v.twiddle = p.d_twiddle;
+    v.gin = gin;
+    v.gout = gout;
+    v.ldg = ldg;
+    v.four = four;
+    v.K = K;
+    v.unscale = (flags & SHT_UNSCALE_COSLAT) ? 1 : 0;
+    v.add = (flags & SHT_ADD) ? 1 : 0;
+    if (image) v.img = p.ana_img;
+    return v;
+}
+
+cudaError_t launch_fft_grouped(const FftView* views, const GroupItem* items, int nitems, bool synthesis, int smem,
+                               int grid, cudaStream_t s) {
+    if (nitems == 0) return cudaSuccess;
+    const int g = std::max(1, std::min(nitems, grid));
+    fft_grouped_kernel<<<g, kFftThreads, smem, s>>>(views, items, nitems, synthesis ? 1 : 0);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, bool to_image) {
     const dim3 g(p.n_fft_items);
@@ -725,23 +788,35 @@ cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, i
         const cudaError_t e = tc_analysis_scale(p, grid, ldg, K, s);
         if (e != cudaSuccess) return e;
     }
-    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, p.d_rings, p.d_twiddle, grid, ldg, p.d_four, K,
-                                                              (to_image || p.tc) ? p.ana_img : none);
+    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(
+        p.d_fft_items, fft_view(p, grid, nullptr, ldg, p.d_four, K, 0, to_image || p.tc));
+    (void)none;
     return cudaGetLastError();
 }
 
 cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags, cudaStream_t s) {
     const dim3 g(p.n_fft_items);
-    fft_synthesis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, p.d_rings, p.d_twiddle, p.d_four, grid, ldg, K,
-                                                               (flags & SHT_UNSCALE_COSLAT) ? 1 : 0,
-                                                               (flags & SHT_ADD) ? 1 : 0);
+    fft_synthesis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(
+        p.d_fft_items, fft_view(p, nullptr, grid, ldg, p.d_four, K, flags, false));
     return cudaGetLastError();
 }
 
+// The limit is a property of the kernel, not of a plan: it is raised to the per-CTA
+// budget (or a larger plan's need) and never lowered, so plans of any size coexist.
 cudaError_t fft_set_smem(int bytes) {
-    cudaError_t e = cudaFuncSetAttribute(fft_analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    static std::mutex mu;
+    static std::map<int, int> current;     // per device (the attribute is per context)
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(fft_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    bytes = std::max(bytes, kFftSmemBudget);
+    std::lock_guard<std::mutex> lock(mu);
+    if (bytes <= current[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(fft_analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fft_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fft_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) current[dev] = bytes;
+    return e;
 }
 
 }  // namespace sht
@@ -752,8 +827,8 @@ namespace sht {
 cudaError_t launch_fft_analysis_to(const Plan& p, const float* grid, int64_t ldg, int K, float2* scratch,
                                    cudaStream_t s) {
     const dim3 g(p.n_fft_items);
-    const TcImage none{};
-    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, p.d_rings, p.d_twiddle, grid, ldg, scratch, K, none);
+    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(
+        p.d_fft_items, fft_view(p, grid, nullptr, ldg, scratch, K, 0, false));
     return cudaGetLastError();
 }
 }  // namespace sht

@@ -50,6 +50,28 @@ struct LegItem {
     int32_t tile;         // ring tile (synthesis) or parity-row tile (analysis)
 };
 
+// The operands of one transform's FP32 Legendre stage (plan tables, data pointers).
+struct LegView {
+    const float* lam;
+    const int64_t* lam_off;
+    const int32_t* rows;
+    const int32_t* j0;
+    const int64_t* lm_off;
+    const RingDesc* rings;
+    int nh, nh_pad, lmax;
+    const float2* cin;    // synthesis input coefficients
+    float2* cout;         // analysis output coefficients
+    int64_t ldc;
+    float2* four;         // Fourier scratch
+    int K, add;
+};
+
+// One work item of a grouped (batched) launch over several transforms.
+struct GroupItem {
+    int32_t task;         // index into the batch's per-transform argument array
+    int32_t a, b, c;      // Legendre: m, tile, column tile * 2 + parity; FFT: ring, chunk, -
+};
+
 // Layout of the analysis data operand the FFT writes for the tensor-core Legendre
 // stage: pre-swizzled (SWIZZLE_128B, MN-major) 16-bit tiles of 64 rings x N columns,
 // one tile per (order m, parity, ring block, piece).
@@ -62,6 +84,18 @@ struct TcImage {
     int32_t tile_bytes = 0;             // bytes of one tile
     int32_t fp16 = 0;                   // 0: bf16 pieces, 1: fp16 pieces
     const float2* kscale = nullptr;     // fp16: per layer (2^(e_k - 15), 2^(15 - e_k)) data scale
+};
+
+// The operands of one transform's FFT stage.
+struct FftView {
+    const RingDesc* rings;
+    const float2* twiddle;
+    const float* gin;     // analysis input grid
+    float* gout;          // synthesis output grid
+    int64_t ldg;
+    float2* four;         // Fourier scratch
+    int K, unscale, add;
+    TcImage img;          // analysis operand image of tensor-core plans (base == nullptr: FP32 scratch)
 };
 
 struct Plan {
@@ -113,6 +147,11 @@ struct Plan {
     int min_chunk = 1;
     int2* d_fft_items = nullptr;        // FFT work list: (ring, layer chunk), costliest first
     int n_fft_items = 0;
+    int leg_bn_syn = 128, leg_bn_ana = 128;   // FP32 Legendre tile widths (autotuned)
+    // host copies for batches (grouped launches over several plans)
+    std::vector<RingDesc> h_rings;
+    std::vector<double> h_ring_cost;     // per ring: estimated FFT cost per layer
+    std::vector<LegItem> h_syn_items, h_ana_items;
 };
 
 enum GradIdx {
@@ -121,11 +160,21 @@ enum GradIdx {
 };
 
 // ---- launchers (return cudaError_t of the launch) ----------------------------------
+FftView fft_view(const Plan& p, const float* gin, float* gout, int64_t ldg, float2* four, int K, unsigned flags,
+                 bool image);
+cudaError_t launch_fft_grouped(const FftView* views, const GroupItem* items, int nitems, bool synthesis, int smem,
+                               int grid, cudaStream_t s);
 cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s);
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s,
                                 bool to_image = false);
 cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags,
                                  cudaStream_t s);
+LegView leg_view(const Plan& p, const float2* cin, float2* cout, int64_t ldc, const float2* four, int K, bool add);
+cudaError_t legendre_grouped_grids(int nsm, int (&grid)[3]);
+cudaError_t launch_legendre_grouped(const LegView* views, const GroupItem* items, int nitems, int bn, bool synthesis,
+                                    int grid, cudaStream_t s);
+cudaError_t launch_legendre_analysis_fp32_from(const Plan& p, const float2* scratch, float2* coeffs, int64_t ldc,
+                                               int K, bool add, cudaStream_t s);
 cudaError_t launch_legendre_synthesis_fp32(const Plan& p, const float2* coeffs, int64_t ldc, int K,
                                            cudaStream_t s);
 cudaError_t launch_legendre_analysis_fp32(const Plan& p, float2* coeffs, int64_t ldc, int K, bool add,

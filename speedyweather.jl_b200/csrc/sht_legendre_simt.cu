@@ -9,8 +9,12 @@
 // (the north/south symmetry lambda_lm(-x) = (-1)^(l-m) lambda_lm(x)):
 //   synthesis  X_p[j, c] = sum_i Lam[m][p][i][j] * a[m + 2i + p, c]      -> E (p=0), O (p=1)
 //   analysis   a[m + 2i + p, c] = sum_j Lam[m][p][i][j] * Y_p[j, c]      Y_0 = E, Y_1 = O
-// with c running over the 2K real columns (re, im of each layer). One CTA
-// computes a 64 x 128 tile of one parity with register tiles of 8 x 8 per thread.
+// with c running over the 2K real columns (re, im of each layer). One CTA of 128
+// threads computes a 64 x BN tile of one parity (BN = 32, 64 or 128 real columns,
+// register tiles of 8 x BN/16 per thread). The contraction runs in steps of 8 in the
+// same order for every BN, so the tile width changes the speed, not the result: the
+// autotuner picks it per plan and direction, and the grouped launch of a batch of
+// transforms (one CTA loop over the tiles of all of them) reuses the same tile bodies.
 #include "sht_internal.h"
 
 namespace sht {
@@ -18,58 +22,116 @@ namespace sht {
 namespace {
 
 constexpr int BM = 64;    // rings (synthesis) or parity rows (analysis) per CTA
-constexpr int BN = 128;   // real columns per CTA (64 complex layers)
 constexpr int BK = 8;     // contraction depth per shared-memory stage
 constexpr int NT = 128;   // threads
 
-__global__ void __launch_bounds__(NT) legendre_synthesis_fp32_kernel(
-    const LegItem* __restrict__ items, const float* __restrict__ lam, const int64_t* __restrict__ lam_off,
-    const int32_t* __restrict__ rows_of, const int64_t* __restrict__ lm_off, const RingDesc* __restrict__ rings,
-    int nh, int nh_pad, int lmax, const float2* __restrict__ coeffs, int64_t ldc, float2* __restrict__ four, int K) {
-    __shared__ __align__(16) float As[2][BK][BM];
-    __shared__ __align__(16) float Bs[2][BK][BN];
-    const LegItem it = items[blockIdx.x];
-    const int m = it.m;
-    const int par = blockIdx.z;
-    const int j0 = it.tile * BM;
-    const int kt0 = blockIdx.y * (BN / 2);
-    const int rows = rows_of[m];
-    const float* L = lam + lam_off[m] + (int64_t)par * rows * nh_pad;
-    const int64_t lmo = lm_off[m];
+template <int N>
+struct Vec;
+template <>
+struct Vec<2> {
+    static __device__ __forceinline__ void ld(const float* p, float* v) {
+        const float2 a = *reinterpret_cast<const float2*>(p);
+        v[0] = a.x;
+        v[1] = a.y;
+    }
+};
+template <>
+struct Vec<4> {
+    static __device__ __forceinline__ void ld(const float* p, float* v) {
+        const float4 a = *reinterpret_cast<const float4*>(p);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = a.z;
+        v[3] = a.w;
+    }
+};
+
+// 8 x TN register tile, TN = BN / 16: rows ty*4 + {0..3} and 32 + ty*4 + {0..3};
+// columns tx*H + {0..H-1} and BN/2 + tx*H + {0..H-1} (H = TN/2, TN >= 4) or
+// tx*2 + {0, 1} (TN = 2); tx < 16, ty < 8. Columns 2c, 2c + 1 of a thread are the
+// re, im parts of one layer.
+template <int BN>
+struct Cols {
+    static constexpr int TN = BN / 16;
+    static constexpr bool SPLIT = TN >= 4;
+    static constexpr int H = SPLIT ? TN / 2 : TN;
+    static __device__ __forceinline__ int col(int tx, int c) {
+        return SPLIT ? (c < H ? tx * H + c : BN / 2 + tx * H + (c - H)) : tx * TN + c;
+    }
+};
+
+template <int BN>
+__device__ __forceinline__ void mma_step(const float (&As)[BK][BM], const float (&Bs)[BK][BN], int tx, int ty,
+                                         float (&acc)[8][BN / 16]) {
+    constexpr int TN = Cols<BN>::TN, H = Cols<BN>::H;
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+        const float4 a0 = *reinterpret_cast<const float4*>(&As[kk][ty * 4]);
+        const float4 a1 = *reinterpret_cast<const float4*>(&As[kk][32 + ty * 4]);
+        float bv[TN];
+        if constexpr (Cols<BN>::SPLIT) {
+            Vec<H>::ld(&Bs[kk][tx * H], bv);
+            Vec<H>::ld(&Bs[kk][BN / 2 + tx * H], bv + H);
+        } else {
+            Vec<TN>::ld(&Bs[kk][tx * TN], bv);
+        }
+        const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int c = 0; c < TN; ++c) acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
+    }
+}
+
+template <int BN>
+__device__ __forceinline__ int col_of(int tx, int c) {
+    return Cols<BN>::col(tx, c);
+}
+
+template <int BN>
+__device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[2][BK][BM],
+                         float (&Bs)[2][BK][BN]) {
+    constexpr int TN = BN / 16;
+    constexpr int NB = BN / 32;                   // complex coefficients per thread and stage
+    const int j0 = tile * BM;
+    const int kt0 = ct * (BN / 2);
+    const int rows = v.rows[m];
+    const float* L = v.lam + v.lam_off[m] + (int64_t)par * rows * v.nh_pad;
+    const int64_t lmo = v.lm_off[m];
     const int t = threadIdx.x;
-    const int tx = t % 16, ty = t / 16;   // 16 column groups x 8 row groups
-
-    // global load mapping
+    const int tx = t % 16, ty = t / 16;
     const int a_i = t / 16, a_j = (t % 16) * 4;   // one float4 of Lam per thread
-    const int b_k = t % 64, b_i0 = (t / 64);     // 4 complex coefficients per thread
+    const int b_k = t % (BN / 2), b_i0 = t / (BN / 2);
+    constexpr int BSTEP = NT / (BN / 2);          // rows of B covered per load pass
 
-    float acc[8][8];
+    float acc[8][TN];
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[r][c] = 0.f;
+        for (int c = 0; c < TN; ++c) acc[r][c] = 0.f;
 
-    auto load_tiles = [&](int i0, float4& ra, float2 (&rb)[4]) {
+    auto load_tiles = [&](int i0, float4& ra, float2 (&rb)[NB]) {
         const int i = i0 + a_i;
-        ra = (i < rows) ? *reinterpret_cast<const float4*>(L + (int64_t)i * nh_pad + j0 + a_j)
+        ra = (i < rows) ? *reinterpret_cast<const float4*>(L + (int64_t)i * v.nh_pad + j0 + a_j)
                         : make_float4(0.f, 0.f, 0.f, 0.f);
         const int k = kt0 + b_k;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int ii = i0 + b_i0 + 2 * q;
+        for (int q = 0; q < NB; ++q) {
+            const int ii = i0 + b_i0 + BSTEP * q;
             const int l = m + 2 * ii + par;
-            rb[q] = (ii < rows && l < lmax && k < K) ? coeffs[(int64_t)k * ldc + lmo + 2 * ii + par]
-                                                     : make_float2(0.f, 0.f);
+            rb[q] = (ii < rows && l < v.lmax && k < v.K) ? v.cin[(int64_t)k * v.ldc + lmo + 2 * ii + par]
+                                                          : make_float2(0.f, 0.f);
         }
     };
-    auto store_tiles = [&](int buf, const float4& ra, const float2 (&rb)[4]) {
+    auto store_tiles = [&](int buf, const float4& ra, const float2 (&rb)[NB]) {
         *reinterpret_cast<float4*>(&As[buf][a_i][a_j]) = ra;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) *reinterpret_cast<float2*>(&Bs[buf][b_i0 + 2 * q][2 * b_k]) = rb[q];
+        for (int q = 0; q < NB; ++q) *reinterpret_cast<float2*>(&Bs[buf][b_i0 + BSTEP * q][2 * b_k]) = rb[q];
     };
 
     float4 ra;
-    float2 rb[4];
+    float2 rb[NB];
+    __syncthreads();                               // the previous tile's reads of As/Bs are done
     load_tiles(0, ra, rb);
     store_tiles(0, ra, rb);
     __syncthreads();
@@ -77,19 +139,7 @@ __global__ void __launch_bounds__(NT) legendre_synthesis_fp32_kernel(
     for (int i0 = 0; i0 < rows; i0 += BK) {
         const bool more = i0 + BK < rows;
         if (more) load_tiles(i0 + BK, ra, rb);
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
-            const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][32 + ty * 4]);
-            const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
-            const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][kk][64 + tx * 4]);
-            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-#pragma unroll
-                for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
-        }
+        mma_step<BN>(As[buf], Bs[buf], tx, ty, acc);
         if (more) {
             store_tiles(buf ^ 1, ra, rb);
             __syncthreads();
@@ -100,95 +150,77 @@ __global__ void __launch_bounds__(NT) legendre_synthesis_fp32_kernel(
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         const int j = j0 + (r < 4 ? ty * 4 + r : 32 + ty * 4 + (r - 4));
-        if (j >= nh) continue;
-        const RingDesc& rd = rings[j];
+        if (j >= v.nh) continue;
+        const RingDesc& rd = v.rings[j];
         if (m > rd.mt) continue;
-        float2* dst = four + ((rd.gofs + m) * 2 + par) * K;
+        float2* dst = v.four + ((rd.gofs + m) * 2 + par) * v.K;
 #pragma unroll
-        for (int cp = 0; cp < 4; ++cp) {
-            const int col = (cp < 2 ? tx * 4 + 2 * cp : 64 + tx * 4 + 2 * (cp - 2));
-            const int k = kt0 + col / 2;
-            if (k < K) dst[k] = make_float2(acc[r][2 * cp], acc[r][2 * cp + 1]);
+        for (int c = 0; c < TN; c += 2) {
+            const int k = kt0 + col_of<BN>(tx, c) / 2;
+            if (k < v.K) dst[k] = make_float2(acc[r][c], acc[r][c + 1]);
         }
     }
-    (void)nh_pad;
 }
 
-__global__ void __launch_bounds__(NT) legendre_analysis_fp32_kernel(
-    const LegItem* __restrict__ items, const float* __restrict__ lam, const int64_t* __restrict__ lam_off,
-    const int32_t* __restrict__ rows_of, const int32_t* __restrict__ j0_of, const int64_t* __restrict__ lm_off,
-    const RingDesc* __restrict__ rings, int nh, int nh_pad, int lmax, const float2* __restrict__ four,
-    float2* __restrict__ coeffs, int64_t ldc, int K, int add) {
-    __shared__ __align__(16) float As[2][BK][BM];
-    __shared__ __align__(16) float Bs[2][BK][BN];
-    const LegItem it = items[blockIdx.x];
-    const int m = it.m;
-    const int par = blockIdx.z;
-    const int i_base = it.tile * BM;
-    const int kt0 = blockIdx.y * (BN / 2);
-    const int rows = rows_of[m];
-    const float* L = lam + lam_off[m] + (int64_t)par * rows * nh_pad;
-    const int64_t lmo = lm_off[m];
-    const int jstart = (j0_of[m] / BK) * BK;
+template <int BN>
+__device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[2][BK][BM],
+                         float (&Bs)[2][BK][BN]) {
+    constexpr int TN = BN / 16;
+    constexpr int NB = BN / 32;
+    const int i_base = tile * BM;
+    const int kt0 = ct * (BN / 2);
+    const int rows = v.rows[m];
+    const float* L = v.lam + v.lam_off[m] + (int64_t)par * rows * v.nh_pad;
+    const int64_t lmo = v.lm_off[m];
+    const int jstart = (v.j0[m] / BK) * BK;
     const int t = threadIdx.x;
     const int tx = t % 16, ty = t / 16;
-
     const int a_i = t / 2, a_j = (t % 2) * 4;     // 64 rows x 8 rings: one float4 per thread
-    const int b_k = t % 64, b_j0 = t / 64;       // 4 complex per thread
+    const int b_k = t % (BN / 2), b_j0 = t / (BN / 2);
+    constexpr int BSTEP = NT / (BN / 2);
 
-    float acc[8][8];
+    float acc[8][TN];
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[r][c] = 0.f;
+        for (int c = 0; c < TN; ++c) acc[r][c] = 0.f;
 
-    auto load_tiles = [&](int jc, float4& ra, float2 (&rb)[4]) {
+    auto load_tiles = [&](int jc, float4& ra, float2 (&rb)[NB]) {
         const int i = i_base + a_i;
-        ra = (i < rows && jc < nh) ? *reinterpret_cast<const float4*>(L + (int64_t)i * nh_pad + jc + a_j)
-                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+        ra = (i < rows && jc < v.nh) ? *reinterpret_cast<const float4*>(L + (int64_t)i * v.nh_pad + jc + a_j)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
         const int k = kt0 + b_k;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int j = jc + b_j0 + 2 * q;
-            float2 v = make_float2(0.f, 0.f);
-            if (j < nh && k < K) {
-                const RingDesc& rd = rings[j];
-                if (m <= rd.mt) v = four[((rd.gofs + m) * 2 + par) * K + k];
+        for (int q = 0; q < NB; ++q) {
+            const int j = jc + b_j0 + BSTEP * q;
+            float2 x = make_float2(0.f, 0.f);
+            if (j < v.nh && k < v.K) {
+                const RingDesc& rd = v.rings[j];
+                if (m <= rd.mt) x = v.four[((rd.gofs + m) * 2 + par) * v.K + k];
             }
-            rb[q] = v;
+            rb[q] = x;
         }
     };
-    auto store_tiles = [&](int buf, const float4& ra, const float2 (&rb)[4]) {
+    auto store_tiles = [&](int buf, const float4& ra, const float2 (&rb)[NB]) {
         As[buf][a_j + 0][a_i] = ra.x;
         As[buf][a_j + 1][a_i] = ra.y;
         As[buf][a_j + 2][a_i] = ra.z;
         As[buf][a_j + 3][a_i] = ra.w;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) *reinterpret_cast<float2*>(&Bs[buf][b_j0 + 2 * q][2 * b_k]) = rb[q];
+        for (int q = 0; q < NB; ++q) *reinterpret_cast<float2*>(&Bs[buf][b_j0 + BSTEP * q][2 * b_k]) = rb[q];
     };
 
     float4 ra;
-    float2 rb[4];
+    float2 rb[NB];
+    __syncthreads();
     load_tiles(jstart, ra, rb);
     store_tiles(0, ra, rb);
     __syncthreads();
     int buf = 0;
-    for (int jc = jstart; jc < nh; jc += BK) {
-        const bool more = jc + BK < nh;
+    for (int jc = jstart; jc < v.nh; jc += BK) {
+        const bool more = jc + BK < v.nh;
         if (more) load_tiles(jc + BK, ra, rb);
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
-            const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][32 + ty * 4]);
-            const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
-            const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][kk][64 + tx * 4]);
-            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-#pragma unroll
-                for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
-        }
+        mma_step<BN>(As[buf], Bs[buf], tx, ty, acc);
         if (more) {
             store_tiles(buf ^ 1, ra, rb);
             __syncthreads();
@@ -199,57 +231,148 @@ __global__ void __launch_bounds__(NT) legendre_analysis_fp32_kernel(
     for (int r = 0; r < 8; ++r) {
         const int i = i_base + (r < 4 ? ty * 4 + r : 32 + ty * 4 + (r - 4));
         const int l = m + 2 * i + par;
-        if (i >= rows || l >= lmax) continue;
+        if (i >= rows || l >= v.lmax) continue;
 #pragma unroll
-        for (int cp = 0; cp < 4; ++cp) {
-            const int col = (cp < 2 ? tx * 4 + 2 * cp : 64 + tx * 4 + 2 * (cp - 2));
-            const int k = kt0 + col / 2;
-            if (k >= K) continue;
-            float2* dst = coeffs + (int64_t)k * ldc + lmo + 2 * i + par;
-            float2 v = make_float2(acc[r][2 * cp], acc[r][2 * cp + 1]);
-            if (add) {
+        for (int c = 0; c < TN; c += 2) {
+            const int k = kt0 + col_of<BN>(tx, c) / 2;
+            if (k >= v.K) continue;
+            float2* dst = v.cout + (int64_t)k * v.ldc + lmo + 2 * i + par;
+            float2 x = make_float2(acc[r][c], acc[r][c + 1]);
+            if (v.add) {
                 const float2 o = *dst;
-                v.x += o.x;
-                v.y += o.y;
+                x.x += o.x;
+                x.y += o.y;
             }
-            *dst = v;
+            *dst = x;
         }
     }
-    (void)nh_pad;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(NT) legendre_synthesis_fp32_kernel(const LegItem* __restrict__ items,
+                                                                     const LegView v) {
+    __shared__ __align__(16) float As[2][BK][BM];
+    __shared__ __align__(16) float Bs[2][BK][BN];
+    const LegItem it = items[blockIdx.x];
+    syn_tile<BN>(v, it.m, it.tile, blockIdx.y, blockIdx.z, As, Bs);
+}
+
+template <int BN>
+__global__ void __launch_bounds__(NT) legendre_analysis_fp32_kernel(const LegItem* __restrict__ items,
+                                                                    const LegView v) {
+    __shared__ __align__(16) float As[2][BK][BM];
+    __shared__ __align__(16) float Bs[2][BK][BN];
+    const LegItem it = items[blockIdx.x];
+    ana_tile<BN>(v, it.m, it.tile, blockIdx.y, blockIdx.z, As, Bs);
+}
+
+// Persistent grouped launch over the tiles of many transforms: CTA b takes the items
+// b, b + gridDim.x, ... of the batch's list (task, m, tile, column tile, parity).
+template <int BN>
+__global__ void __launch_bounds__(NT) legendre_grouped_kernel(const LegView* __restrict__ views,
+                                                              const GroupItem* __restrict__ items, int nitems,
+                                                              int synthesis) {
+    __shared__ __align__(16) float As[2][BK][BM];
+    __shared__ __align__(16) float Bs[2][BK][BN];
+    for (int ix = blockIdx.x; ix < nitems; ix += gridDim.x) {
+        const GroupItem it = items[ix];
+        const LegView& v = views[it.task];
+        if (synthesis)
+            syn_tile<BN>(v, it.a, it.b, it.c >> 1, it.c & 1, As, Bs);
+        else
+            ana_tile<BN>(v, it.a, it.b, it.c >> 1, it.c & 1, As, Bs);
+    }
+}
+
+template <int BN>
+cudaError_t launch_syn(const Plan& p, const LegView& v, cudaStream_t s) {
+    dim3 g(p.n_syn_items, (2 * v.K + BN - 1) / BN, 2);
+    legendre_synthesis_fp32_kernel<BN><<<g, NT, 0, s>>>(p.d_syn_items, v);
+    return cudaGetLastError();
+}
+template <int BN>
+cudaError_t launch_ana(const Plan& p, const LegView& v, const LegItem* items, int nitems, cudaStream_t s) {
+    dim3 g(nitems, (2 * v.K + BN - 1) / BN, 2);
+    legendre_analysis_fp32_kernel<BN><<<g, NT, 0, s>>>(items, v);
+    return cudaGetLastError();
 }
 
 }  // namespace
 
+LegView leg_view(const Plan& p, const float2* cin, float2* cout, int64_t ldc, const float2* four, int K, bool add) {
+    LegView v{};
+    v.lam = p.d_lam;
+    v.lam_off = p.d_lam_off;
+    v.rows = p.d_rows;
+    v.j0 = p.d_j0;
+    v.lm_off = p.d_lm_off;
+    v.rings = p.d_rings;
+    v.nh = p.nh;
+    v.nh_pad = p.nh_pad;
+    v.lmax = p.lmax;
+    v.cin = cin;
+    v.cout = cout;
+    v.ldc = ldc;
+    v.four = const_cast<float2*>(four);
+    v.K = K;
+    v.add = add ? 1 : 0;
+    return v;
+}
+
 cudaError_t launch_legendre_synthesis_fp32(const Plan& p, const float2* coeffs, int64_t ldc, int K, cudaStream_t s) {
-    if (p.n_syn_items == 0) return cudaSuccess;
-    dim3 g(p.n_syn_items, (2 * K + BN - 1) / BN, 2);
-    legendre_synthesis_fp32_kernel<<<g, NT, 0, s>>>(p.d_syn_items, p.d_lam, p.d_lam_off, p.d_rows, p.d_lm_off,
-                                                    p.d_rings, p.nh, p.nh_pad, p.lmax, coeffs, ldc, p.d_four, K);
-    return cudaGetLastError();
+    if (p.n_syn_items == 0 || K == 0) return cudaSuccess;
+    const LegView v = leg_view(p, coeffs, nullptr, ldc, p.d_four, K, false);
+    switch (p.leg_bn_syn) {
+        case 32: return launch_syn<32>(p, v, s);
+        case 64: return launch_syn<64>(p, v, s);
+        default: return launch_syn<128>(p, v, s);
+    }
 }
 
 cudaError_t launch_legendre_analysis_fp32(const Plan& p, float2* coeffs, int64_t ldc, int K, bool add,
                                           cudaStream_t s) {
-    if (p.n_ana_items == 0) return cudaSuccess;
-    dim3 g(p.n_ana_items, (2 * K + BN - 1) / BN, 2);
-    legendre_analysis_fp32_kernel<<<g, NT, 0, s>>>(p.d_ana_items, p.d_lam, p.d_lam_off, p.d_rows, p.d_j0,
-                                                   p.d_lm_off, p.d_rings, p.nh, p.nh_pad, p.lmax, p.d_four, coeffs,
-                                                   ldc, K, add ? 1 : 0);
-    return cudaGetLastError();
+    return launch_legendre_analysis_fp32_from(p, p.d_four, coeffs, ldc, K, add, s);
 }
 
-}  // namespace sht
-
-namespace sht {
 // The FP32 Legendre analysis reading the Fourier coefficients from a caller-chosen
-// scratch (used by the static-scratch analysis entry point).
+// scratch (the static-scratch analysis entry point uses it).
 cudaError_t launch_legendre_analysis_fp32_from(const Plan& p, const float2* scratch, float2* coeffs, int64_t ldc,
                                                int K, bool add, cudaStream_t s) {
-    if (p.n_ana_items == 0) return cudaSuccess;
-    dim3 g(p.n_ana_items, (2 * K + BN - 1) / BN, 2);
-    legendre_analysis_fp32_kernel<<<g, NT, 0, s>>>(p.d_ana_items, p.d_lam, p.d_lam_off, p.d_rows, p.d_j0, p.d_lm_off,
-                                                   p.d_rings, p.nh, p.nh_pad, p.lmax, scratch, coeffs, ldc, K,
-                                                   add ? 1 : 0);
+    if (p.n_ana_items == 0 || K == 0) return cudaSuccess;
+    const LegView v = leg_view(p, nullptr, coeffs, ldc, scratch, K, add);
+    switch (p.leg_bn_ana) {
+        case 32: return launch_ana<32>(p, v, p.d_ana_items, p.n_ana_items, s);
+        case 64: return launch_ana<64>(p, v, p.d_ana_items, p.n_ana_items, s);
+        default: return launch_ana<128>(p, v, p.d_ana_items, p.n_ana_items, s);
+    }
+}
+
+// Persistent grid of the grouped launch per tile width (32, 64, 128): the SMs times
+// the CTAs that fit on one.
+cudaError_t legendre_grouped_grids(int nsm, int (&grid)[3]) {
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, legendre_grouped_kernel<32>, NT, 0);
+    if (e != cudaSuccess) return e;
+    grid[0] = nsm * std::max(1, occ);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, legendre_grouped_kernel<64>, NT, 0)) != cudaSuccess)
+        return e;
+    grid[1] = nsm * std::max(1, occ);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, legendre_grouped_kernel<128>, NT, 0)) != cudaSuccess)
+        return e;
+    grid[2] = nsm * std::max(1, occ);
+    return cudaSuccess;
+}
+
+cudaError_t launch_legendre_grouped(const LegView* views, const GroupItem* items, int nitems, int bn, bool synthesis,
+                                    int grid, cudaStream_t s) {
+    if (nitems == 0) return cudaSuccess;
+    const int g = std::max(1, std::min(nitems, grid));
+    switch (bn) {
+        case 32: legendre_grouped_kernel<32><<<g, NT, 0, s>>>(views, items, nitems, synthesis ? 1 : 0); break;
+        case 64: legendre_grouped_kernel<64><<<g, NT, 0, s>>>(views, items, nitems, synthesis ? 1 : 0); break;
+        default: legendre_grouped_kernel<128><<<g, NT, 0, s>>>(views, items, nitems, synthesis ? 1 : 0); break;
+    }
     return cudaGetLastError();
 }
+
 }  // namespace sht

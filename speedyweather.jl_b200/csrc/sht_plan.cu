@@ -392,6 +392,16 @@ int build_plan(Plan& p) {
                      [](const std::pair<double, int2>& a, const std::pair<double, int2>& b) { return a.first > b.first; });
     std::vector<int2> fft_items;
     for (auto& f : fitems) fft_items.push_back(f.second);
+    p.h_rings = rings;
+    p.h_ring_cost.assign(nh, 0.0);
+    for (int j = 0; j < nh; ++j) {
+        const RingDesc& r = rings[j];
+        double per_layer = 4.0 * r.n;
+        for (int s2 = 0; s2 < r.nfac; ++s2)
+            per_layer += r.fac[s2] > 8 ? 2.0 * r.n * ((r.fac[s2] - 1) / 2 + kPrimeGroup - 1) / kPrimeGroup * kPrimeGroup
+                                       : 3.0 * r.n;
+        p.h_ring_cost[j] = per_layer;
+    }
 
     // --- work lists of the Legendre kernels (64-row tiles, heavy orders first) ---
     std::vector<LegItem> syn, ana;
@@ -461,6 +471,8 @@ int build_plan(Plan& p) {
     p.n_syn_items = (int)syn.size();
     p.n_ana_items = (int)ana.size();
     p.n_fft_items = (int)fft_items.size();
+    p.h_syn_items = syn;
+    p.h_ana_items = ana;
     p.table_bytes = tb;
 
     p.four_elems = p.scratch_rows * 2 * std::max(1, d.nlayers);
@@ -585,6 +597,55 @@ int sht_plan_tables(const sht_plan* plan, double* latd, double* weights, int32_t
     if (weights) std::memcpy(weights, p.weights.data(), p.nlat * sizeof(double));
     if (nlons) std::memcpy(nlons, p.nlons.data(), p.nlat * sizeof(int32_t));
     if (mmax_truncation) std::memcpy(mmax_truncation, p.mt.data(), p.nh * sizeof(int32_t));
+    return SHT_OK;
+}
+
+int sht_plan_autotune(sht_plan* plan, int K, void* stream, int32_t* tile_columns) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_plan_autotune")) != SHT_OK) return rc;
+    if (tile_columns) tile_columns[0] = tile_columns[1] = 0;
+    Plan& p = plan->p;
+    if (p.d.precision != SHT_PREC_FP32 || K == 0) return SHT_OK;
+    DeviceGuard g(p.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    float2* c = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&c, p.nlm * K * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c, 0, p.nlm * K * sizeof(float2), s);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    int best[2] = {p.leg_bn_syn, p.leg_bn_ana};
+    for (int dir = 0; dir < 2 && e == cudaSuccess; ++dir) {
+        float best_ms = 1e30f;
+        for (int bn : {32, 64, 128}) {
+            (dir == 0 ? p.leg_bn_syn : p.leg_bn_ana) = bn;
+            auto launch = [&]() {
+                return dir == 0 ? launch_legendre_synthesis_fp32(p, c, p.nlm, K, s)
+                                : launch_legendre_analysis_fp32(p, c, p.nlm, K, false, s);
+            };
+            for (int w = 0; w < 2 && e == cudaSuccess; ++w) e = launch();
+            if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+            for (int r = 0; r < 5 && e == cudaSuccess; ++r) e = launch();
+            if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && ms < best_ms) {
+                best_ms = ms;
+                best[dir] = bn;
+            }
+        }
+    }
+    p.leg_bn_syn = best[0];
+    p.leg_bn_ana = best[1];
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (c) cudaFree(c);
+    if (e != cudaSuccess) return cuda_fail(e, "sht_plan_autotune");
+    if (tile_columns) {
+        tile_columns[0] = best[0];
+        tile_columns[1] = best[1];
+    }
     return SHT_OK;
 }
 

@@ -10,12 +10,14 @@ SpeedyTransforms/src/spectral_gradients.jl) over the C ABI of libsht.so:
   ``transform(in, S)`` allocates;
 * operators ``curl_``, ``divergence_``, ``UV_from_vor_``, ``UV_from_vordiv_``,
   ``laplace_`` (``∇²!``), ``inverse_laplace_`` (``∇⁻²!``), ``gradient_`` (``∇!``)
-  and their allocating forms.
+  and their allocating forms;
+* ``Batch`` -- many transforms in one grouped launch per stage, CUDA-graph capture.
 
 Every compute call runs the CUDA kernels of libsht; there is no CPU path.
 """
 from ._lib import DimensionMismatch, ShtError  # noqa: F401
 from .core import (  # noqa: F401
+    Batch,
     Field,
     FullGaussianGrid,
     LowerTriangularArray,

@@ -16,6 +16,7 @@ GRID_FULL_GAUSSIAN, GRID_OCTAHEDRAL_GAUSSIAN = 0, 1
 PREC_FP32, PREC_BF16X3, PREC_FP16X3, PREC_BF16X5 = 0, 1, 2, 3
 SHORTCUTS = {"linear": 0, "quadratic": 1, "cubic": 2, "linquadcoslat2": 3, "lincubcoslat": 4}
 UNSCALE_COSLAT, ADD, FLIPSIGN, INVERSE = 1, 2, 4, 8
+SYNTHESIS, ANALYSIS = 0, 1
 
 
 class ShtDesc(C.Structure):
@@ -28,6 +29,11 @@ class ShtInfo(C.Structure):
                 ("nlon_max", C.c_int32), ("nfreq_max", C.c_int32), ("lmax", C.c_int32), ("mmax", C.c_int32),
                 ("nlayers", C.c_int32), ("precision", C.c_int32), ("scratch_bytes", C.c_int64),
                 ("table_bytes", C.c_int64)]
+
+
+class ShtBatchItem(C.Structure):
+    _fields_ = [("plan", C.c_void_p), ("direction", C.c_int), ("coeffs", C.c_void_p), ("ldc", C.c_int64),
+                ("grid", C.c_void_p), ("ldg", C.c_int64), ("nlayers", C.c_int), ("flags", C.c_uint)]
 
 
 # name -> (restype, argtypes); every symbol the header declares
@@ -52,6 +58,14 @@ SIGNATURES = {
     "sht_gradient": (C.c_int, [_P, _P, _P, _P, _I64, C.c_int, C.c_double, _P]),
     "sht_device_status": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "sht_analyze_static_scratch": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
+    "sht_plan_autotune": (C.c_int, [_P, C.c_int, _P, C.POINTER(C.c_int32)]),
+    "sht_batch_create": (C.c_int, [C.POINTER(ShtBatchItem), C.c_int, C.POINTER(C.c_void_p)]),
+    "sht_batch_run": (C.c_int, [_P, _P]),
+    "sht_batch_run_each": (C.c_int, [_P, _P]),
+    "sht_batch_capture": (C.c_int, [_P, _P]),
+    "sht_batch_launch": (C.c_int, [_P, _P]),
+    "sht_batch_autotune": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
+    "sht_batch_destroy": (C.c_int, [_P]),
     "sht_last_error": (C.c_char_p, []),
     "sht_version": (C.c_char_p, []),
 }

@@ -312,9 +312,82 @@ class SpectralTransform:
         check(lib.sht_device_status(self._plan, C.byref(v)))
         return int(v.value)
 
+    def autotune(self, nlayers: int | None = None):
+        """Time the FP32 Legendre kernels at ``nlayers`` layers for each tile width and
+        keep the fastest per direction (results are bitwise independent of the choice).
+        Returns (synthesis, analysis) tile widths; (0, 0) for tensor-core plans."""
+        cols = (C.c_int32 * 2)()
+        check(lib.sht_plan_autotune(self._plan, int(nlayers or self.nlayers), _stream_ptr(self.device), cols))
+        return int(cols[0]), int(cols[1])
+
     def __repr__(self):
         return (f"SpectralTransform({self.spectrum}, {self.grid}, nlayers={self.nlayers}, "
                 f"precision={self.precision!r})")
+
+
+class Batch:
+    """Many transforms in one grouped launch per stage (sht_batch_*): all syntheses,
+    then all analyses, each item with its own scratch.
+
+    ``Batch([(out, in, S, flags...), ...])`` where each entry is
+    ``(Field, LowerTriangularArray, S)`` for a synthesis or
+    ``(LowerTriangularArray, Field, S)`` for an analysis, optionally followed by a dict
+    ``{"unscale_coslat": bool, "add": bool}``. The arrays are bound at construction.
+    ``run()`` launches the grouped kernels, ``run_each()`` the same transforms one call
+    each, ``capture()``/``launch()`` a CUDA graph of ``run()``, ``autotune()`` picks the
+    Legendre tile width. FP32 plans.
+    """
+
+    def __init__(self, entries):
+        items = (_lib.ShtBatchItem * len(entries))()
+        self._keep = []
+        self.device = None
+        for i, e in enumerate(entries):
+            out, inp, S = e[0], e[1], e[2]
+            opts = e[3] if len(e) > 3 else {}
+            if isinstance(out, Field) and isinstance(inp, LowerTriangularArray):
+                ldg, K = _field_arg(out, S, "field")
+                ldc, K2 = _coeff_arg(inp, S, "coeffs")
+                _check_k(S, K, K2)
+                flags = (_lib.UNSCALE_COSLAT if opts.get("unscale_coslat") else 0) | (_lib.ADD if opts.get("add") else 0)
+                items[i] = _lib.ShtBatchItem(S.handle.value, _lib.SYNTHESIS, inp.data.data_ptr(), ldc,
+                                             out.data.data_ptr(), ldg, K, flags)
+            elif isinstance(out, LowerTriangularArray) and isinstance(inp, Field):
+                ldc, K = _coeff_arg(out, S, "coeffs")
+                ldg, K2 = _field_arg(inp, S, "field")
+                _check_k(S, K, K2)
+                items[i] = _lib.ShtBatchItem(S.handle.value, _lib.ANALYSIS, out.data.data_ptr(), ldc,
+                                             inp.data.data_ptr(), ldg, K, _lib.ADD if opts.get("add") else 0)
+            else:
+                raise TypeError("batch entries are (Field, LowerTriangularArray, S) or (LowerTriangularArray, Field, S)")
+            self._keep += [out, inp, S]
+            self.device = S.device
+        h = C.c_void_p()
+        self._b = None
+        check(lib.sht_batch_create(items, len(entries), C.byref(h)))
+        self._b = h
+
+    def run(self):
+        check(lib.sht_batch_run(self._b, _stream_ptr(self.device)))
+
+    def run_each(self):
+        check(lib.sht_batch_run_each(self._b, _stream_ptr(self.device)))
+
+    def capture(self):
+        check(lib.sht_batch_capture(self._b, _stream_ptr(self.device)))
+
+    def launch(self):
+        check(lib.sht_batch_launch(self._b, _stream_ptr(self.device)))
+
+    def autotune(self) -> int:
+        v = C.c_int32(0)
+        check(lib.sht_batch_autotune(self._b, _stream_ptr(self.device), C.byref(v)))
+        return int(v.value)
+
+    def __del__(self):
+        if getattr(self, "_b", None) is not None:
+            lib.sht_batch_destroy(self._b)
+            self._b = None
 
 
 # ------------------------------------------------------------------------------------------
