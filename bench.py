@@ -254,6 +254,62 @@ def time_stages(S, lt, field, out, reps):
     return res
 
 
+MIX = [(32, 24, 1), (64, 48, 8), (128, 96, 16), (256, 192, 64)]   # (T + 1, nlat_half, layers)
+
+
+def run_mixed_batch(args):
+    """The batching workload: octahedral T31 / T63 / T127 / T255 (nlat 48 / 96 / 192 / 384)
+    with 1 / 8 / 16 / 64 layers, FP32, each synthesised then analysed. One step = the
+    whole batch. Timed three ways with CUDA events: one sht_synthesize / sht_analyze
+    call per transform (16 kernel launches), the grouped persistent launches (4), and
+    their CUDA graph (1 graph launch). Prints one JSON line (not the headline metric)."""
+    import torch
+    import speedytransforms as st
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sht_oracle as O
+    device = torch.device("cuda", 0)
+    entries = []
+    for T_, nh, K in MIX:
+        S = st.SpectralTransform(st.Spectrum(T_, T_), st.OctahedralGaussianGrid(nh), nlayers=K, precision="fp32",
+                                 device=device)
+        c = O.random_coeffs(O.Spectrum(T_, T_), K, seed=T_)
+        lt = st.LowerTriangularArray(torch.tensor(np.ascontiguousarray(c.T), dtype=torch.complex64).to(device),
+                                     S.spectrum)
+        f = st.Field.zeros(S.grid, K, device=device)
+        a = st.LowerTriangularArray.zeros(S.spectrum, K, device=device)
+        entries += [(f, lt, S), (a, f, S)]
+    b = st.Batch(entries)
+    bn = b.autotune()
+    b.capture()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / args.steps
+
+    t_each = timed(b.run_each)
+    t_grouped = timed(b.run)
+    t_graph = timed(b.launch)
+    line = {"metric": "mixed-batch round trips/s (octahedral T31 K1 + T63 K8 + T127 K16 + T255 K64, FP32)",
+            "value": 1.0 / t_graph, "unit": "batches/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_graph * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": "mixed batch of 4 round trips, one grouped launch per stage, CUDA graph",
+                       "legendre_tile_columns": bn},
+            "ms_per_batch": {"one_call_per_transform": t_each * 1e3, "grouped_launches": t_grouped * 1e3,
+                             "grouped_graph": t_graph * 1e3},
+            "gpu_launches_per_batch": {"one_call_per_transform": 16, "grouped_launches": 4, "grouped_graph": 4}}
+    print(json.dumps(line))
+    return 0
+
+
 def profile_run(args):
     """W + K round trips of one precision at the benchmark workload and nothing else:
     the command ncu wraps for the launch list and the per-kernel captures."""
@@ -443,6 +499,8 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3", "fp16x3", "bf16x5"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="t511", choices=["t511", "mixed-batch"],
+                    help="t511: the headline benchmark; mixed-batch: the grouped-launch comparison")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W + K round trips of one precision (default bf16x3), for profilers")
     ap.add_argument("--ref-sample-layers", type=int, default=16)
@@ -452,6 +510,8 @@ def main():
         return run_reference(args)
     if args.profile_run:
         return profile_run(args)
+    if args.workload == "mixed-batch":
+        return run_mixed_batch(args)
     return run_ours(args)
 
 

@@ -182,6 +182,24 @@ SHT_API int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p, 
 SHT_API int sht_analyze_static_scratch(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, int64_t ldc,
                                        int K, unsigned flags, void* stream);
 
+/* Adjoints (vector-Jacobian products) of the two transforms, for training through them.
+ * replaces the reverse rules of SpeedyTransforms/ext/SpeedyTransformsEnzymeExt.jl:263-323
+ * (spec2grid_pullback!, grid2spec_pullback!): the adjoint of the synthesis is the
+ * analysis with each Fourier coefficient of order m weighted by the rfft adjoint scale
+ * (1 for m = 0 and the Nyquist frequency, 2 otherwise; :33-57) instead of the solid
+ * angle (and by 1 / cos(lat) if the synthesis unscaled); the adjoint of the analysis is
+ * the synthesis with the Fourier coefficients weighted by solid angle / that scale.
+ * Adjoint with respect to the real inner products of the Float32 storage (re and im of
+ * each coefficient separately). The reference always accumulates (add = true); here
+ * SHT_ADD accumulates and its absence overwrites.
+ * sht_synthesize_adjoint: coeffs_bar (+)= S_syn^T grid_bar; flags SHT_UNSCALE_COSLAT (as in
+ * the primal synthesis), SHT_ADD. sht_analyze_adjoint: grid_bar (+)= S_ana^T coeffs_bar;
+ * flags SHT_ADD. Both use the plan's Legendre arithmetic. */
+SHT_API int sht_synthesize_adjoint(sht_plan* plan, const float* grid_bar, int64_t ldg, void* coeffs_bar, int64_t ldc,
+                                   int K, unsigned flags, void* stream);
+SHT_API int sht_analyze_adjoint(sht_plan* plan, const void* coeffs_bar, int64_t ldc, float* grid_bar, int64_t ldg,
+                                int K, unsigned flags, void* stream);
+
 /* Autotuner of a plan's own launches: times the FP32 Legendre kernels of an
  * SHT_PREC_FP32 plan at K layers for each tile width (32, 64, 128 real columns) on
  * scratch buffers it allocates, keeps the fastest per direction for later calls, and

@@ -370,6 +370,52 @@ class SpectralTransform:
         return out[:, 0] if squeeze else out
 
 
+    # --- adjoints (SpeedyTransforms/ext/SpeedyTransformsEnzymeExt.jl) ----------------
+    def adjoint_scale(self):
+        """rfft adjoint scale [nh, nfreq_max] (SpeedyTransformsEnzymeExt.jl:33-57): 1 for
+        m = 0 and, for even n, the Nyquist frequency; 2 otherwise; 0 beyond the ring's."""
+        nh = self.grid.nlat_half
+        sc = np.zeros((nh, self.nfreq_max))
+        for j in range(nh):
+            n = int(self.grid.nlons[j])
+            nf = n // 2 + 1
+            s = np.full(nf, 2.0)
+            s[0] = 1.0
+            if n % 2 == 0:
+                s[nf - 1] = 1.0
+            sc[j, :nf] = s
+        return sc
+
+    def synthesize_adjoint(self, field_bar, unscale_coslat=False):
+        """spec2grid_pullback! (SpeedyTransformsEnzymeExt.jl:263-289): forward FFT, times
+        the adjoint scale (and 1/cos lat), divided by the solid angle that the forward
+        Legendre applies, then the forward Legendre."""
+        field_bar = np.asarray(field_bar, dtype=np.float64)
+        squeeze = field_bar.ndim == 1
+        if squeeze:
+            field_bar = field_bar[:, None]
+        nh = self.grid.nlat_half
+        fN, fS = self.fourier_analysis(field_bar)
+        f = self.adjoint_scale()[:, :, None] / self.solid_angles[:nh, None, None]
+        if unscale_coslat:
+            f = f / self.coslat[:nh, None, None]
+        out = self.legendre_analysis(fN * f, fS * f)
+        return out[:, 0] if squeeze else out
+
+    def analyze_adjoint(self, coeffs_bar):
+        """grid2spec_pullback! (SpeedyTransformsEnzymeExt.jl:294-323): inverse Legendre,
+        times the solid angle, divided by the adjoint scale, then the inverse FFT."""
+        coeffs_bar = np.asarray(coeffs_bar, dtype=np.complex128)
+        squeeze = coeffs_bar.ndim == 1
+        if squeeze:
+            coeffs_bar = coeffs_bar[:, None]
+        nh = self.grid.nlat_half
+        gN, gS = self.legendre_synthesis(coeffs_bar)
+        sc = self.adjoint_scale()
+        f = np.where(sc > 0, self.solid_angles[:nh, None] / np.where(sc > 0, sc, 1.0), 0.0)[:, :, None]
+        out = self.fourier_synthesis(gN * f, gS * f)
+        return out[:, 0] if squeeze else out
+
 # ----------------------------------------------------------------------------------------
 # gradient arrays (gradient_arrays.jl) -- all indexed by packed lm, 0-based l, m
 # ----------------------------------------------------------------------------------------

@@ -187,7 +187,7 @@ int sht_batch_create(const sht_batch_item* items, int nitems, sht_batch** out) {
         lv[t] = leg_view(p, syn ? (const float2*)it.coeffs : nullptr, syn ? nullptr : (float2*)it.coeffs, it.ldc,
                          b->scratch[t], it.nlayers, !syn && (it.flags & SHT_ADD));
         fv[t] = fft_view(p, syn ? nullptr : it.grid, syn ? it.grid : nullptr, it.ldg, b->scratch[t], it.nlayers,
-                         syn ? it.flags : 0u, false);
+                         syn ? it.flags : 0u, false, false);
         b->fft_smem = std::max(b->fft_smem, p.smem_fft);
     }
     if (e == cudaSuccess) e = cudaMalloc(&b->d_leg, nitems * sizeof(LegView));

@@ -92,12 +92,14 @@ __device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P]) 
         float2 e[4], o[4];
         dft4<INV>(v[0], v[2], v[4], v[6], e[0], e[1], e[2], e[3]);
         dft4<INV>(v[1], v[3], v[5], v[7], o[0], o[1], o[2], o[3]);
+        // (products rounded on their own: no contraction into the following sums, so
+        // every kernel instantiating this gives the same bits)
         constexpr float h = 0.7071067811865476f;
-        const float2 o1 = INV ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
-                              : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+        const float2 o1 = INV ? make_float2(__fmul_rn(h, o[1].x - o[1].y), __fmul_rn(h, o[1].x + o[1].y))
+                              : make_float2(__fmul_rn(h, o[1].x + o[1].y), __fmul_rn(h, o[1].y - o[1].x));
         const float2 o2 = INV ? make_float2(-o[2].y, o[2].x) : make_float2(o[2].y, -o[2].x);
-        const float2 o3 = INV ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
-                              : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+        const float2 o3 = INV ? make_float2(__fmul_rn(-h, o[3].x + o[3].y), __fmul_rn(h, o[3].x - o[3].y))
+                              : make_float2(__fmul_rn(h, o[3].y - o[3].x), __fmul_rn(-h, o[3].x + o[3].y));
         y[0] = cadd(e[0], o[0]);
         y[4] = csub(e[0], o[0]);
         y[1] = cadd(e[1], o1);
@@ -506,6 +508,23 @@ __device__ __forceinline__ void put_pieces(uint8_t* dst, int64_t piece_stride, c
 // shared memory: W (n twiddles, padded to even) | G (prime tables) | X (C ldx) | Y (C ldx);
 // ldx >= n is the padded layer stride
 
+// Weight of order m in the analysis epilogue, times (2 F_N +- 2 F_S): the solid angle
+// / 2 for the transform; for the adjoint of the synthesis the rfft adjoint scale
+// (1 for m = 0 and the Nyquist frequency, 2 otherwise; SpeedyTransformsEnzymeExt.jl:33-57)
+// / 2, times 1/cos(lat) when the synthesis unscaled by it.
+__device__ __forceinline__ float ana_weight(const RingDesc& rd, int m, int adjoint, int unscale) {
+    if (!adjoint) return 0.5f * rd.domega;
+    const float sm = (m == 0 || 2 * m == rd.n) ? 1.f : 2.f;
+    return 0.5f * sm * (unscale ? rd.coslat_inv : 1.f);
+}
+// Factor of the Fourier coefficients of order m in the synthesis prologue: 1 / cos(lat)
+// or 1 for the transform; for the adjoint of the analysis the solid angle / the rfft
+// adjoint scale (SpeedyTransformsEnzymeExt.jl:294-323).
+__device__ __forceinline__ float syn_weight(const RingDesc& rd, int m, int adjoint, int unscale) {
+    if (!adjoint) return unscale ? rd.coslat_inv : 1.f;
+    return (m == 0 || 2 * m == rd.n) ? rd.domega : 0.5f * rd.domega;
+}
+
 // grid -> Fourier scratch (E/O combinations weighted by the solid angle), one work
 // item (ring, layer chunk) of one transform
 __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2* sm) {
@@ -565,7 +584,7 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
     }
     __syncthreads();
     const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G);
-    const float half_domega = 0.5f * rd.domega;
+    const int adj = v.adjoint, unsc = v.unscale;
     const int nm = rd.mt + 1;
     if (img.base != nullptr) {
         // tensor-core operand: E (parity 0) and O (parity 1) split into 16-bit pieces,
@@ -592,11 +611,12 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
                     const float2 fn = make_float2(a.x + b.x, a.y - b.y);
                     const float2 fs = make_float2(a.y + b.y, b.x - a.x);
                     // fp16 pieces: the layer's data scale 2^(15 - e_k) folded into the weight
-                    const float hw = img.fp16 ? half_domega * img.kscale[k0 + kl].y : half_domega;
-                    ev[2 * t] = hw * (fn.x + fs.x);
-                    ev[2 * t + 1] = hw * (fn.y + fs.y);
-                    ov[2 * t] = hw * (fn.x - fs.x);
-                    ov[2 * t + 1] = hw * (fn.y - fs.y);
+                    const float w0 = ana_weight(rd, m, adj, unsc);
+                    const float hw = img.fp16 ? w0 * img.kscale[k0 + kl].y : w0;
+                    ev[2 * t] = __fmul_rn(hw, fn.x + fs.x);
+                    ev[2 * t + 1] = __fmul_rn(hw, fn.y + fs.y);
+                    ov[2 * t] = __fmul_rn(hw, fn.x - fs.x);
+                    ov[2 * t + 1] = __fmul_rn(hw, fn.y - fs.y);
                     mask |= 3u << (2 * t);
                 }
             }
@@ -630,8 +650,9 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
         // F_N = (a + conj b)/2, F_S = (a - conj b)/(2i)
         const float2 fn = make_float2(a.x + b.x, a.y - b.y);
         const float2 fs = make_float2(a.y + b.y, b.x - a.x);
-        const float2 e = make_float2(half_domega * (fn.x + fs.x), half_domega * (fn.y + fs.y));
-        const float2 o = make_float2(half_domega * (fn.x - fs.x), half_domega * (fn.y - fs.y));
+        const float hw = ana_weight(rd, m, adj, unsc);
+        const float2 e = make_float2(__fmul_rn(hw, fn.x + fs.x), __fmul_rn(hw, fn.y + fs.y));
+        const float2 o = make_float2(__fmul_rn(hw, fn.x - fs.x), __fmul_rn(hw, fn.y - fs.y));
         const int64_t row = (rd.gofs + m) * 2;
         four[row * K + k0 + c] = e;
         four[(row + 1) * K + k0 + c] = o;
@@ -676,7 +697,7 @@ __device__ void fft_synthesis_body(const FftView& v, int ring, int chunk, float2
     }
     cp_async_wait_all();
     __syncthreads();
-    const float scale = unscale ? rd.coslat_inv : 1.0f;
+    const int adj = v.adjoint;
     const int nhalf = n / 2;   // highest source frequency
     // layer fastest across the lanes (a warp reads whole runs of C layers of a scratch
     // row), four items per thread in flight: the scratch reads are the latency
@@ -707,8 +728,10 @@ __device__ void fft_synthesis_body(const FftView& v, int ring, int chunk, float2
             if (w >= tot) break;
             const int m = quo(w, dC);
             const int c = w - m * C;
-            const float2 gn = make_float2(scale * (e[u].x + o[u].x), scale * (e[u].y + o[u].y));
-            const float2 gs = make_float2(scale * (e[u].x - o[u].x), scale * (e[u].y - o[u].y));
+            const float scale = syn_weight(rd, m, adj, unscale);
+            // products rounded on their own (no contraction into the packing below)
+            const float2 gn = make_float2(__fmul_rn(scale, e[u].x + o[u].x), __fmul_rn(scale, e[u].y + o[u].y));
+            const float2 gs = make_float2(__fmul_rn(scale, e[u].x - o[u].x), __fmul_rn(scale, e[u].y - o[u].y));
             const bool selfconj = (m == 0) || (2 * m == n);
             if (selfconj) {
                 X[c * ldx + m] = make_float2(gn.x, gs.x);
@@ -758,7 +781,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_grouped_kernel
 static int fft_threads(const Plan&) { return kFftThreads; }
 
 FftView fft_view(const Plan& p, const float* gin, float* gout, int64_t ldg, float2* four, int K, unsigned flags,
-                 bool image) {
+                 bool image, bool adjoint) {
     FftView v{};
     v.rings = p.d_rings;
     v.twiddle = p.d_twiddle;
@@ -769,6 +792,7 @@ FftView fft_view(const Plan& p, const float* gin, float* gout, int64_t ldg, floa
     v.K = K;
     v.unscale = (flags & SHT_UNSCALE_COSLAT) ? 1 : 0;
     v.add = (flags & SHT_ADD) ? 1 : 0;
+    v.adjoint = adjoint ? 1 : 0;
     if (image) v.img = p.ana_img;
     return v;
 }
@@ -781,23 +805,29 @@ cudaError_t launch_fft_grouped(const FftView* views, const GroupItem* items, int
     return cudaGetLastError();
 }
 
-cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, bool to_image) {
+cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, bool to_image,
+                                unsigned flags, bool adjoint) {
     const dim3 g(p.n_fft_items);
-    const TcImage none{};
     if ((to_image || p.tc) && p.ana_img.fp16) {
-        const cudaError_t e = tc_analysis_scale(p, grid, ldg, K, s);
+        // bound of |E|, |O| per unit grid value: 4 pi max w (the transform: E = dOmega (F_N + F_S),
+        // |F| <= n max|f|) or, for the adjoint of the synthesis (E = s_m c (F_N + F_S), s_m <= 2),
+        // 4 nlon_max max(1 / cos lat)
+        const float mul = adjoint ? 4.0000005f * p.nlon_max * ((flags & SHT_UNSCALE_COSLAT) ? p.coslat_inv_max : 1.f)
+                                  : 0.f;
+        const cudaError_t e = tc_analysis_scale(p, grid, ldg, K, s, mul);
         if (e != cudaSuccess) return e;
     }
     fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(
-        p.d_fft_items, fft_view(p, grid, nullptr, ldg, p.d_four, K, 0, to_image || p.tc));
-    (void)none;
+        p.d_fft_items, fft_view(p, grid, nullptr, ldg, p.d_four, K, flags & SHT_UNSCALE_COSLAT, to_image || p.tc,
+                                adjoint));
     return cudaGetLastError();
 }
 
-cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags, cudaStream_t s) {
+cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags, cudaStream_t s,
+                                 bool adjoint) {
     const dim3 g(p.n_fft_items);
     fft_synthesis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(
-        p.d_fft_items, fft_view(p, nullptr, grid, ldg, p.d_four, K, flags, false));
+        p.d_fft_items, fft_view(p, nullptr, grid, ldg, p.d_four, K, flags, false, adjoint));
     return cudaGetLastError();
 }
 
@@ -828,7 +858,7 @@ cudaError_t launch_fft_analysis_to(const Plan& p, const float* grid, int64_t ldg
                                    cudaStream_t s) {
     const dim3 g(p.n_fft_items);
     fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(
-        p.d_fft_items, fft_view(p, grid, nullptr, ldg, scratch, K, 0, false));
+        p.d_fft_items, fft_view(p, grid, nullptr, ldg, scratch, K, 0, false, false));
     return cudaGetLastError();
 }
 }  // namespace sht

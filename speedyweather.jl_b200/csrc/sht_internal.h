@@ -95,12 +95,14 @@ struct FftView {
     int64_t ldg;
     float2* four;         // Fourier scratch
     int K, unscale, add;
+    int adjoint;          // 1: the adjoint weights (of the synthesis for the analysis direction and v.v.)
     TcImage img;          // analysis operand image of tensor-core plans (base == nullptr: FP32 scratch)
 };
 
 struct Plan {
     sht_desc d{};
     int nh = 0, nlat = 0, lmax = 0, mmax = 0, nlon_max = 0, nfreq_max = 0;
+    float coslat_inv_max = 1.f;         // max over rings of 1 / cos(latitude)
     int64_t npoints = 0, nlm = 0;
     int64_t scratch_rows = 0;           // sum_j (mt_j + 1)
     int device = 0;
@@ -161,14 +163,14 @@ enum GradIdx {
 
 // ---- launchers (return cudaError_t of the launch) ----------------------------------
 FftView fft_view(const Plan& p, const float* gin, float* gout, int64_t ldg, float2* four, int K, unsigned flags,
-                 bool image);
+                 bool image, bool adjoint);
 cudaError_t launch_fft_grouped(const FftView* views, const GroupItem* items, int nitems, bool synthesis, int smem,
                                int grid, cudaStream_t s);
-cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s);
+cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, float mul);
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s,
-                                bool to_image = false);
+                                bool to_image = false, unsigned flags = 0, bool adjoint = false);
 cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags,
-                                 cudaStream_t s);
+                                 cudaStream_t s, bool adjoint = false);
 LegView leg_view(const Plan& p, const float2* cin, float2* cout, int64_t ldc, const float2* four, int K, bool add);
 cudaError_t legendre_grouped_grids(int nsm, int (&grid)[3]);
 cudaError_t launch_legendre_grouped(const LegView* views, const GroupItem* items, int nitems, int bn, bool synthesis,

@@ -904,14 +904,15 @@ cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, in
     return cudaGetLastError();
 }
 
-cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t st) {
+// mul: bound of the analysis data per unit grid value; 0 = the transform's (4 pi max w)
+cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t st, float mul) {
     const TcState* s = static_cast<const TcState*>(p.tc);
     if (!s || !s->fp16 || K <= 0) return cudaSuccess;
     float* out = s->d_absmax + p.d.nlayers;
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * K, st);
     if (e != cudaSuccess) return e;
     absmax_kernel<<<dim3(std::max(1, 2 * s->nsm / std::max(1, K)) * 4, K), 256, 0, st>>>(grid, ldg, p.npoints, out);
-    kscale_kernel<<<1, 256, 0, st>>>(out, s->ana_mul, K, s->d_kscale + p.d.nlayers);
+    kscale_kernel<<<1, 256, 0, st>>>(out, mul > 0.f ? mul : s->ana_mul, K, s->d_kscale + p.d.nlayers);
     return cudaGetLastError();
 }
 

@@ -350,6 +350,7 @@ int build_plan(Plan& p) {
         r.gen_len = (int32_t)((int64_t)tw.size() - r.tw_off - ((r.n + 1) & ~1));
         r.domega = (float)(p.weights[j] * (2.0 * M_PI / r.n));                  // quadrature_weights.jl:48-49
         r.coslat_inv = (float)(1.0 / std::cos(p.latd[j] * M_PI / 180.0));       // spectral_transform.jl:150-151
+        p.coslat_inv_max = std::max(p.coslat_inv_max, r.coslat_inv);
         // shared memory of the FFT kernels: twiddles, prime tables and two buffers of
         // chunk x n complex
         const int tw_bytes = (((r.n + 1) & ~1) + r.gen_len) * 8;
@@ -731,6 +732,38 @@ int sht_analyze(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, in
     if (e != cudaSuccess) return cuda_fail(e, "sht_analyze (Fourier)");
     return finish(legendre_analysis(plan->p, (float2*)coeffs, ldc, K, (flags & SHT_ADD) != 0, s),
                   "sht_analyze (Legendre)");
+}
+
+int sht_synthesize_adjoint(sht_plan* plan, const float* grid_bar, int64_t ldg, void* coeffs_bar, int64_t ldc, int K,
+                           unsigned flags, void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_synthesize_adjoint")) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, "sht_synthesize_adjoint")) != SHT_OK) return rc;
+    if ((rc = check_ldg(plan->p, ldg, "sht_synthesize_adjoint")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(coeffs_bar) || !ok_ptr(grid_bar)) return fail(SHT_EINVAL, "sht_synthesize_adjoint: NULL array");
+    DeviceGuard g(plan->p.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = launch_fft_analysis(plan->p, grid_bar, ldg, K, s, false, flags & SHT_UNSCALE_COSLAT, true);
+    if (e != cudaSuccess) return cuda_fail(e, "sht_synthesize_adjoint (Fourier)");
+    return finish(legendre_analysis(plan->p, (float2*)coeffs_bar, ldc, K, (flags & SHT_ADD) != 0, s),
+                  "sht_synthesize_adjoint (Legendre)");
+}
+
+int sht_analyze_adjoint(sht_plan* plan, const void* coeffs_bar, int64_t ldc, float* grid_bar, int64_t ldg, int K,
+                        unsigned flags, void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_analyze_adjoint")) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, "sht_analyze_adjoint")) != SHT_OK) return rc;
+    if ((rc = check_ldg(plan->p, ldg, "sht_analyze_adjoint")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(coeffs_bar) || !ok_ptr(grid_bar)) return fail(SHT_EINVAL, "sht_analyze_adjoint: NULL array");
+    DeviceGuard g(plan->p.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = legendre_synthesis(plan->p, (const float2*)coeffs_bar, ldc, K, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sht_analyze_adjoint (Legendre)");
+    return finish(launch_fft_synthesis(plan->p, grid_bar, ldg, K, flags & SHT_ADD, s, true),
+                  "sht_analyze_adjoint (Fourier)");
 }
 
 static int ops_check(sht_plan* plan, int64_t ldc, int K, const char* what, std::initializer_list<const void*> ptrs) {

@@ -11,7 +11,8 @@ SpeedyTransforms/src/spectral_gradients.jl) over the C ABI of libsht.so:
 * operators ``curl_``, ``divergence_``, ``UV_from_vor_``, ``UV_from_vordiv_``,
   ``laplace_`` (``∇²!``), ``inverse_laplace_`` (``∇⁻²!``), ``gradient_`` (``∇!``)
   and their allocating forms;
-* ``Batch`` -- many transforms in one grouped launch per stage, CUDA-graph capture.
+* ``Batch`` -- many transforms in one grouped launch per stage, CUDA-graph capture;
+* ``spec2grid_pullback_``, ``grid2spec_pullback_`` -- the adjoints of the transforms.
 
 Every compute call runs the CUDA kernels of libsht; there is no CPU path.
 """
@@ -36,10 +37,12 @@ from .core import (  # noqa: F401
     get_truncation,
     gradient,
     gradient_,
+    grid2spec_pullback_,
     inverse_laplace,
     inverse_laplace_,
     laplace,
     laplace_,
+    spec2grid_pullback_,
     transform,
     transform_,
 )

@@ -425,6 +425,31 @@ def transform_(out, inp, S: SpectralTransform, *, unscale_coslat: bool = False, 
     raise TypeError("transform_(out, in, S) needs (Field, LowerTriangularArray) or (LowerTriangularArray, Field)")
 
 
+def spec2grid_pullback_(coeffs_bar, field_bar, S: SpectralTransform, *, unscale_coslat: bool = False,
+                        add: bool = True):
+    """Adjoint of the synthesis ``transform_(field, coeffs, S; unscale_coslat)``:
+    ``coeffs_bar (+)= S^T field_bar`` (spec2grid_pullback!,
+    SpeedyTransformsEnzymeExt.jl:263-289; accumulates by default, as the reference)."""
+    ldc, K = _coeff_arg(coeffs_bar, S, "coeffs_bar")
+    ldg, K2 = _field_arg(field_bar, S, "field_bar")
+    _check_k(S, K, K2)
+    flags = (_lib.UNSCALE_COSLAT if unscale_coslat else 0) | (_lib.ADD if add else 0)
+    check(lib.sht_synthesize_adjoint(S.handle, field_bar.data.data_ptr(), ldg, coeffs_bar.data.data_ptr(), ldc, K,
+                                     flags, _stream_ptr(S.device)))
+    return coeffs_bar
+
+
+def grid2spec_pullback_(field_bar, coeffs_bar, S: SpectralTransform, *, add: bool = True):
+    """Adjoint of the analysis ``transform_(coeffs, field, S)``: ``field_bar (+)= A^T coeffs_bar``
+    (grid2spec_pullback!, SpeedyTransformsEnzymeExt.jl:294-323; accumulates by default)."""
+    ldg, K = _field_arg(field_bar, S, "field_bar")
+    ldc, K2 = _coeff_arg(coeffs_bar, S, "coeffs_bar")
+    _check_k(S, K, K2)
+    check(lib.sht_analyze_adjoint(S.handle, coeffs_bar.data.data_ptr(), ldc, field_bar.data.data_ptr(), ldg, K,
+                                  _lib.ADD if add else 0, _stream_ptr(S.device)))
+    return field_bar
+
+
 def transform(inp, S: SpectralTransform, *, unscale_coslat: bool = False):
     """Allocating transform (spectral_transform.jl:638-661)."""
     K = inp.nlayers if inp.data.dim() == 2 else None

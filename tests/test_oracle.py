@@ -201,3 +201,28 @@ def test_flipsign_add_semantics():
     np.testing.assert_array_equal(d2, -d)
     d3 = O.divergence(sp, u, v, add=True, out=d)
     np.testing.assert_allclose(d3, 2 * d)
+
+
+def _rdot(a, b):
+    """Real inner product of the Float32 storage: re and im parts as separate reals."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.sum(a.real * b.real) + np.sum(a.imag * b.imag))
+
+
+@pytest.mark.parametrize("grid", [O.FULL_GAUSSIAN, O.OCTAHEDRAL_GAUSSIAN])
+@pytest.mark.parametrize("unscale", [False, True])
+def test_adjoint_dot_products(grid, unscale):
+    """The restated pullbacks (SpeedyTransformsEnzymeExt.jl:263-323) are the adjoints of
+    the transforms: <S c, g> = <c, S^T g> and <A g, c> = <g, A^T c>."""
+    T = O.Spectrum(32, 32)
+    S = O.SpectralTransform(T, O.Grid(grid, 24))
+    rng = np.random.default_rng(7)
+    c = rng.standard_normal((T.nlm, 3)) + 1j * rng.standard_normal((T.nlm, 3))
+    g = rng.standard_normal((S.grid.npoints, 3))
+    lhs = _rdot(S.synthesize(c, unscale_coslat=unscale), g)
+    rhs = _rdot(c, S.synthesize_adjoint(g, unscale_coslat=unscale))
+    assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1.0)
+    lhs = _rdot(S.analyze(g), c)
+    rhs = _rdot(g, S.analyze_adjoint(c))
+    assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), 1.0)
