@@ -248,6 +248,26 @@ SHT_API int sht_batch_launch(sht_batch* b, void* stream);
 SHT_API int sht_batch_autotune(sht_batch* b, void* stream, int32_t* tile_columns);
 SHT_API int sht_batch_destroy(sht_batch* b);
 
+/* ---- dense-matrix transforms (MatrixSpectralTransform) ------------------------------
+ * replaces SpeedyTransforms/src/matrix_transform.jl:56-260: the transforms as products
+ * with precomputed dense matrices (the transforms of unit vectors, :134-173), built here
+ * by this library's FP32 transforms. desc as for sht_plan_create; precision
+ * SHT_PREC_FP32 runs cuBLAS SGEMM (the reference's Float32 mul!), SHT_PREC_BF16X3 /
+ * SHT_PREC_FP16X3 / SHT_PREC_BF16X5 the tcgen05 kernel with the matrix in 16-bit pieces.
+ * Matrices: npoints x 2 nlm floats each (T63 octahedral: 188 MB in FP32), so this suits
+ * the small truncations the reference uses it for.
+ * sht_matrix_synthesize: coeffs [K][ldc] complex -> grid [K][ldg]; flags SHT_UNSCALE_COSLAT.
+ * sht_matrix_analyze: grid -> coeffs; no flags. */
+typedef struct sht_matrix sht_matrix;
+SHT_API int sht_matrix_create(const sht_desc* desc, sht_matrix** out);
+SHT_API int sht_matrix_synthesize(sht_matrix* m, const void* coeffs, int64_t ldc, float* grid, int64_t ldg, int K,
+                                  unsigned flags, void* stream);
+SHT_API int sht_matrix_analyze(sht_matrix* m, const float* grid, int64_t ldg, void* coeffs, int64_t ldc, int K,
+                               unsigned flags, void* stream);
+/* as sht_device_status, for the tensor-core matrix kernel's bounded waits */
+SHT_API int sht_matrix_device_status(sht_matrix* m, int32_t* status);
+SHT_API int sht_matrix_destroy(sht_matrix* m);
+
 /* Synchronises the device and returns (then clears) the plan's device status word:
  * 0 = no kernel gave up waiting; otherwise the code of the first bounded wait in a
  * tensor-core kernel that expired (1 s limit), whose outputs are then incomplete.

@@ -166,6 +166,13 @@ FftView fft_view(const Plan& p, const float* gin, float* gout, int64_t ldg, floa
                  bool image, bool adjoint);
 cudaError_t launch_fft_grouped(const FftView* views, const GroupItem* items, int nitems, bool synthesis, int smem,
                                int grid, cudaStream_t s);
+// dense matrix transforms on the tensor cores (sht_legendre_tc.cu)
+struct TcMatrix;
+cudaError_t tc_matrix_create(TcMatrix** out, int precision, const float* const a[2], const int depth[2],
+                             const int M[2], int nlayers);
+void tc_matrix_destroy(TcMatrix* x);
+cudaError_t tc_matrix_apply(const TcMatrix* x, int which, const float* in, int64_t ld, float* out, int64_t ldo, int K,
+                            const float* row_scale, int32_t* d_err, cudaStream_t st);
 cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, float mul);
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s,
                                 bool to_image = false, unsigned flags = 0, bool adjoint = false);

@@ -87,6 +87,15 @@ struct TcDev {
     const int32_t* mexp;           // per m: e_m of the Legendre scaling
     const float2* kscale_syn;      // per layer: (2^(e_k - 15), 2^(15 - e_k)) of the synthesis input
     const float2* kscale_ana;      // per layer: the same for the analysis data (E, O)
+    // dense matrix transforms (MatrixSpectralTransform): one "order" m = 0 whose A operand
+    // is the matrix; the epilogue writes out[n ldo + row] for the K layer columns n
+    int matrix;
+    int mrows;                     // rows of the matrix (output length per layer)
+    float* mout;
+    int64_t ldo;
+    const float* row_scale;        // per output row (1 / cos lat of its ring) or nullptr
+    int kchunk;                    // > 0: accumulate the depth in chunks of kchunk 64-deep blocks,
+                                   // each on a fresh accumulator, summed in FP32 by the epilogue
 };
 
 struct TcState {
@@ -243,9 +252,30 @@ __device__ __forceinline__ int item_steps(const TcDev& t, const TcItem& it) {
 
 template <bool SYN>
 __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_cols, int K, uint32_t taddr, int r,
-                               float2* four, float2* coeffs, int64_t ldc, int add, bool good) {
+                               float2* four, float2* coeffs, int64_t ldc, int add, bool good, bool accumulate) {
     const int m = it.m, par = it.par, tile = it.tile;
     const float mscale = t.fp16 ? ldexpf(1.f, t.mexp[m] - F16_TOP) : 1.f;
+    if (SYN && t.matrix) {
+        const int row = tile * 128 + r;
+        const bool valid = good && row < t.mrows;
+        const float rs = (valid && t.row_scale) ? t.row_scale[row] : 1.f;
+        for (int c0 = 0; c0 < nt_cols; c0 += 32) {
+            float v[32];
+            tmem_ld32(taddr + c0, v);
+            if (!valid) continue;
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                const int n = ct * 256 + c0 + q;
+                if (n >= K) break;
+                float x = v[q];
+                if (t.fp16) x = x * mscale * t.kscale_syn[n].x;
+                x = x * rs;
+                float* o = t.mout + (int64_t)n * t.ldo + row;
+                *o = accumulate ? *o + x : x;      // later depth chunks: this thread wrote *o before
+            }
+        }
+        return;
+    }
     if (SYN) {
         const int j = t.j0[m] + tile * 128 + r;
         const bool valid = good && j < t.nh && m <= t.rings[j].mt;
@@ -398,15 +428,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const TcItem it = items[ix];
             const int nsteps = item_steps<SYN>(t, it);
             if (nsteps == 0) continue;
+            const int kch = t.kchunk > 0 ? t.kchunk : nsteps;
+          for (int ks0 = 0; ks0 < nsteps && ok; ks0 += kch) {
             const int a = ti & 1;
             if (ti >= 2 && !mbar_wait(&acce[a], ((ti / 2) - 1) & 1)) {
                 *abort_flag = 1;
                 atomicExch(t.err, 4);
+                ok = false;
                 break;
             }
             tc_fence_after();
             const uint32_t dacc = tmem + (uint32_t)(a * acc_cols);
-            for (int ks = 0; ks < nsteps; ++ks, ++g) {
+            for (int ks = ks0; ks < min(nsteps, ks0 + kch); ++ks, ++g) {
                 const int s = g % stages;
                 if (!mbar_wait(&full_bar[s], (g / stages) & 1)) {
                     *abort_flag = 1;
@@ -429,13 +462,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                             da = sdesc(aa + kk * 32, 16, 1024);
                             db = sdesc(bb + kk * 2048, BOX_BYTES, 1024);
                         }
-                        umma_f16(dacc, da, db, idesc, (ks | kk | q) ? 1u : 0u);
+                        umma_f16(dacc, da, db, idesc, (ks != ks0 || kk || q) ? 1u : 0u);
                     }
                 }
                 umma_commit(&empty_bar[s]);      // frees the stage once these MMAs complete
             }
             umma_commit(&accf[a]);               // accumulator ready (or drained after an abort)
             ++ti;
+          }
         }
         // Every MMA must have completed before the tensor memory is released.
         if (ti > 0 && !mbar_wait(&accf[(ti - 1) & 1], ((ti - 1) / 2) & 1)) atomicExch(t.err, 6);
@@ -456,19 +490,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 continue;
             }
-            const int a = ti & 1;
-            // warp-uniform outcome: tcgen05.ld below is a warp-collective instruction
-            const bool ok = __all_sync(0xffffffffu, mbar_wait(&accf[a], (ti / 2) & 1));
-            if (!ok) {
-                *abort_flag = 1;
-                atomicExch(t.err, 3);
+            const int nsteps = item_steps<SYN>(t, it);
+            const int kch = t.kchunk > 0 ? t.kchunk : nsteps;
+            bool ok = true;
+            for (int ks0 = 0; ks0 < nsteps; ks0 += kch) {
+                const int a = ti & 1;
+                // warp-uniform outcome: tcgen05.ld below is a warp-collective instruction
+                ok = __all_sync(0xffffffffu, mbar_wait(&accf[a], (ti / 2) & 1));
+                if (!ok) {
+                    *abort_flag = 1;
+                    atomicExch(t.err, 3);
+                }
+                tc_fence_after();
+                const uint32_t taddr = tmem + (uint32_t)(a * acc_cols) + ((uint32_t)(quarter * 32) << 16);
+                epilogue_store<SYN>(t, it, ct, nt_cols, K, taddr, r, four, coeffs, ldc, add, ok && !*abort_flag,
+                                    ks0 > 0);
+                tc_fence_before();
+                mbar_arrive(&acce[a]);
+                ++ti;
+                if (!ok) break;
             }
-            tc_fence_after();
-            const uint32_t taddr = tmem + (uint32_t)(a * acc_cols) + ((uint32_t)(quarter * 32) << 16);
-            epilogue_store<SYN>(t, it, ct, nt_cols, K, taddr, r, four, coeffs, ldc, add, ok && !*abort_flag);
-            tc_fence_before();
-            mbar_arrive(&acce[a]);
-            ++ti;
             if (!ok) break;
         }
     }
@@ -905,6 +946,231 @@ cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, in
 }
 
 // mul: bound of the analysis data per unit grid value; 0 = the transform's (4 pi max w)
+// ---------------------------------------------------------------- dense matrix transforms
+// A matrix operand [depth][M] (M contiguous, FP32) as 16-bit pieces [piece][depth][Mp]
+// (Mp = M rounded up to 8 for 16-byte TMA strides), scaled by 2^(15 - e) for fp16.
+__global__ void matrix_pieces_kernel(const float* __restrict__ a, int64_t depth, int M, int Mp, int npa, int fp16,
+                                     float scale, uint16_t* __restrict__ out) {
+    const int64_t total = depth * (int64_t)Mp;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = i / Mp;
+        const int m = (int)(i - d * Mp);
+        float r = m < M ? a[d * M + m] * scale : 0.f;
+        for (int q = 0; q < npa; ++q) {
+            const uint32_t b = fp16 ? piece_bits<true>(r) : piece_bits<false>(r);
+            out[(int64_t)q * total + i] = (uint16_t)b;
+        }
+    }
+}
+
+// B operand image of a matrix product: layer columns n < K of depth values from
+// in[n ld + d] (FP32), as K-major SWIZZLE_128B tiles per (64-deep block, piece),
+// nmax columns; depth past the end written as zeros.
+template <int NPB, bool F16>
+__global__ void __launch_bounds__(256) matrix_image_kernel(const float* __restrict__ in, int64_t ld, int depth, int K,
+                                                           const float2* __restrict__ kscale, uint16_t* __restrict__ img,
+                                                           int64_t tile_bytes) {
+    const int kt = blockIdx.x;
+    const int ib8 = threadIdx.x & 7;
+    const int n = blockIdx.y * 32 + (threadIdx.x >> 3);
+    if (n >= K) return;
+    const int d0 = kt * BLK + 8 * ib8;
+    float v[8];
+    const float sc = F16 ? kscale[n].y : 1.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = d0 + q < depth ? __ldg(in + (int64_t)n * ld + d0 + q) * sc : 0.f;
+    uint32_t w[NPB][4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+        float r0 = v[2 * h], r1 = v[2 * h + 1];
+#pragma unroll
+        for (int q = 0; q < NPB; ++q) {
+            const uint32_t b0 = piece_bits<F16>(r0);
+            w[q][h] = b0 | (piece_bits<F16>(r1) << 16);
+        }
+    }
+    const int64_t off = (int64_t)(n / 8) * 1024 + (n % 8) * 128 + ((ib8 ^ (n % 8)) * 16);
+    uint8_t* base = reinterpret_cast<uint8_t*>(img);
+#pragma unroll
+    for (int q = 0; q < NPB; ++q)
+        *reinterpret_cast<uint4*>(base + ((int64_t)kt * NPB + q) * tile_bytes + off) =
+            make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+}
+
+struct TcMatrixDir {               // one matrix (analysis or synthesis direction)
+    int depth = 0, M = 0, Mp = 0, nkt = 0;
+    uint16_t* d_a = nullptr;       // pieces
+    CUtensorMap* d_map = nullptr;
+    int32_t* d_nkt = nullptr;
+    int32_t* d_mexp = nullptr;     // fp16: e of the matrix
+    TcItem* d_items = nullptr;
+    int nitems = 0;
+};
+
+struct TcMatrix {
+    int npa = 2, npb = 2, nprod = 3, fp16 = 0;
+    uint32_t prod = 0;
+    int nmax = 0, nsm = 148, nlayers = 0;
+    TcMatrixDir dir[2];            // 0: analysis (A = F^T as [npoints][2 nlm]), 1: synthesis
+    int64_t* d_base = nullptr;     // {0}
+    uint16_t* d_img = nullptr;
+    int64_t tile_bytes = 0;
+    float* d_absmax = nullptr;
+    float2* d_kscale = nullptr;
+};
+
+cudaError_t tc_matrix_create(TcMatrix** out, int precision, const float* const a[2], const int depth[2],
+                             const int M[2], int nlayers) {
+    TcMatrix* x = new TcMatrix();
+    *out = x;
+    if (precision == SHT_PREC_BF16X3 || precision == SHT_PREC_FP16X3) {
+        x->npa = 2; x->npb = 2; x->nprod = 3; x->fp16 = precision == SHT_PREC_FP16X3;
+        x->prod = (0u | (0u << 2)) | ((0u | (1u << 2)) << 4) | ((1u | (0u << 2)) << 8);
+    } else if (precision == SHT_PREC_BF16X5) {
+        x->npa = 3; x->npb = 2; x->nprod = 5;
+        x->prod = (0u | (0u << 2)) | ((0u | (1u << 2)) << 4) | ((1u | (0u << 2)) << 8) | ((1u | (1u << 2)) << 12) |
+                  ((2u | (0u << 2)) << 16);
+    } else {
+        return cudaErrorNotSupported;
+    }
+    x->nlayers = nlayers;
+    x->nmax = nlayers <= 256 ? (nlayers + 63) / 64 * 64 : (nlayers + 255) / 256 * 256;
+    x->tile_bytes = (int64_t)x->nmax * 128;
+    {
+        int dev = 0, nsm = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
+            x->nsm = nsm;
+    }
+    cudaError_t e;
+    auto enc = get_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    const int64_t zero = 0;
+    if ((e = cudaMalloc(&x->d_base, sizeof(int64_t))) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(x->d_base, &zero, sizeof(int64_t), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    int max_nkt = 0;
+    for (int d = 0; d < 2; ++d) {
+        TcMatrixDir& m = x->dir[d];
+        m.depth = depth[d];
+        m.M = M[d];
+        m.Mp = (M[d] + 7) / 8 * 8;
+        m.nkt = (depth[d] + BLK - 1) / BLK;
+        max_nkt = std::max(max_nkt, m.nkt);
+        // fp16: e of max |A| (the whole matrix shares one power-of-two scale)
+        int ex = 0;
+        if (x->fp16) {
+            float* d_mx = nullptr;
+            if ((e = cudaMalloc(&d_mx, sizeof(float))) != cudaSuccess) return e;
+            cudaMemset(d_mx, 0, sizeof(float));
+            absmax_kernel<<<dim3(4 * x->nsm, 1), 256>>>(a[d], (int64_t)depth[d] * M[d], (int64_t)depth[d] * M[d], d_mx);
+            float mx = 0.f;
+            e = cudaMemcpy(&mx, d_mx, sizeof(float), cudaMemcpyDeviceToHost);
+            cudaFree(d_mx);
+            if (e != cudaSuccess) return e;
+            if (mx > 0.f) std::frexp((double)mx, &ex);
+        }
+        const int64_t total = (int64_t)m.depth * m.Mp;
+        if ((e = cudaMalloc(&m.d_a, std::max<int64_t>(16, total * x->npa * 2))) != cudaSuccess) return e;
+        matrix_pieces_kernel<<<4 * x->nsm, 256>>>(a[d], m.depth, m.M, m.Mp, x->npa, x->fp16,
+                                                  x->fp16 ? std::ldexp(1.f, F16_TOP - ex) : 1.f, m.d_a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof map);
+        cuuint64_t dims[3] = {(cuuint64_t)m.Mp, (cuuint64_t)m.depth, (cuuint64_t)x->npa};
+        cuuint64_t strides[2] = {(cuuint64_t)m.Mp * 2, (cuuint64_t)m.Mp * 2 * m.depth};
+        cuuint32_t box[3] = {BLK, BLK, 1};
+        cuuint32_t estr[3] = {1, 1, 1};
+        if (enc(&map, x->fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, m.d_a, dims,
+                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+        if ((e = cudaMalloc(&m.d_map, sizeof(CUtensorMap))) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(m.d_map, &map, sizeof map, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&m.d_nkt, sizeof(int32_t))) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(m.d_nkt, &m.nkt, sizeof(int32_t), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&m.d_mexp, sizeof(int32_t))) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(m.d_mexp, &ex, sizeof(int32_t), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+        std::vector<TcItem> items;
+        for (int tl = 0; tl * 128 < m.M; ++tl) items.push_back({0, 0, tl, 0});
+        m.nitems = (int)items.size();
+        if ((e = cudaMalloc(&m.d_items, items.size() * sizeof(TcItem))) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(m.d_items, items.data(), items.size() * sizeof(TcItem), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return e;
+    }
+    const int64_t img_bytes = (int64_t)max_nkt * x->npb * x->tile_bytes;
+    if ((e = cudaMalloc(&x->d_img, std::max<int64_t>(16, img_bytes))) != cudaSuccess) return e;
+    if ((e = cudaMemset(x->d_img, 0, std::max<int64_t>(16, img_bytes))) != cudaSuccess) return e;
+    if (x->fp16) {
+        if ((e = cudaMalloc(&x->d_absmax, sizeof(float) * std::max(1, nlayers))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&x->d_kscale, sizeof(float2) * std::max(1, nlayers))) != cudaSuccess) return e;
+    }
+    if ((e = cudaFuncSetAttribute(legendre_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  227 * 1024)) != cudaSuccess)
+        return e;
+    return cudaDeviceSynchronize();
+}
+
+void tc_matrix_destroy(TcMatrix* x) {
+    if (!x) return;
+    for (auto& m : x->dir) {
+        void* ptrs[] = {m.d_a, m.d_map, m.d_nkt, m.d_mexp, m.d_items};
+        for (void* q : ptrs)
+            if (q) cudaFree(q);
+    }
+    void* ptrs[] = {x->d_base, x->d_img, x->d_absmax, x->d_kscale};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    delete x;
+}
+
+// out[n ldo + row] = sum_d A[d][row] in[n ld + d] (times row_scale[row]) for n < K.
+cudaError_t tc_matrix_apply(const TcMatrix* x, int which, const float* in, int64_t ld, float* out, int64_t ldo, int K,
+                            const float* row_scale, int32_t* d_err, cudaStream_t st) {
+    const TcMatrixDir& m = x->dir[which];
+    if (K <= 0 || K > x->nlayers) return cudaErrorInvalidValue;
+    cudaError_t e;
+    if (x->fp16) {
+        if ((e = cudaMemsetAsync(x->d_absmax, 0, sizeof(float) * K, st)) != cudaSuccess) return e;
+        absmax_kernel<<<dim3(std::max(1, 2 * x->nsm / K) * 4, K), 256, 0, st>>>(in, ld, m.depth, x->d_absmax);
+        kscale_kernel<<<1, 256, 0, st>>>(x->d_absmax, 1.f, K, x->d_kscale);
+    }
+    const dim3 ig(m.nkt, (K + 31) / 32);
+    if (x->fp16)
+        matrix_image_kernel<2, true><<<ig, 256, 0, st>>>(in, ld, m.depth, K, x->d_kscale, x->d_img, x->tile_bytes);
+    else
+        matrix_image_kernel<2, false><<<ig, 256, 0, st>>>(in, ld, m.depth, K, nullptr, x->d_img, x->tile_bytes);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    TcDev t{};
+    t.maps = m.d_map;
+    t.syn_tile_base = x->d_base;
+    t.nkt = m.d_nkt;
+    t.syn_img = x->d_img;
+    t.err = d_err;
+    t.npa = x->npa;
+    t.npb = x->npb;
+    t.nprod = x->nprod;
+    t.prod = x->prod;
+    t.syn_tile_bytes = x->tile_bytes;
+    t.nmax = x->nmax;
+    t.fp16 = x->fp16;
+    t.mexp = m.d_mexp;
+    t.kscale_syn = x->d_kscale;
+    t.matrix = 1;
+    t.mrows = m.M;
+    t.mout = out;
+    t.ldo = ldo;
+    t.row_scale = row_scale;
+    t.kchunk = 8;                  // 512-deep accumulation chunks
+    const int nct = (K + 255) / 256;
+    const int nt_cols = std::min(256, (K + 63) / 64 * 64);
+    int stages;
+    const int smem = smem_for(x->npa, x->npb, nt_cols, stages);
+    legendre_tc_kernel<true><<<dim3(std::min(m.nitems, x->nsm), nct), TC_THREADS, smem, st>>>(
+        t, m.d_items, m.nitems, K, nt_cols, stages, tmem_cols_for(nt_cols), nullptr, nullptr, 0, 0);
+    return cudaGetLastError();
+}
+
 cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t st, float mul) {
     const TcState* s = static_cast<const TcState*>(p.tc);
     if (!s || !s->fp16 || K <= 0) return cudaSuccess;

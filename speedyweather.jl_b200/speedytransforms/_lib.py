@@ -68,6 +68,11 @@ SIGNATURES = {
     "sht_batch_launch": (C.c_int, [_P, _P]),
     "sht_batch_autotune": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
     "sht_batch_destroy": (C.c_int, [_P]),
+    "sht_matrix_create": (C.c_int, [C.POINTER(ShtDesc), C.POINTER(C.c_void_p)]),
+    "sht_matrix_synthesize": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
+    "sht_matrix_analyze": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
+    "sht_matrix_device_status": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "sht_matrix_destroy": (C.c_int, [_P]),
     "sht_last_error": (C.c_char_p, []),
     "sht_version": (C.c_char_p, []),
 }

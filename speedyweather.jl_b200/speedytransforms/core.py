@@ -325,6 +325,48 @@ class SpectralTransform:
                 f"precision={self.precision!r})")
 
 
+class MatrixSpectralTransform:
+    """Dense-matrix spectral transform (matrix_transform.jl:56-260):
+    ``MatrixSpectralTransform(spectrum, grid, nlayers=K, precision="fp32")``; the
+    matrices are the transforms of unit vectors. "fp32" multiplies with cuBLAS SGEMM
+    (the reference's Float32 mul!), "bf16x3" / "fp16x3" / "bf16x5" on the tensor cores.
+    Used through ``transform_`` / ``transform`` like a SpectralTransform (no ``add``)."""
+
+    def __init__(self, spectrum: Spectrum, grid: _GaussianGrid, *, nlayers: int = 1, LegendreShortcut: str = "linear",
+                 precision: str = "fp32", device=None):
+        if precision not in _PRECISIONS:
+            raise ValueError(f"unknown precision {precision!r}")
+        self.spectrum, self.grid = spectrum, grid
+        self.nlayers = int(nlayers)
+        self.precision = precision
+        self.device = torch.device(device) if device is not None else _default_device()
+        d = _lib.ShtDesc(grid.kind, grid.nlat_half, spectrum.lmax, spectrum.mmax, self.nlayers,
+                         _PRECISIONS[precision], _lib.SHORTCUTS[LegendreShortcut],
+                         self.device.index if self.device.index is not None else torch.cuda.current_device())
+        h = C.c_void_p()
+        self._m = None
+        check(lib.sht_matrix_create(C.byref(d), C.byref(h)))
+        self._m = h
+
+    @property
+    def handle(self):
+        return self._m
+
+    def device_status(self) -> int:
+        v = C.c_int32(0)
+        check(lib.sht_matrix_device_status(self._m, C.byref(v)))
+        return int(v.value)
+
+    def __del__(self):
+        if getattr(self, "_m", None) is not None:
+            lib.sht_matrix_destroy(self._m)
+            self._m = None
+
+    def __repr__(self):
+        return (f"MatrixSpectralTransform({self.spectrum}, {self.grid}, nlayers={self.nlayers}, "
+                f"precision={self.precision!r})")
+
+
 class Batch:
     """Many transforms in one grouped launch per stage (sht_batch_*): all syntheses,
     then all analyses, each item with its own scratch.
@@ -405,6 +447,8 @@ def transform_(out, inp, S: SpectralTransform, *, unscale_coslat: bool = False, 
     """transform!(out, in, S): synthesis if ``out`` is a Field, analysis if it is a
     LowerTriangularArray (spectral_transform.jl:515-531, 579-593)."""
     dev = S.device
+    if isinstance(S, MatrixSpectralTransform):
+        return _matrix_transform_(out, inp, S, unscale_coslat=unscale_coslat, add=add)
     if isinstance(out, Field) and isinstance(inp, LowerTriangularArray):
         ldg, K = _field_arg(out, S, "field")
         ldc, K2 = _coeff_arg(inp, S, "coeffs")
@@ -423,6 +467,30 @@ def transform_(out, inp, S: SpectralTransform, *, unscale_coslat: bool = False, 
                               _lib.ADD if add else 0, _stream_ptr(dev)))
         return out
     raise TypeError("transform_(out, in, S) needs (Field, LowerTriangularArray) or (LowerTriangularArray, Field)")
+
+
+def _matrix_transform_(out, inp, M, *, unscale_coslat=False, add=False):
+    """transform! with a MatrixSpectralTransform (matrix_transform.jl:196-260)."""
+    if add:
+        raise TypeError("MatrixSpectralTransform has no add option (matrix_transform.jl:228-260)")
+    dev = M.device
+    if isinstance(out, Field) and isinstance(inp, LowerTriangularArray):
+        ldg, K = _field_arg(out, M, "field")
+        ldc, K2 = _coeff_arg(inp, M, "coeffs")
+        _check_k(M, K, K2)
+        check(lib.sht_matrix_synthesize(M.handle, inp.data.data_ptr(), ldc, out.data.data_ptr(), ldg, K,
+                                        _lib.UNSCALE_COSLAT if unscale_coslat else 0, _stream_ptr(dev)))
+        return out
+    if isinstance(out, LowerTriangularArray) and isinstance(inp, Field):
+        if unscale_coslat:
+            raise TypeError("unscale_coslat applies to spectral-to-grid transforms only")
+        ldc, K = _coeff_arg(out, M, "coeffs")
+        ldg, K2 = _field_arg(inp, M, "field")
+        _check_k(M, K, K2)
+        check(lib.sht_matrix_analyze(M.handle, inp.data.data_ptr(), ldg, out.data.data_ptr(), ldc, K, 0,
+                                     _stream_ptr(dev)))
+        return out
+    raise TypeError("transform_(out, in, M) needs (Field, LowerTriangularArray) or (LowerTriangularArray, Field)")
 
 
 def spec2grid_pullback_(coeffs_bar, field_bar, S: SpectralTransform, *, unscale_coslat: bool = False,

@@ -1,0 +1,74 @@
+"""MatrixSpectralTransform (sht_matrix_*): the transforms as dense products.
+
+The matrices are this library's FP32 transforms of unit vectors (matrix_transform.jl:134-173),
+so the FP32 products (cuBLAS SGEMM) agree with the SpectralTransform to FP32 rounding;
+the tensor-core products carry their split-precision error. Against the FP64 oracle:
+FP32 1e-5; every tensor-core form 3e-5 (relative L2). A dense product is one dot product
+of length npoints (analysis) or 2 nlm (synthesis) whose terms cancel heavily (the DFT and
+Legendre sums fused into one), accumulated in the tensor core's FP32: its error is ~1-2e-5
+at T31 whatever the operand split (the transform's FFT plus short Legendre sums stay lower)."""
+import numpy as np
+import pytest
+
+import sht_oracle as O
+from test_gpu_parity import nan_field, nan_lta, np_of, setup, to_field, to_lta
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp32": 1e-5, "bf16x3": 3e-5, "bf16x5": 3e-5, "fp16x3": 3e-5}
+_cache = {}
+
+
+@pytest.fixture(scope="module")
+def st():
+    import speedytransforms as st
+    return st
+
+
+def matrix(st, T, grid, nh, K, prec):
+    key = (T, grid, nh, K, prec)
+    if key not in _cache:
+        g = st.OctahedralGaussianGrid(nh) if grid == "octa" else st.FullGaussianGrid(nh)
+        _cache[key] = st.MatrixSpectralTransform(st.Spectrum(T, T), g, nlayers=K, precision=prec)
+    return _cache[key]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16x3", "fp16x3", "bf16x5"])
+@pytest.mark.parametrize("T,grid,nh,K", [(31, "full", 24, 3), (63, "octa", 48, 8)])
+def test_matrix_transform_vs_oracle(st, prec, T, grid, nh, K):
+    M = matrix(st, T, grid, nh, K, prec)
+    S, So = setup(st, T, grid, K, nh=nh)
+    c = O.random_coeffs(So.spectrum, K, seed=T + 11)
+    f = nan_field(st, S, K)
+    st.transform_(f, to_lta(st, S, c), M)
+    assert M.device_status() == 0
+    ref = So.synthesize(c)
+    assert O.rel_err(np_of(f), ref) < TOL[prec]
+    g = ref.astype(np.float32)
+    a = nan_lta(st, S, K)
+    st.transform_(a, to_field(st, S, g), M)
+    assert M.device_status() == 0
+    assert O.rel_err(np_of(a), So.analyze(g.astype(np.float64))) < TOL[prec]
+
+
+def test_matrix_fp32_matches_spectral_transform(st):
+    M = matrix(st, 31, "full", 24, 3, "fp32")
+    S, So = setup(st, 31, "full", 3, nh=24)
+    c = O.random_coeffs(So.spectrum, 3, seed=4)
+    lt = to_lta(st, S, c)
+    fm, fs = st.transform(lt, M, unscale_coslat=True), st.transform(lt, S, unscale_coslat=True)
+    assert O.rel_err(np_of(fm), np_of(fs)) < 2e-6
+    am, as_ = st.transform(fs, M), st.transform(fs, S)
+    assert O.rel_err(np_of(am), np_of(as_)) < 2e-6
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16x3"])
+def test_matrix_unscale_and_single_layer(st, prec):
+    M = matrix(st, 63, "octa", 48, 8, prec)
+    S, So = setup(st, 63, "octa", 8, nh=48)
+    c = O.random_coeffs(So.spectrum, 1, seed=9)
+    f = st.transform(to_lta(st, S, c), M, unscale_coslat=True)
+    ref = So.synthesize(c, unscale_coslat=True)
+    assert O.rel_err(np_of(f), ref) < TOL[prec]
+    with pytest.raises(TypeError):
+        st.transform_(st.Field.zeros(S.grid, 1), to_lta(st, S, c), M, add=True)
