@@ -268,6 +268,59 @@ SHT_API int sht_matrix_analyze(sht_matrix* m, const float* grid, int64_t ldg, vo
 SHT_API int sht_matrix_device_status(sht_matrix* m, int32_t* status);
 SHT_API int sht_matrix_destroy(sht_matrix* m);
 
+/* ---- column physics and its learned emulator (primitive-equation wet model) ---------
+ * sht_column_physics: large-scale condensation + simplified Betts-Miller convection
+ * tendencies of ncol columns (replaces the column loops of
+ * SpeedyWeather/src/parameterizations/large_scale_condensation.jl:55-178 and
+ * SpeedyWeather/src/parameterizations/convection.jl:33-253, in the driver's order,
+ * SpeedyWeather/src/parameterizations/tendencies.jl:3-90). Fields layer-major like a
+ * Field{npoints, nlayers}: temp[k ld + ij] [K], humid [kg/kg], surface_pressure[ij] [Pa];
+ * outputs dtemp [K/s], dhumid [kg/kg/s] (SHT_ADD accumulates, as the reference does).
+ * nlayers = SHT_COLUMN_LAYERS (sigma coordinates with equispaced half levels), dt the
+ * model time step [s], flat orography. */
+#define SHT_COLUMN_LAYERS 8
+SHT_API int sht_column_physics(const float* temp, const float* humid, const float* surface_pressure, int64_t ld,
+                               int ncol, int nlayers, double dt, float* dtemp, float* dhumid, unsigned flags,
+                               void* stream);
+
+/* MLP column emulator with hand-written BF16 training and inference kernels (tcgen05):
+ * 33 inputs (temp, humid, u, v on 8 layers, log surface pressure) -> 3 x 256 (GELU) ->
+ * 16 outputs (temperature and humidity tendencies on 8 layers); BF16 weights with FP32
+ * masters and Adam moments, FP32 accumulate. It stands in for the two parameterizations
+ * of sht_column_physics through the parameterization interface
+ * parameterization!(ij, vars, p, model) (SpeedyWeather/src/parameterizations/tendencies.jl:3-90).
+ * x: [B][33] raw inputs (layer order: temp 0..7, humid, u, v, then log ps), y: [B][16]
+ * (dtemp 0..7, dhumid 0..7), device FP32, row-major. No counterpart in the reference. */
+typedef struct sht_mlp sht_mlp;
+SHT_API int sht_mlp_create(int batch_capacity, uint64_t seed, int device, sht_mlp** out);
+/* per-input / per-output mean and standard deviation (host arrays of 33 and 16) */
+SHT_API int sht_mlp_set_normalization(sht_mlp* m, const float* x_mean, const float* x_std, const float* y_mean,
+                                      const float* y_std);
+/* one Adam step (lr) on the mean squared error of the normalised outputs over B rows */
+SHT_API int sht_mlp_train_step(sht_mlp* m, const float* x, const float* y, int B, float lr, void* stream);
+/* the last train step's loss (synchronises) */
+SHT_API int sht_mlp_loss(sht_mlp* m, float* loss);
+SHT_API int sht_mlp_infer(sht_mlp* m, const float* x, float* y, int B, void* stream);
+/* layer 0..3 parameters as FP32 host arrays (w [out][in], in = 64 for layer 0 with inputs
+ * 33..63 zero, 256 otherwise; b [out]); set = 1 uploads, 0 downloads */
+SHT_API int sht_mlp_params(sht_mlp* m, int layer, float* w, float* b, int set);
+/* The emulator as a parameterization: gathers the columns of layer-major fields
+ * (x[k ld + ij]), runs the network, and writes its tendencies for columns whose every
+ * normalised input lies within z_max of the training mean, the plain parameterizations'
+ * (sht_column_physics, dt) otherwise; *nfallback (if not NULL; synchronises) counts the
+ * latter. flags: SHT_ADD. */
+SHT_API int sht_column_emulate(sht_mlp* m, const float* temp, const float* humid, const float* u, const float* v,
+                               const float* surface_pressure, int64_t ld, int ncol, double dt, double z_max,
+                               float* dtemp, float* dhumid, unsigned flags, int32_t* nfallback, void* stream);
+SHT_API int sht_mlp_device_status(sht_mlp* m, int32_t* status);
+SHT_API int sht_mlp_destroy(sht_mlp* m);
+/* The network's matrix product on its own: C [M][ldc] FP32 = A B, BF16 operands,
+ * A [M][K] (a_mn = 0: stored [M][lda]; 1: stored [K][lda]), B [K][N] (b_mn = 0: stored
+ * [N][ldb]; 1: stored [K][ldb]); leading dimensions multiples of 8 elements; the kernel's
+ * bounded waits report into *device_error (device memory). */
+SHT_API int sht_bf16_gemm(const void* A, int64_t lda, int a_mn, const void* B, int64_t ldb, int b_mn, float* C,
+                          int64_t ldc, int M, int N, int K, int32_t* device_error, void* stream);
+
 /* Synchronises the device and returns (then clears) the plan's device status word:
  * 0 = no kernel gave up waiting; otherwise the code of the first bounded wait in a
  * tensor-core kernel that expired (1 s limit), whose outputs are then incomplete.

@@ -1,0 +1,719 @@
+// MLP column emulator: hand-written BF16 training and inference kernels on tcgen05.
+//
+// Stands in for the column parameterizations large-scale condensation and convection
+// of the primitive-equation wet model (SpeedyWeather/src/parameterizations/
+// large_scale_condensation.jl:55-178, convection.jl:33-253), called per column through
+// the parameterization interface parameterization!(ij, vars, p, model)
+// (SpeedyWeather/src/parameterizations/tendencies.jl:3-90). The plain parameterizations
+// (column_physics.cu) label the training columns, judge the emulator, and replace it
+// for columns outside the range of its training inputs.
+//
+// Network: 33 inputs (T, q, u, v on 8 layers and log surface pressure, normalised)
+// -> 256 -> 256 -> 256 (GELU) -> 16 outputs (dT/dt and dq/dt on 8 layers, normalised).
+// Weights in BF16 (FP32 master copies and Adam moments for training), FP32 accumulate.
+//
+// Every matrix product is one launch of a tcgen05 GEMM: C[M x N] = A[M x K] B[K x N],
+// A and B row-major BF16 in global memory, each either K-major (K contiguous) or
+// MN-major (M or N contiguous), loaded by 2-D TMA boxes of 64 x 64 with 128-byte
+// swizzle into a ring of shared-memory stages; one elected thread issues
+// tcgen05.mma kind::f16 (M = 128, N <= 256) into a TMEM accumulator; four warps read it
+// (tcgen05.ld) and apply a fused epilogue:
+//   forward hidden layer   Z = A W^T + b, A' = bf16(GELU(Z)) (Z kept for the backward)
+//   forward output layer   Y = A W^T + b
+//   backward data          dZ = bf16((dZ' W) * GELU'(Z))
+//   backward weights       dW = dZ^T A (FP32)
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "sht_internal.h"
+#include "tc_ptx.cuh"
+
+namespace sht {
+int set_error(int code, const char* msg);
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+}  // namespace sht
+
+using namespace sht;
+using namespace sht::tcx;
+
+namespace {
+
+constexpr int G_THREADS = 192;
+constexpr int G_BOX = 64;                       // TMA box edge (elements) = K block
+constexpr int G_BOX_BYTES = G_BOX * G_BOX * 2;  // 8 KB
+constexpr int G_STAGES = 3;
+
+enum Epi { EPI_F32 = 0, EPI_BIAS_F32 = 1, EPI_BIAS_GELU = 2, EPI_GELU_BWD = 3 };
+
+struct GemmArgs {
+    int M, N, K;
+    int a_mn, b_mn;                 // operand major-ness: 1 = M (N) contiguous, 0 = K contiguous
+    int epi;
+    float* out_f32;                 // EPI_F32 / EPI_BIAS_F32 output, or EPI_BIAS_GELU pre-activation copy
+    int64_t ld_f32;
+    __nv_bfloat16* out_bf16;        // EPI_BIAS_GELU / EPI_GELU_BWD output
+    int64_t ld_bf16;
+    const float* bias;              // [N]
+    const float* zin;               // EPI_GELU_BWD: pre-activation [M][ld_z]
+    int64_t ld_z;
+    int32_t* err;
+};
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+    return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.3989422804014327f * expf(-0.5f * x * x);
+}
+
+// One 128 x NT output tile per CTA (NT = N rounded up to 16, <= 256).
+__global__ void __launch_bounds__(G_THREADS, 1)
+    bf16_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                     const GemmArgs g, int nt, uint32_t tmem_cols) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * 256;
+    const int nbox_b = (nt + G_BOX - 1) / G_BOX;
+    const int a_bytes = 2 * G_BOX_BYTES;
+    const int stage_bytes = a_bytes + nbox_b * G_BOX_BYTES;
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + (size_t)G_STAGES * stage_bytes);
+    uint64_t* empty_bar = full_bar + G_STAGES;
+    uint64_t* acc_bar = empty_bar + G_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_bar + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    const int nk = (g.K + G_BOX - 1) / G_BOX;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < G_STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        mbar_init(acc_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---- producer: A tile (128 x 64 K) and B tile (nt x 64 K) per K block
+        int issued = 0;
+        for (int kb = 0; kb < nk && !*abort_flag; ++kb, ++issued) {
+            const int s = kb % G_STAGES;
+            if (kb >= G_STAGES && !mbar_wait(&empty_bar[s], ((kb / G_STAGES) - 1) & 1)) {
+                *abort_flag = 1;
+                atomicExch(g.err, 11);
+                break;
+            }
+            uint8_t* st = smem + (size_t)s * stage_bytes;
+            mbar_expect_tx(&full_bar[s], (uint32_t)stage_bytes);
+            for (int h = 0; h < 2; ++h) {   // A: rows (K-major) or columns (MN-major) m0 + 64 h
+                if (g.a_mn)
+                    tma_load_2d(st + h * G_BOX_BYTES, &map_a, m0 + h * G_BOX, kb * G_BOX, &full_bar[s]);
+                else
+                    tma_load_2d(st + h * G_BOX_BYTES, &map_a, kb * G_BOX, m0 + h * G_BOX, &full_bar[s]);
+            }
+            for (int h = 0; h < nbox_b; ++h) {
+                if (g.b_mn)
+                    tma_load_2d(st + a_bytes + h * G_BOX_BYTES, &map_b, n0 + h * G_BOX, kb * G_BOX, &full_bar[s]);
+                else
+                    tma_load_2d(st + a_bytes + h * G_BOX_BYTES, &map_b, kb * G_BOX, n0 + h * G_BOX, &full_bar[s]);
+            }
+        }
+        // no copy may still land after the CTA exits
+        for (int u = issued - 1; u >= 0 && u >= issued - G_STAGES; --u)
+            if (!mbar_wait(&full_bar[u % G_STAGES], (u / G_STAGES) & 1)) atomicExch(g.err, 12);
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)g.a_mn << 15) |
+                               ((uint32_t)g.b_mn << 16) | (((uint32_t)nt >> 3) << 17) | ((128u >> 4) << 24);
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % G_STAGES;
+            if (!mbar_wait(&full_bar[s], (kb / G_STAGES) & 1)) {
+                *abort_flag = 1;
+                atomicExch(g.err, 13);
+                break;
+            }
+            tc_fence_after();
+            const uint32_t st = smem_u32(smem + (size_t)s * stage_bytes);
+            for (int kk = 0; kk < G_BOX / 16; ++kk) {
+                const uint64_t da = g.a_mn ? sdesc(st + kk * 2048, G_BOX_BYTES, 1024) : sdesc(st + kk * 32, 16, 1024);
+                const uint64_t db = g.b_mn ? sdesc(st + a_bytes + kk * 2048, G_BOX_BYTES, 1024)
+                                           : sdesc(st + a_bytes + kk * 32, 16, 1024);
+                umma_f16(tmem, da, db, idesc, (kb | kk) ? 1u : 0u);
+            }
+            umma_commit(&empty_bar[s]);
+        }
+        umma_commit(acc_bar);
+        if (!mbar_wait(acc_bar, 0)) atomicExch(g.err, 14);     // all MMAs done before the dealloc
+    } else if (warp >= 2) {
+        // ---- epilogue: thread = output row
+        const int quarter = warp % 4;
+        const int row = m0 + quarter * 32 + lane;
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(acc_bar, 0));
+        if (!ok) {
+            *abort_flag = 1;
+            atomicExch(g.err, 15);
+        }
+        tc_fence_after();
+        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
+        for (int c0 = 0; c0 < nt; c0 += 32) {
+            float v[32];
+            tmem_ld32(taddr + c0, v);
+            if (!ok || row >= g.M) continue;
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                const int n = n0 + c0 + q;
+                if (c0 + q >= nt || n >= g.N) break;
+                float x = v[q];
+                switch (g.epi) {
+                    case EPI_F32:
+                        g.out_f32[(int64_t)row * g.ld_f32 + n] = x;
+                        break;
+                    case EPI_BIAS_F32:
+                        g.out_f32[(int64_t)row * g.ld_f32 + n] = x + g.bias[n];
+                        break;
+                    case EPI_BIAS_GELU:
+                        x += g.bias[n];
+                        if (g.out_f32) g.out_f32[(int64_t)row * g.ld_f32 + n] = x;
+                        g.out_bf16[(int64_t)row * g.ld_bf16 + n] = __float2bfloat16_rn(gelu(x));
+                        break;
+                    default:   // EPI_GELU_BWD
+                        g.out_bf16[(int64_t)row * g.ld_bf16 + n] =
+                            __float2bfloat16_rn(x * gelu_grad(g.zin[(int64_t)row * g.ld_z + n]));
+                        break;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
+    }
+}
+
+// 2-D tensor map of a row-major BF16 matrix [rows][cols] (row pitch ld elements),
+// box 64 x 64, 128-byte swizzle, zero fill outside.
+bool make_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, int64_t ld) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    std::memset(map, 0, sizeof *map);
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    cuuint32_t box[2] = {G_BOX, G_BOX};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// C = A B with A [M][K] (a_mn = 0: stored [M][lda], K contiguous; 1: stored [K][lda],
+// M contiguous) and B [K][N] (b_mn = 0: stored [N][ldb]; 1: stored [K][ldb]).
+cudaError_t gemm(const __nv_bfloat16* A, int64_t lda, int a_mn, const __nv_bfloat16* B, int64_t ldb, int b_mn,
+                 GemmArgs g, cudaStream_t s) {
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaSuccess;
+    if ((lda * 2) % 16 || (ldb * 2) % 16) return cudaErrorInvalidValue;   // TMA row pitch
+    CUtensorMap ma, mb;
+    const bool ok_a = a_mn ? make_map(&ma, A, g.K, g.M, lda) : make_map(&ma, A, g.M, g.K, lda);
+    const bool ok_b = b_mn ? make_map(&mb, B, g.K, g.N, ldb) : make_map(&mb, B, g.N, g.K, ldb);
+    if (!ok_a || !ok_b) return cudaErrorInvalidValue;
+    g.a_mn = a_mn;
+    g.b_mn = b_mn;
+    const int nt = std::min(256, (g.N + 15) / 16 * 16);
+    uint32_t cols = 32;
+    while ((int)cols < nt) cols <<= 1;
+    const int stage_bytes = 2 * G_BOX_BYTES + ((nt + G_BOX - 1) / G_BOX) * G_BOX_BYTES;
+    const int smem = 1024 + G_STAGES * stage_bytes + 256;
+    const cudaError_t ea = cudaFuncSetAttribute(bf16_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (ea != cudaSuccess) return ea;
+    dim3 grid((g.M + 127) / 128, (g.N + 255) / 256);
+    bf16_gemm_kernel<<<grid, G_THREADS, smem, s>>>(ma, mb, g, nt, cols);
+    return cudaGetLastError();
+}
+
+// ---- elementwise kernels ----
+// X0[b][0..63] = bf16((x[b][i] - mean[i]) / std[i]) for i < nin, 0 beyond
+__global__ void normalize_in_kernel(const float* __restrict__ x, int64_t ldx, int B, int nin, const float* __restrict__ mean,
+                                    const float* __restrict__ stdv, __nv_bfloat16* __restrict__ X0, int ld0) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)B * ld0) return;
+    const int b = (int)(i / ld0), c = (int)(i % ld0);
+    const float v = c < nin ? (x[(int64_t)b * ldx + c] - mean[c]) / stdv[c] : 0.f;
+    X0[i] = __float2bfloat16_rn(v);
+}
+// dY = bf16(2 (Y - yn) / (B nout)), yn = (y - mean) / std; loss += sum (Y - yn)^2 / (B nout)
+__global__ void output_grad_kernel(const float* __restrict__ Y, const float* __restrict__ y, int B, int nout,
+                                   const float* __restrict__ mean, const float* __restrict__ stdv,
+                                   __nv_bfloat16* __restrict__ dY, float* __restrict__ loss) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (i < (int64_t)B * nout) {
+        const int c = (int)(i % nout);
+        const float d = Y[i] - (y[i] - mean[c]) / stdv[c];
+        const float inv = 1.f / ((float)B * nout);
+        dY[i] = __float2bfloat16_rn(2.f * d * inv);
+        l = d * d * inv;
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
+}
+// db[n] = sum_b dZ[b][n] in two deterministic passes: partial[p][n] over rows
+// [256 p, 256 p + 256), then the partials in order
+constexpr int BIAS_ROWS = 256;
+__global__ void bias_partial_kernel(const __nv_bfloat16* __restrict__ dZ, int B, int N, int64_t ld,
+                                    float* __restrict__ partial) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (n >= N) return;
+    float s = 0.f;
+    const int b1 = min(B, (p + 1) * BIAS_ROWS);
+    for (int b = p * BIAS_ROWS; b < b1; ++b) s += __bfloat162float(dZ[(int64_t)b * ld + n]);
+    partial[(int64_t)p * N + n] = s;
+}
+__global__ void bias_final_kernel(const float* __restrict__ partial, int P, int N, float* __restrict__ db) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    float s = 0.f;
+    for (int p = 0; p < P; ++p) s += partial[(int64_t)p * N + n];
+    db[n] = s;
+}
+// Adam (FP32 master, bias-corrected), then the BF16 copy
+__global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ grad, float* __restrict__ m,
+                            float* __restrict__ v, __nv_bfloat16* __restrict__ wb, int64_t n, float lr, float b1,
+                            float b2, float c1, float c2, float eps) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float g = grad[i];
+    const float mi = b1 * m[i] + (1.f - b1) * g;
+    const float vi = b2 * v[i] + (1.f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16_rn(wi);
+}
+// y[b][c] = Y[b][c] std[c] + mean[c]
+__global__ void denormalize_kernel(const float* __restrict__ Y, int B, int nout, const float* __restrict__ mean,
+                                   const float* __restrict__ stdv, float* __restrict__ y, int64_t ldy) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)B * nout) return;
+    const int b = (int)(i / nout), c = (int)(i % nout);
+    y[(int64_t)b * ldy + c] = Y[i] * stdv[c] + mean[c];
+}
+__global__ void to_bf16_kernel(const float* __restrict__ w, __nv_bfloat16* __restrict__ wb, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
+}
+
+// Column emulator glue: gather inputs [ncol][33] from layer-major fields, and scatter the
+// outputs back (emulator where every normalised input lies within z_max, plain physics
+// otherwise).
+constexpr int NLC = SHT_COLUMN_LAYERS;
+__global__ void gather_columns_kernel(const float* __restrict__ T, const float* __restrict__ q,
+                                      const float* __restrict__ u, const float* __restrict__ v,
+                                      const float* __restrict__ ps, int64_t ld, int ncol, float* __restrict__ x) {
+    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= ncol) return;
+    float* r = x + (int64_t)ij * (4 * NLC + 1);
+#pragma unroll
+    for (int k = 0; k < NLC; ++k) {
+        r[k] = T[(int64_t)k * ld + ij];
+        r[NLC + k] = q[(int64_t)k * ld + ij];
+        r[2 * NLC + k] = u[(int64_t)k * ld + ij];
+        r[3 * NLC + k] = v[(int64_t)k * ld + ij];
+    }
+    r[4 * NLC] = logf(ps[ij]);
+}
+__global__ void scatter_columns_kernel(const float* __restrict__ x, const float* __restrict__ mean,
+                                       const float* __restrict__ stdv, float zmax, const float* __restrict__ y,
+                                       const float* __restrict__ dT_plain, const float* __restrict__ dq_plain,
+                                       int64_t ld, int ncol, float* __restrict__ dT, float* __restrict__ dq, int add,
+                                       int* __restrict__ nfallback) {
+    // dT_plain, dq_plain: [layer][ncol]
+    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= ncol) return;
+    const float* r = x + (int64_t)ij * (4 * NLC + 1);
+    bool inside = true;
+    for (int c = 0; c < 4 * NLC + 1; ++c) inside = inside && fabsf((r[c] - mean[c]) / stdv[c]) <= zmax;
+    if (!inside) atomicAdd(nfallback, 1);
+    const float* yo = y + (int64_t)ij * 2 * NLC;
+#pragma unroll
+    for (int k = 0; k < NLC; ++k) {
+        const float a = inside ? yo[k] : dT_plain[(int64_t)k * ncol + ij];
+        const float b = inside ? yo[NLC + k] : dq_plain[(int64_t)k * ncol + ij];
+        float* pa = dT + (int64_t)k * ld + ij;
+        float* pb = dq + (int64_t)k * ld + ij;
+        *pa = add ? *pa + a : a;
+        *pb = add ? *pb + b : b;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+struct sht_mlp {
+    static constexpr int NLAYER = 4;
+    int device = 0, cap = 0;
+    int nin = 4 * SHT_COLUMN_LAYERS + 1, in_pad = 64, hidden = 256, nout = 2 * SHT_COLUMN_LAYERS;
+    int fan_in[NLAYER], fan_out[NLAYER];          // padded input width, output width
+    float *W[NLAYER] = {}, *b[NLAYER] = {};        // FP32 masters [out][in_pad], [out]
+    __nv_bfloat16* Wb[NLAYER] = {};
+    float *mW[NLAYER] = {}, *vW[NLAYER] = {}, *mb[NLAYER] = {}, *vb[NLAYER] = {};
+    float *dW[NLAYER] = {}, *db[NLAYER] = {};
+    __nv_bfloat16* X0 = nullptr;                    // [cap][in_pad]
+    float* Z[3] = {};                               // pre-activations [cap][hidden]
+    __nv_bfloat16* A[3] = {};                       // activations [cap][hidden]
+    __nv_bfloat16* dZ[3] = {};                      // [cap][hidden]
+    float* Y = nullptr;                             // [cap][nout]
+    __nv_bfloat16* dY = nullptr;                    // [cap][nout]
+    float *xm = nullptr, *xs = nullptr, *ym = nullptr, *ys = nullptr;   // normalisation
+    float* loss = nullptr;
+    float* colbuf = nullptr;                        // [cap][nin]  gathered columns
+    float* ybuf = nullptr;                          // [cap][nout] de-normalised outputs
+    float *plainT = nullptr, *plainq = nullptr;     // [NLC][cap] plain-physics fallback
+    int* nfallback = nullptr;
+    float* partial = nullptr;                       // [cap / 256][hidden] bias-gradient partial sums
+    int32_t* err = nullptr;
+    int step = 0;
+};
+
+namespace {
+thread_local char g_msg[256];
+int mcuda(cudaError_t e, const char* what) {
+    snprintf(g_msg, sizeof g_msg, "%s: %s", what, cudaGetErrorString(e));
+    return set_error(e == cudaErrorMemoryAllocation ? SHT_ENOMEM : SHT_ECUDA, g_msg);
+}
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int dev) {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+    }
+    ~DevGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+template <class T>
+cudaError_t alloc(T** p, size_t n) {
+    return cudaMalloc((void**)p, std::max<size_t>(1, n) * sizeof(T));
+}
+void release(sht_mlp* m) {
+    for (int l = 0; l < sht_mlp::NLAYER; ++l) {
+        void* ps[] = {m->W[l], m->b[l], m->Wb[l], m->mW[l], m->vW[l], m->mb[l], m->vb[l], m->dW[l], m->db[l]};
+        for (void* q : ps)
+            if (q) cudaFree(q);
+    }
+    for (int l = 0; l < 3; ++l) {
+        void* ps[] = {m->Z[l], m->A[l], m->dZ[l]};
+        for (void* q : ps)
+            if (q) cudaFree(q);
+    }
+    void* ps[] = {m->X0, m->Y, m->dY, m->xm, m->xs, m->ym, m->ys, m->loss, m->colbuf, m->ybuf, m->plainT, m->plainq,
+                  m->nfallback, m->partial, m->err};
+    for (void* q : ps)
+        if (q) cudaFree(q);
+}
+
+GemmArgs args(sht_mlp* m, int M, int N, int K, int epi) {
+    GemmArgs g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.epi = epi;
+    g.err = m->err;
+    return g;
+}
+
+// forward pass over B rows of X0; keep = store pre-activations
+cudaError_t forward(sht_mlp* m, int B, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    const __nv_bfloat16* in = m->X0;
+    int64_t ld_in = m->in_pad;
+    for (int l = 0; l < 3 && e == cudaSuccess; ++l) {
+        GemmArgs g = args(m, B, m->hidden, m->fan_in[l], EPI_BIAS_GELU);
+        g.out_f32 = m->Z[l];
+        g.ld_f32 = m->hidden;
+        g.out_bf16 = m->A[l];
+        g.ld_bf16 = m->hidden;
+        g.bias = m->b[l];
+        e = gemm(in, ld_in, 0, m->Wb[l], m->fan_in[l], 0, g, s);
+        in = m->A[l];
+        ld_in = m->hidden;
+    }
+    if (e != cudaSuccess) return e;
+    GemmArgs g = args(m, B, m->nout, m->hidden, EPI_BIAS_F32);
+    g.out_f32 = m->Y;
+    g.ld_f32 = m->nout;
+    g.bias = m->b[3];
+    return gemm(in, ld_in, 0, m->Wb[3], m->hidden, 0, g, s);
+}
+}  // namespace
+
+int sht_mlp_create(int batch_capacity, uint64_t seed, int device, sht_mlp** out) {
+    if (!out || batch_capacity < 1) return set_error(SHT_EINVAL, "sht_mlp_create: bad arguments");
+    *out = nullptr;
+    DevGuard dg(device);
+    sht_mlp* m = new sht_mlp();
+    m->device = device;
+    m->cap = (batch_capacity + 127) / 128 * 128;
+    const int fi[4] = {m->in_pad, m->hidden, m->hidden, m->hidden};
+    const int fo[4] = {m->hidden, m->hidden, m->hidden, m->nout};
+    cudaError_t e = cudaSuccess;
+    std::mt19937_64 rng(seed);
+    for (int l = 0; l < 4 && e == cudaSuccess; ++l) {
+        m->fan_in[l] = fi[l];
+        m->fan_out[l] = fo[l];
+        const size_t nw = (size_t)fo[l] * fi[l];
+        const int real_in = l == 0 ? m->nin : fi[l];
+        // He initialisation for GELU layers, Xavier for the output; padded inputs get 0
+        std::normal_distribution<float> nd(0.f, l < 3 ? std::sqrt(2.f / real_in) : std::sqrt(1.f / real_in));
+        std::vector<float> w(nw, 0.f);
+        for (int o = 0; o < fo[l]; ++o)
+            for (int i = 0; i < real_in; ++i) w[(size_t)o * fi[l] + i] = nd(rng);
+        std::vector<float> z(nw, 0.f);
+        if ((e = alloc(&m->W[l], nw)) != cudaSuccess) break;
+        if ((e = cudaMemcpy(m->W[l], w.data(), nw * 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((e = alloc(&m->Wb[l], nw)) != cudaSuccess) break;
+        to_bf16_kernel<<<(unsigned)((nw + 255) / 256), 256>>>(m->W[l], m->Wb[l], (int64_t)nw);
+        if ((e = alloc(&m->mW[l], nw)) == cudaSuccess) e = cudaMemset(m->mW[l], 0, nw * 4);
+        if (e == cudaSuccess && (e = alloc(&m->vW[l], nw)) == cudaSuccess) e = cudaMemset(m->vW[l], 0, nw * 4);
+        if (e == cudaSuccess) e = alloc(&m->dW[l], nw);
+        if (e == cudaSuccess && (e = alloc(&m->b[l], fo[l])) == cudaSuccess) e = cudaMemset(m->b[l], 0, fo[l] * 4);
+        if (e == cudaSuccess && (e = alloc(&m->mb[l], fo[l])) == cudaSuccess) e = cudaMemset(m->mb[l], 0, fo[l] * 4);
+        if (e == cudaSuccess && (e = alloc(&m->vb[l], fo[l])) == cudaSuccess) e = cudaMemset(m->vb[l], 0, fo[l] * 4);
+        if (e == cudaSuccess) e = alloc(&m->db[l], fo[l]);
+    }
+    const size_t cap = m->cap;
+    if (e == cudaSuccess && (e = alloc(&m->X0, cap * m->in_pad)) == cudaSuccess) e = cudaMemset(m->X0, 0, cap * m->in_pad * 2);
+    for (int l = 0; l < 3 && e == cudaSuccess; ++l) {
+        if ((e = alloc(&m->Z[l], cap * m->hidden)) != cudaSuccess) break;
+        if ((e = alloc(&m->A[l], cap * m->hidden)) != cudaSuccess) break;
+        e = alloc(&m->dZ[l], cap * m->hidden);
+    }
+    if (e == cudaSuccess) e = alloc(&m->Y, cap * m->nout);
+    if (e == cudaSuccess) e = alloc(&m->dY, cap * m->nout);
+    if (e == cudaSuccess) e = alloc(&m->xm, m->nin);
+    if (e == cudaSuccess) e = alloc(&m->xs, m->nin);
+    if (e == cudaSuccess) e = alloc(&m->ym, m->nout);
+    if (e == cudaSuccess) e = alloc(&m->ys, m->nout);
+    if (e == cudaSuccess) e = alloc(&m->loss, 1);
+    if (e == cudaSuccess) e = alloc(&m->colbuf, cap * m->nin);
+    if (e == cudaSuccess) e = alloc(&m->ybuf, cap * m->nout);
+    if (e == cudaSuccess) e = alloc(&m->plainT, cap * NLC);
+    if (e == cudaSuccess) e = alloc(&m->plainq, cap * NLC);
+    if (e == cudaSuccess) e = alloc(&m->nfallback, 1);
+    if (e == cudaSuccess) e = alloc(&m->partial, (cap / BIAS_ROWS + 1) * m->hidden);
+    if (e == cudaSuccess && (e = alloc(&m->err, 1)) == cudaSuccess) e = cudaMemset(m->err, 0, 4);
+    if (e == cudaSuccess) {          // identity normalisation until set
+        std::vector<float> zero(m->nin, 0.f), one(m->nin, 1.f);
+        cudaMemcpy(m->xm, zero.data(), m->nin * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(m->xs, one.data(), m->nin * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(m->ym, zero.data(), m->nout * 4, cudaMemcpyHostToDevice);
+        e = cudaMemcpy(m->ys, one.data(), m->nout * 4, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        release(m);
+        delete m;
+        return mcuda(e, "sht_mlp_create");
+    }
+    *out = m;
+    return SHT_OK;
+}
+
+int sht_mlp_set_normalization(sht_mlp* m, const float* x_mean, const float* x_std, const float* y_mean,
+                              const float* y_std) {
+    if (!m || !x_mean || !x_std || !y_mean || !y_std) return set_error(SHT_EINVAL, "sht_mlp_set_normalization: NULL");
+    for (int i = 0; i < m->nin; ++i)
+        if (!(x_std[i] > 0)) return set_error(SHT_EINVAL, "sht_mlp_set_normalization: std must be > 0");
+    for (int i = 0; i < m->nout; ++i)
+        if (!(y_std[i] > 0)) return set_error(SHT_EINVAL, "sht_mlp_set_normalization: std must be > 0");
+    DevGuard dg(m->device);
+    cudaError_t e = cudaMemcpy(m->xm, x_mean, m->nin * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(m->xs, x_std, m->nin * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(m->ym, y_mean, m->nout * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(m->ys, y_std, m->nout * 4, cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_set_normalization");
+}
+
+int sht_mlp_train_step(sht_mlp* m, const float* x, const float* y, int B, float lr, void* stream) {
+    if (!m || !x || !y) return set_error(SHT_EINVAL, "sht_mlp_train_step: NULL argument");
+    if (B < 1 || B > m->cap) return set_error(SHT_EINVAL, "sht_mlp_train_step: batch outside 1 .. capacity");
+    DevGuard dg(m->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(m->loss, 0, 4, s);
+    const int64_t nx = (int64_t)B * m->in_pad;
+    normalize_in_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, s>>>(x, m->nin, B, m->nin, m->xm, m->xs, m->X0,
+                                                                     m->in_pad);
+    if (e == cudaSuccess) e = forward(m, B, s);
+    const int64_t ny = (int64_t)B * m->nout;
+    if (e == cudaSuccess)
+        output_grad_kernel<<<(unsigned)((ny + 255) / 256), 256, 0, s>>>(m->Y, y, B, m->nout, m->ym, m->ys, m->dY,
+                                                                         m->loss);
+    // backward: layer 3 (output), then the hidden layers
+    const __nv_bfloat16* act[4] = {m->X0, m->A[0], m->A[1], m->A[2]};
+    const int64_t ld_act[4] = {m->in_pad, m->hidden, m->hidden, m->hidden};
+    const __nv_bfloat16* dz = m->dY;
+    int64_t ld_dz = m->nout;
+    for (int l = 3; l >= 0 && e == cudaSuccess; --l) {
+        const int fo = m->fan_out[l], fi = m->fan_in[l];
+        // dW[l] [fo][fi] = dz^T act[l]   (A = dz MN-major, B = act MN-major)
+        GemmArgs gw = args(m, fo, fi, B, EPI_F32);
+        gw.out_f32 = m->dW[l];
+        gw.ld_f32 = fi;
+        e = gemm(dz, ld_dz, 1, act[l], ld_act[l], 1, gw, s);
+        if (e != cudaSuccess) break;
+        const int P = (B + BIAS_ROWS - 1) / BIAS_ROWS;
+        bias_partial_kernel<<<dim3((fo + 127) / 128, P), 128, 0, s>>>(dz, B, fo, ld_dz, m->partial);
+        bias_final_kernel<<<(fo + 127) / 128, 128, 0, s>>>(m->partial, P, fo, m->db[l]);
+        if (l == 0) break;
+        // dZ[l-1] = (dz W[l]) * GELU'(Z[l-1])   (A = dz K-major, B = W[l] [fo][fi] MN-major)
+        GemmArgs gd = args(m, B, fi, fo, EPI_GELU_BWD);
+        gd.out_bf16 = m->dZ[l - 1];
+        gd.ld_bf16 = m->hidden;
+        gd.zin = m->Z[l - 1];
+        gd.ld_z = m->hidden;
+        e = gemm(dz, ld_dz, 0, m->Wb[l], fi, 1, gd, s);
+        dz = m->dZ[l - 1];
+        ld_dz = m->hidden;
+    }
+    // Adam
+    ++m->step;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)m->step), c2 = 1.f - std::pow(b2, (float)m->step);
+    for (int l = 0; l < 4 && e == cudaSuccess; ++l) {
+        const int64_t nw = (int64_t)m->fan_out[l] * m->fan_in[l];
+        adam_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(m->W[l], m->dW[l], m->mW[l], m->vW[l], m->Wb[l], nw, lr,
+                                                                 b1, b2, c1, c2, 1e-8f);
+        adam_kernel<<<(m->fan_out[l] + 255) / 256, 256, 0, s>>>(m->b[l], m->db[l], m->mb[l], m->vb[l], nullptr,
+                                                                m->fan_out[l], lr, b1, b2, c1, c2, 1e-8f);
+        e = cudaGetLastError();
+    }
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_train_step");
+}
+
+int sht_mlp_infer(sht_mlp* m, const float* x, float* y, int B, void* stream) {
+    if (!m || !x || !y) return set_error(SHT_EINVAL, "sht_mlp_infer: NULL argument");
+    if (B < 0 || B > m->cap) return set_error(SHT_EINVAL, "sht_mlp_infer: batch outside 0 .. capacity");
+    if (B == 0) return SHT_OK;
+    DevGuard dg(m->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t nx = (int64_t)B * m->in_pad;
+    normalize_in_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, s>>>(x, m->nin, B, m->nin, m->xm, m->xs, m->X0,
+                                                                     m->in_pad);
+    cudaError_t e = forward(m, B, s);
+    const int64_t ny = (int64_t)B * m->nout;
+    if (e == cudaSuccess)
+        denormalize_kernel<<<(unsigned)((ny + 255) / 256), 256, 0, s>>>(m->Y, B, m->nout, m->ym, m->ys, y, m->nout);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_infer");
+}
+
+int sht_mlp_loss(sht_mlp* m, float* loss) {
+    if (!m || !loss) return set_error(SHT_EINVAL, "sht_mlp_loss: NULL argument");
+    DevGuard dg(m->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(loss, m->loss, 4, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_loss");
+}
+
+int sht_mlp_params(sht_mlp* m, int layer, float* w, float* b, int set) {
+    if (!m || layer < 0 || layer >= 4) return set_error(SHT_EINVAL, "sht_mlp_params: bad layer");
+    DevGuard dg(m->device);
+    const size_t nw = (size_t)m->fan_out[layer] * m->fan_in[layer];
+    cudaError_t e = cudaSuccess;
+    if (set) {
+        if (w) e = cudaMemcpy(m->W[layer], w, nw * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && b) e = cudaMemcpy(m->b[layer], b, m->fan_out[layer] * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) to_bf16_kernel<<<(unsigned)((nw + 255) / 256), 256>>>(m->W[layer], m->Wb[layer], nw);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    } else {
+        if (w) e = cudaMemcpy(w, m->W[layer], nw * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && b) e = cudaMemcpy(b, m->b[layer], m->fan_out[layer] * 4, cudaMemcpyDeviceToHost);
+    }
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_params");
+}
+
+int sht_column_emulate(sht_mlp* m, const float* temp, const float* humid, const float* u, const float* v,
+                       const float* surface_pressure, int64_t ld, int ncol, double dt, double z_max, float* dtemp,
+                       float* dhumid, unsigned flags, int32_t* nfallback, void* stream) {
+    if (!m || !temp || !humid || !u || !v || !surface_pressure || !dtemp || !dhumid)
+        return set_error(SHT_EINVAL, "sht_column_emulate: NULL argument");
+    if (ncol < 0 || ncol > m->cap || ld < ncol)
+        return set_error(SHT_EINVAL, "sht_column_emulate: DimensionMismatch: ncol outside capacity or ld < ncol");
+    if (ncol == 0) return SHT_OK;
+    DevGuard dg(m->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    gather_columns_kernel<<<(ncol + 127) / 128, 128, 0, s>>>(temp, humid, u, v, surface_pressure, ld, ncol,
+                                                             m->colbuf);
+    int rc = sht_mlp_infer(m, m->colbuf, m->ybuf, ncol, stream);
+    if (rc != SHT_OK) return rc;
+    cudaError_t e = launch_column_physics(temp, humid, surface_pressure, ld, ncol, (float)dt, m->plainT, m->plainq,
+                                          ncol, false, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->nfallback, 0, 4, s);
+    if (e == cudaSuccess)
+        scatter_columns_kernel<<<(ncol + 127) / 128, 128, 0, s>>>(m->colbuf, m->xm, m->xs, (float)z_max, m->ybuf,
+                                                                  m->plainT, m->plainq, ld, ncol, dtemp, dhumid,
+                                                                  (flags & SHT_ADD) ? 1 : 0, m->nfallback);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess && nfallback) {
+        e = cudaMemcpyAsync(nfallback, m->nfallback, 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_column_emulate");
+}
+
+int sht_mlp_device_status(sht_mlp* m, int32_t* status) {
+    if (!m || !status) return set_error(SHT_EINVAL, "sht_mlp_device_status: NULL argument");
+    DevGuard dg(m->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(status, m->err, 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemset(m->err, 0, 4);
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_device_status");
+}
+
+int sht_mlp_destroy(sht_mlp* m) {
+    if (!m) return SHT_OK;
+    DevGuard dg(m->device);
+    release(m);
+    delete m;
+    return SHT_OK;
+}
+
+// A general BF16 matrix product on the tensor cores (the MLP's building block):
+// C [M][ldc] FP32 = A B, A [M][K] (a_mn = 0: stored [M][lda]; 1: stored [K][lda]) and
+// B [K][N] (b_mn = 0: stored [N][ldb]; 1: stored [K][ldb]); leading dimensions in elements,
+// multiples of 8.
+int sht_bf16_gemm(const void* A, int64_t lda, int a_mn, const void* B, int64_t ldb, int b_mn, float* C, int64_t ldc,
+                  int M, int N, int K, int32_t* device_error, void* stream) {
+    if (!A || !B || !C || !device_error) return set_error(SHT_EINVAL, "sht_bf16_gemm: NULL argument");
+    if (M < 0 || N < 0 || K < 0 || ldc < N || (lda % 8) || (ldb % 8))
+        return set_error(SHT_EINVAL, "sht_bf16_gemm: DimensionMismatch: sizes or leading dimensions");
+    GemmArgs g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.epi = EPI_F32;
+    g.out_f32 = C;
+    g.ld_f32 = ldc;
+    g.err = device_error;
+    const cudaError_t e = gemm((const __nv_bfloat16*)A, lda, a_mn, (const __nv_bfloat16*)B, ldb, b_mn, g,
+                               (cudaStream_t)stream);
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_bf16_gemm");
+}

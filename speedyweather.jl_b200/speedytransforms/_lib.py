@@ -73,6 +73,18 @@ SIGNATURES = {
     "sht_matrix_analyze": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
     "sht_matrix_device_status": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "sht_matrix_destroy": (C.c_int, [_P]),
+    "sht_column_physics": (C.c_int, [_P, _P, _P, _I64, C.c_int, C.c_int, C.c_double, _P, _P, C.c_uint, _P]),
+    "sht_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_void_p)]),
+    "sht_mlp_set_normalization": (C.c_int, [_P, _P, _P, _P, _P]),
+    "sht_mlp_train_step": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, _P]),
+    "sht_mlp_loss": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "sht_mlp_infer": (C.c_int, [_P, _P, _P, C.c_int, _P]),
+    "sht_mlp_params": (C.c_int, [_P, C.c_int, _P, _P, C.c_int]),
+    "sht_column_emulate": (C.c_int, [_P, _P, _P, _P, _P, _P, _I64, C.c_int, C.c_double, C.c_double, _P, _P, C.c_uint,
+                                     C.POINTER(C.c_int32), _P]),
+    "sht_mlp_device_status": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "sht_mlp_destroy": (C.c_int, [_P]),
+    "sht_bf16_gemm": (C.c_int, [_P, _I64, C.c_int, _P, _I64, C.c_int, _P, _I64, C.c_int, C.c_int, C.c_int, _P, _P]),
     "sht_last_error": (C.c_char_p, []),
     "sht_version": (C.c_char_p, []),
 }

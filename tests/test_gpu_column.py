@@ -1,0 +1,159 @@
+"""Column physics kernel, the tcgen05 BF16 GEMM, and the MLP column emulator.
+
+* sht_column_physics vs the FP32 mode of the column oracle: the schemes branch on
+  thresholds (condensation onset, convective criteria), so FP32 rounding can flip a
+  borderline column; >= 99.5 % of the columns must agree to 1e-3 of the tendency scale.
+* sht_bf16_gemm vs numpy on BF16-rounded operands for all four operand layouts, ragged
+  sizes (FP32 accumulation: relative 1e-5).
+* the MLP: forward pass vs numpy with the downloaded parameters (BF16 weights and
+  activations: relative 2e-2), training reduces the loss on columns labelled by the plain
+  physics, and the emulator falls back to the plain physics bit for bit outside its range.
+"""
+import numpy as np
+import pytest
+
+import column_oracle as CO
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sp():
+    import speedyphysics as sp
+    return sp
+
+
+def to_dev(a):
+    import torch
+    return torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device="cuda")
+
+
+def test_column_physics_vs_oracle(sp):
+    import torch
+    T, q, u, v, ps = CO.synthetic_columns(4096, seed=11)
+    dT = torch.zeros((8, 4096), device="cuda")
+    dq = torch.zeros((8, 4096), device="cuda")
+    sp.column_physics_(dT, dq, to_dev(T.T), to_dev(q.T), to_dev(ps))
+    torch.cuda.synchronize()
+    rT, rq = CO.column_tendencies(T, q, ps, dtype=np.float32)
+    gT, gq = dT.cpu().numpy().T, dq.cpu().numpy().T
+    okT = np.all(np.abs(gT - rT) <= 1e-3 * np.abs(rT).max(), axis=1)
+    okq = np.all(np.abs(gq - rq) <= 1e-3 * np.abs(rq).max(), axis=1)
+    print("column physics: fraction of columns within 1e-3:", (okT & okq).mean())
+    assert (okT & okq).mean() >= 0.995
+    # add accumulates
+    sp.column_physics_(dT, dq, to_dev(T.T), to_dev(q.T), to_dev(ps), add=True)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(dT.cpu().numpy().T, 2 * gT, rtol=1e-6, atol=1e-12)
+
+
+def bf16(a):
+    import torch
+    return torch.tensor(a, dtype=torch.float32).to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("a_mn,b_mn", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K", [(300, 256, 64), (130, 16, 256), (256, 64, 1000), (64, 200, 16)])
+def test_bf16_gemm_layouts(sp, a_mn, b_mn, M, N, K):
+    import torch
+    rng = np.random.default_rng(M + N + K)
+    A = rng.standard_normal((M, K)).astype(np.float32)
+    B = rng.standard_normal((K, N)).astype(np.float32)
+    pad = lambda x: x if x % 8 == 0 else x + 8 - x % 8   # noqa: E731
+    At = np.zeros((K, pad(M)), np.float32) if a_mn else np.zeros((M, pad(K)), np.float32)
+    if a_mn:
+        At[:, :M] = A.T
+    else:
+        At[:, :K] = A
+    Bt = np.zeros((K, pad(N)), np.float32) if b_mn else np.zeros((N, pad(K)), np.float32)
+    if b_mn:
+        Bt[:, :N] = B
+    else:
+        Bt[:, :K] = B.T
+    Ad, Bd = bf16(At).cuda(), bf16(Bt).cuda()
+    C, err = sp.bf16_gemm(Ad, a_mn, Bd, b_mn, M, N, K)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    Ar = Ad.float().cpu().numpy()
+    Br = Bd.float().cpu().numpy()
+    Aref = Ar[:, :M].T if a_mn else Ar[:, :K]
+    Bref = Br[:, :N] if b_mn else Br[:, :K].T
+    ref = Aref.astype(np.float64) @ Bref.astype(np.float64)
+    assert np.linalg.norm(C.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-5
+
+
+def gelu(x):
+    from math import sqrt
+    import scipy.special
+    return 0.5 * x * (1 + scipy.special.erf(x / sqrt(2)))
+
+
+@pytest.fixture(scope="module")
+def trained(sp):
+    """An emulator trained on 64k synthetic columns labelled by the GPU plain physics."""
+    import torch
+    n = 65536
+    T, q, u, v, ps = CO.synthetic_columns(n, seed=21)
+    Td, qd, ud, vd, psd = (to_dev(T.T), to_dev(q.T), to_dev(u.T), to_dev(v.T), to_dev(ps))
+    dT = torch.zeros((8, n), device="cuda")
+    dq = torch.zeros((8, n), device="cuda")
+    sp.column_physics_(dT, dq, Td, qd, psd)
+    x = sp.columns_as_rows(Td, qd, ud, vd, psd)
+    y = torch.cat([dT.T, dq.T], dim=1).contiguous()
+    em = sp.ColumnEmulator(8192, seed=3)
+    em.fit_normalization(x, y)
+    losses = em.train(x, y, epochs=4, batch=1024, lr=2e-3)
+    return em, losses, x, y
+
+
+def test_mlp_forward_matches_numpy(sp, trained):
+    import torch
+    em, _, x, _ = trained
+    xs = x[:512]
+    out = em.infer(xs).cpu().numpy().astype(np.float64)
+    z = (xs.cpu().numpy().astype(np.float64) - em.x_mean) / em.x_std
+    h = np.zeros((512, 64))
+    h[:, :33] = torch.tensor(z, dtype=torch.float32).to(torch.bfloat16).float().numpy()
+    for layer in range(4):
+        w, b = em.params(layer)
+        wb = torch.tensor(w).to(torch.bfloat16).float().numpy().astype(np.float64)
+        h = h @ wb.T + b
+        if layer < 3:
+            h = torch.tensor(gelu(h), dtype=torch.float32).to(torch.bfloat16).float().numpy().astype(np.float64)
+    ref = h * em.y_std + em.y_mean
+    rel = np.linalg.norm(out - ref) / np.linalg.norm(ref)
+    print("mlp forward vs numpy:", rel)
+    assert rel < 2e-2
+    assert em.device_status() == 0
+
+
+def test_mlp_training_reduces_loss(trained):
+    em, losses, x, y = trained
+    print("losses per epoch:", losses)
+    assert losses[-1] < 0.5 * losses[0]
+    assert np.isfinite(losses).all()
+
+
+def test_emulator_parameterization_and_fallback(sp, trained):
+    import torch
+    em, _, _, _ = trained
+    n = 4096
+    T, q, u, v, ps = CO.synthetic_columns(n, seed=99)
+    T[: n // 4] += 80.0                          # far outside the training range
+    Td, qd, ud, vd, psd = (to_dev(T.T), to_dev(q.T), to_dev(u.T), to_dev(v.T), to_dev(ps))
+    dT = torch.zeros((8, n), device="cuda")
+    dq = torch.zeros((8, n), device="cuda")
+    nf = em.parameterization_(dT, dq, Td, qd, ud, vd, psd, z_max=5.0)
+    pT = torch.zeros((8, n), device="cuda")
+    pq = torch.zeros((8, n), device="cuda")
+    sp.column_physics_(pT, pq, Td, qd, psd)
+    torch.cuda.synchronize()
+    assert nf >= n // 4
+    gT, gq = dT.cpu().numpy(), dq.cpu().numpy()
+    np.testing.assert_array_equal(gT[:, : n // 4], pT.cpu().numpy()[:, : n // 4])
+    np.testing.assert_array_equal(gq[:, : n // 4], pq.cpu().numpy()[:, : n // 4])
+    # in range: the emulator, judged by the plain physics (relative RMS over the columns)
+    ref = pT.cpu().numpy()[:, n // 4:]
+    err = np.linalg.norm(gT[:, n // 4:] - ref) / np.linalg.norm(ref)
+    print("emulator vs plain physics (relative L2 of dT/dt):", err, "fallbacks:", nf)
+    assert err < 0.5
