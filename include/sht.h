@@ -296,19 +296,23 @@ SHT_API int sht_mlp_create(int batch_capacity, uint64_t seed, int device, sht_ml
 /* per-input / per-output mean and standard deviation (host arrays of 33 and 16) */
 SHT_API int sht_mlp_set_normalization(sht_mlp* m, const float* x_mean, const float* x_std, const float* y_mean,
                                       const float* y_std);
+/* loss and parameter gradients over B rows (no update): the mean squared error of the
+ * normalised outputs, mean over B x 16 */
+SHT_API int sht_mlp_backward(sht_mlp* m, const float* x, const float* y, int B, void* stream);
 /* one Adam step (lr) on the mean squared error of the normalised outputs over B rows */
 SHT_API int sht_mlp_train_step(sht_mlp* m, const float* x, const float* y, int B, float lr, void* stream);
-/* the last train step's loss (synchronises) */
+/* the last backward pass's loss (synchronises) */
 SHT_API int sht_mlp_loss(sht_mlp* m, float* loss);
 SHT_API int sht_mlp_infer(sht_mlp* m, const float* x, float* y, int B, void* stream);
 /* layer 0..3 parameters as FP32 host arrays (w [out][in], in = 64 for layer 0 with inputs
- * 33..63 zero, 256 otherwise; b [out]); set = 1 uploads, 0 downloads */
+ * 33..63 zero, 256 otherwise; b [out]); set = 1 uploads, 0 downloads, 2 downloads the
+ * gradients of the last backward pass (synchronises) */
 SHT_API int sht_mlp_params(sht_mlp* m, int layer, float* w, float* b, int set);
 /* The emulator as a parameterization: gathers the columns of layer-major fields
  * (x[k ld + ij]), runs the network, and writes its tendencies for columns whose every
  * normalised input lies within z_max of the training mean, the plain parameterizations'
  * (sht_column_physics, dt) otherwise; *nfallback (if not NULL; synchronises) counts the
- * latter. flags: SHT_ADD. */
+ * latter. flags: SHT_ADD. Any ncol: columns beyond the batch capacity run in chunks. */
 SHT_API int sht_column_emulate(sht_mlp* m, const float* temp, const float* humid, const float* u, const float* v,
                                const float* surface_pressure, int64_t ld, int ncol, double dt, double z_max,
                                float* dtemp, float* dhumid, unsigned flags, int32_t* nfallback, void* stream);

@@ -19,6 +19,11 @@ Follows, per column (vectorised over columns; FP64 by default, FP32 with dtype=f
 
 Parity with the reference's own runs is unpinned (no Julia toolchain here); the
 restatement is pinned by the invariants in tests/test_column_oracle.py.
+
+The MLP emulator (no counterpart in the reference) has its forward and backward pass
+restated here too (mlp_forward, mlp_backward): FP64 arithmetic with BF16 rounding at the
+points where the CUDA kernels store BF16 (normalised inputs, weights, hidden activations,
+output and hidden gradients), or exact FP64 (bf16=False), which finite differences pin.
 """
 from __future__ import annotations
 
@@ -207,3 +212,54 @@ def synthetic_columns(ncol: int, seed: int = 0, nlayers: int = 8):
     v = rng.normal(0, 4, (ncol, nlayers))
     return (T.astype(np.float32), q.astype(np.float32), u.astype(np.float32), v.astype(np.float32),
             ps.astype(np.float32))
+
+
+# ---- MLP emulator: 33 -> 256 -> 256 -> 256 (GELU) -> 16 ----------------------------
+def bf16_round(a):
+    """Round to the nearest BF16 (ties to even), returned as float64."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def gelu(x):
+    from scipy.special import erf
+    return 0.5 * x * (1 + erf(x / np.sqrt(2.0)))
+
+
+def gelu_grad(x):
+    from scipy.special import erf
+    return 0.5 * (1 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2 * np.pi)
+
+
+def mlp_forward(params, xn, bf16=True):
+    """params: [(w [out][in], b [out])] * 4 with in = 64 for the first layer (inputs
+    padded with zeros); xn [B, 33] normalised inputs. Returns (Y, cache)."""
+    r = bf16_round if bf16 else (lambda a: np.asarray(a, np.float64))
+    B = xn.shape[0]
+    a = np.zeros((B, params[0][0].shape[1]))
+    a[:, :xn.shape[1]] = xn
+    a = r(a)
+    acts, zs = [a], []
+    for layer, (w, b) in enumerate(params):
+        z = a @ r(w).T + np.asarray(b, np.float64)
+        if layer == len(params) - 1:
+            return z, (acts, zs)
+        zs.append(z)
+        a = r(gelu(z))
+        acts.append(a)
+
+
+def mlp_backward(params, xn, yn, bf16=True):
+    """Loss = mean over B x 16 of (Y - yn)^2 and its gradients [(dW, db)] * 4."""
+    r = bf16_round if bf16 else (lambda a: np.asarray(a, np.float64))
+    Y, (acts, zs) = mlp_forward(params, xn, bf16)
+    d = Y - yn
+    loss = float(np.mean(d * d))
+    dz = r(2 * d / d.size)
+    grads = [None] * len(params)
+    for layer in range(len(params) - 1, -1, -1):
+        grads[layer] = (dz.T @ acts[layer], dz.sum(0))
+        if layer > 0:
+            dz = r((dz @ r(params[layer][0])) * gelu_grad(zs[layer - 1]))
+    return loss, grads

@@ -26,8 +26,10 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <vector>
 
@@ -44,7 +46,7 @@ using namespace sht::tcx;
 
 namespace {
 
-constexpr int G_THREADS = 192;
+constexpr int G_THREADS = 320;                 // producer warp, MMA warp, 8 epilogue warps
 constexpr int G_BOX = 64;                       // TMA box edge (elements) = K block
 constexpr int G_BOX_BYTES = G_BOX * G_BOX * 2;  // 8 KB
 constexpr int G_STAGES = 3;
@@ -63,30 +65,42 @@ struct GemmArgs {
     const float* zin;               // EPI_GELU_BWD: pre-activation [M][ld_z]
     int64_t ld_z;
     int32_t* err;
+    int kb_per_split;               // K blocks of 64 per CTA along grid z (split K; EPI_F32 only)
+    int64_t split_stride;           // elements between the partial products of consecutive splits
 };
+constexpr int G_EPI_LD = 33;        // epilogue transpose tile [32 rows][33]
+constexpr int G_EPI_BYTES = 8 * 32 * G_EPI_LD * 4;
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float x) {
     return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.3989422804014327f * expf(-0.5f * x * x);
 }
 
-// One 128 x NT output tile per CTA (NT = N rounded up to 16, <= 256).
-__global__ void __launch_bounds__(G_THREADS, 1)
+// One 128 x nt output tile per CTA (nt a multiple of 16, <= 256; tile y covers columns
+// [nt y, nt y + nt)) over the K blocks [z kb_per_split, (z + 1) kb_per_split) of grid
+// slice z. The epilogue transposes each 32 x 32 block of the accumulator through shared
+// memory (the stage buffers, free once the accumulator is complete) so that a warp's
+// stores cover consecutive columns of one row (coalesced), then applies the fused
+// operation to 32 independent rows at a time.
+__global__ void __launch_bounds__(G_THREADS, 2)
     bf16_gemm_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      const GemmArgs g, int nt, uint32_t tmem_cols) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * 256;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * nt;
+    const int kb0 = blockIdx.z * g.kb_per_split;
     const int nbox_b = (nt + G_BOX - 1) / G_BOX;
     const int a_bytes = 2 * G_BOX_BYTES;
     const int stage_bytes = a_bytes + nbox_b * G_BOX_BYTES;
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + (size_t)G_STAGES * stage_bytes);
     uint64_t* empty_bar = full_bar + G_STAGES;
-    uint64_t* acc_bar = empty_bar + G_STAGES;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_bar + 1);
+    uint64_t* acc_bar = empty_bar + G_STAGES;      // accumulator complete: the epilogue may start
+    uint64_t* mma_bar = acc_bar + 1;               // every issued MMA complete (also after an abort)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    const int nk = (g.K + G_BOX - 1) / G_BOX;
+    float* epi_tile = reinterpret_cast<float*>(smem);
+    const int nk = min((g.K + G_BOX - 1) / G_BOX - kb0, g.kb_per_split);   // >= 1 by construction
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < G_STAGES; ++s) {
@@ -94,6 +108,7 @@ __global__ void __launch_bounds__(G_THREADS, 1)
             mbar_init(&empty_bar[s], 1);
         }
         mbar_init(acc_bar, 1);
+        mbar_init(mma_bar, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -120,17 +135,18 @@ __global__ void __launch_bounds__(G_THREADS, 1)
             }
             uint8_t* st = smem + (size_t)s * stage_bytes;
             mbar_expect_tx(&full_bar[s], (uint32_t)stage_bytes);
+            const int kx = (kb0 + kb) * G_BOX;
             for (int h = 0; h < 2; ++h) {   // A: rows (K-major) or columns (MN-major) m0 + 64 h
                 if (g.a_mn)
-                    tma_load_2d(st + h * G_BOX_BYTES, &map_a, m0 + h * G_BOX, kb * G_BOX, &full_bar[s]);
+                    tma_load_2d(st + h * G_BOX_BYTES, &map_a, m0 + h * G_BOX, kx, &full_bar[s]);
                 else
-                    tma_load_2d(st + h * G_BOX_BYTES, &map_a, kb * G_BOX, m0 + h * G_BOX, &full_bar[s]);
+                    tma_load_2d(st + h * G_BOX_BYTES, &map_a, kx, m0 + h * G_BOX, &full_bar[s]);
             }
             for (int h = 0; h < nbox_b; ++h) {
                 if (g.b_mn)
-                    tma_load_2d(st + a_bytes + h * G_BOX_BYTES, &map_b, n0 + h * G_BOX, kb * G_BOX, &full_bar[s]);
+                    tma_load_2d(st + a_bytes + h * G_BOX_BYTES, &map_b, n0 + h * G_BOX, kx, &full_bar[s]);
                 else
-                    tma_load_2d(st + a_bytes + h * G_BOX_BYTES, &map_b, kb * G_BOX, n0 + h * G_BOX, &full_bar[s]);
+                    tma_load_2d(st + a_bytes + h * G_BOX_BYTES, &map_b, kx, n0 + h * G_BOX, &full_bar[s]);
             }
         }
         // no copy may still land after the CTA exits
@@ -157,12 +173,17 @@ __global__ void __launch_bounds__(G_THREADS, 1)
             }
             umma_commit(&empty_bar[s]);
         }
-        umma_commit(acc_bar);
-        if (!mbar_wait(acc_bar, 0)) atomicExch(g.err, 14);     // all MMAs done before the dealloc
+        // after an abort the epilogue is not released (its bounded wait expires): copies may
+        // still land in the stage buffers it would reuse
+        if (!*abort_flag) umma_commit(acc_bar);
+        umma_commit(mma_bar);
+        if (!mbar_wait(mma_bar, 0)) atomicExch(g.err, 14);     // all MMAs done before the dealloc
     } else if (warp >= 2) {
-        // ---- epilogue: thread = output row
-        const int quarter = warp % 4;
-        const int row = m0 + quarter * 32 + lane;
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows); each 32 x 32
+        // block goes through a padded shared tile so that lane = column for the stores
+        const int quarter = warp % 4, half = (warp - 2) / 4;   // TMEM lanes 32 quarter.., column chunks half, half + 2, ..
+        const int rbase = m0 + quarter * 32;
+        float* tile = epi_tile + (warp - 2) * 32 * G_EPI_LD;
         const bool ok = __all_sync(0xffffffffu, mbar_wait(acc_bar, 0));
         if (!ok) {
             *abort_flag = 1;
@@ -170,32 +191,42 @@ __global__ void __launch_bounds__(G_THREADS, 1)
         }
         tc_fence_after();
         const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
-        for (int c0 = 0; c0 < nt; c0 += 32) {
+        float* out_f32 = g.out_f32 ? g.out_f32 + (int64_t)blockIdx.z * g.split_stride : nullptr;
+        const int rows = min(32, g.M - rbase);
+        for (int c0 = 32 * half; c0 < nt; c0 += 64) {
             float v[32];
             tmem_ld32(taddr + c0, v);
-            if (!ok || row >= g.M) continue;
+            if (!ok || rows <= 0) continue;
 #pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                const int n = n0 + c0 + q;
-                if (c0 + q >= nt || n >= g.N) break;
-                float x = v[q];
-                switch (g.epi) {
-                    case EPI_F32:
-                        g.out_f32[(int64_t)row * g.ld_f32 + n] = x;
-                        break;
-                    case EPI_BIAS_F32:
-                        g.out_f32[(int64_t)row * g.ld_f32 + n] = x + g.bias[n];
-                        break;
-                    case EPI_BIAS_GELU:
-                        x += g.bias[n];
-                        if (g.out_f32) g.out_f32[(int64_t)row * g.ld_f32 + n] = x;
-                        g.out_bf16[(int64_t)row * g.ld_bf16 + n] = __float2bfloat16_rn(gelu(x));
-                        break;
-                    default:   // EPI_GELU_BWD
-                        g.out_bf16[(int64_t)row * g.ld_bf16 + n] =
-                            __float2bfloat16_rn(x * gelu_grad(g.zin[(int64_t)row * g.ld_z + n]));
-                        break;
+            for (int q = 0; q < 32; ++q) tile[lane * G_EPI_LD + q] = v[q];
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < 32; ++r) v[r] = tile[r * G_EPI_LD + lane];   // v[r] = (row rbase + r, column lane)
+            __syncwarp();
+            const int n = n0 + c0 + lane;
+            if (c0 + lane >= nt || n >= g.N) continue;
+            const float bias = g.bias ? g.bias[n] : 0.f;
+            const int64_t base = (int64_t)rbase;
+            if (g.epi == EPI_F32 || g.epi == EPI_BIAS_F32) {
+#pragma unroll
+                for (int r = 0; r < 32; ++r)
+                    if (r < rows) out_f32[(base + r) * g.ld_f32 + n] = v[r] + bias;
+            } else if (g.epi == EPI_BIAS_GELU) {
+                if (out_f32) {
+#pragma unroll
+                    for (int r = 0; r < 32; ++r)
+                        if (r < rows) out_f32[(base + r) * g.ld_f32 + n] = v[r] + bias;
                 }
+#pragma unroll
+                for (int r = 0; r < 32; ++r)
+                    if (r < rows) g.out_bf16[(base + r) * g.ld_bf16 + n] = __float2bfloat16_rn(gelu(v[r] + bias));
+            } else {   // EPI_GELU_BWD
+                float z[32];
+#pragma unroll
+                for (int r = 0; r < 32; ++r) z[r] = r < rows ? g.zin[(base + r) * g.ld_z + n] : 0.f;
+#pragma unroll
+                for (int r = 0; r < 32; ++r)
+                    if (r < rows) g.out_bf16[(base + r) * g.ld_bf16 + n] = __float2bfloat16_rn(v[r] * gelu_grad(z[r]));
             }
         }
     }
@@ -223,28 +254,68 @@ bool make_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols, in
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Dynamic shared memory of a launch with an N tile of nt columns; the kernel's limit is
+// raised once per device to the largest (nt = 256).
+int gemm_smem(int nt) {
+    const int stage_bytes = 2 * G_BOX_BYTES + ((nt + G_BOX - 1) / G_BOX) * G_BOX_BYTES;
+    static_assert(G_EPI_BYTES <= G_STAGES * 3 * G_BOX_BYTES, "the epilogue tiles live in the stage buffers");
+    return 1024 + G_STAGES * stage_bytes + 256;
+}
+cudaError_t gemm_attributes() {
+    static std::mutex mu;
+    static std::vector<bool> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)done.size() <= dev) done.resize(dev + 1, false);
+    if (done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(bf16_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem(256));
+    if (e == cudaSuccess) done[dev] = true;
+    return e;
+}
+
 // C = A B with A [M][K] (a_mn = 0: stored [M][lda], K contiguous; 1: stored [K][lda],
 // M contiguous) and B [K][N] (b_mn = 0: stored [N][ldb]; 1: stored [K][ldb]).
+// ksplit > 1 (EPI_F32 only) splits K over grid z; slice z writes its partial product to
+// g.out_f32 + z g.split_stride, which the caller reduces.
 cudaError_t gemm(const __nv_bfloat16* A, int64_t lda, int a_mn, const __nv_bfloat16* B, int64_t ldb, int b_mn,
-                 GemmArgs g, cudaStream_t s) {
+                 GemmArgs g, cudaStream_t s, int ksplit = 1, int* nz_out = nullptr) {
     if (g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaSuccess;
     if ((lda * 2) % 16 || (ldb * 2) % 16) return cudaErrorInvalidValue;   // TMA row pitch
     CUtensorMap ma, mb;
     const bool ok_a = a_mn ? make_map(&ma, A, g.K, g.M, lda) : make_map(&ma, A, g.M, g.K, lda);
     const bool ok_b = b_mn ? make_map(&mb, B, g.K, g.N, ldb) : make_map(&mb, B, g.N, g.K, ldb);
     if (!ok_a || !ok_b) return cudaErrorInvalidValue;
+    const cudaError_t ea = gemm_attributes();
+    if (ea != cudaSuccess) return ea;
     g.a_mn = a_mn;
     g.b_mn = b_mn;
-    const int nt = std::min(256, (g.N + 15) / 16 * 16);
+    const int nkb = (g.K + G_BOX - 1) / G_BOX;
+    g.kb_per_split = ksplit > 1 ? (nkb + ksplit - 1) / ksplit : nkb;
+    const int nz = (nkb + g.kb_per_split - 1) / g.kb_per_split;     // every slice has >= 1 block
+    if (nz > 1 && g.epi != EPI_F32) return cudaErrorInvalidValue;
+    if (nz_out) *nz_out = nz;
+    // N tile: up to 256 columns; 128 when that still fits two CTAs per SM in one wave
+    // (more SMs share a small product's epilogue)
+    int nt = std::min(256, (g.N + 15) / 16 * 16);
+    const int64_t mtiles = (g.M + 127) / 128;
+    if (nt > 128 && mtiles * ((g.N + 127) / 128) * nz <= 2 * 148) nt = 128;
     uint32_t cols = 32;
     while ((int)cols < nt) cols <<= 1;
-    const int stage_bytes = 2 * G_BOX_BYTES + ((nt + G_BOX - 1) / G_BOX) * G_BOX_BYTES;
-    const int smem = 1024 + G_STAGES * stage_bytes + 256;
-    const cudaError_t ea = cudaFuncSetAttribute(bf16_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (ea != cudaSuccess) return ea;
-    dim3 grid((g.M + 127) / 128, (g.N + 255) / 256);
-    bf16_gemm_kernel<<<grid, G_THREADS, smem, s>>>(ma, mb, g, nt, cols);
+    dim3 grid((unsigned)mtiles, (g.N + nt - 1) / nt, nz);
+    bf16_gemm_kernel<<<grid, G_THREADS, gemm_smem(nt), s>>>(ma, mb, g, nt, cols);
     return cudaGetLastError();
+}
+
+// out[m][n] (row pitch ldo) = sum over z of partial[z][m][n] (pitch N), in order of z
+__global__ void split_reduce_kernel(const float* __restrict__ partial, int nz, int64_t M, int N, float* __restrict__ out,
+                                    int64_t ldo) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= M * N) return;
+    float acc = 0.f;
+    for (int z = 0; z < nz; ++z) acc += partial[z * M * N + i];
+    out[(i / N) * ldo + i % N] = acc;
 }
 
 // ---- elementwise kernels ----
@@ -389,6 +460,8 @@ struct sht_mlp {
     float *plainT = nullptr, *plainq = nullptr;     // [NLC][cap] plain-physics fallback
     int* nfallback = nullptr;
     float* partial = nullptr;                       // [cap / 256][hidden] bias-gradient partial sums
+    static constexpr int MAX_SPLIT = 32;
+    float* splitbuf = nullptr;                      // [MAX_SPLIT][256][256] split-K partial weight gradients
     int32_t* err = nullptr;
     int step = 0;
 };
@@ -425,7 +498,7 @@ void release(sht_mlp* m) {
             if (q) cudaFree(q);
     }
     void* ps[] = {m->X0, m->Y, m->dY, m->xm, m->xs, m->ym, m->ys, m->loss, m->colbuf, m->ybuf, m->plainT, m->plainq,
-                  m->nfallback, m->partial, m->err};
+                  m->nfallback, m->partial, m->splitbuf, m->err};
     for (void* q : ps)
         if (q) cudaFree(q);
 }
@@ -440,14 +513,14 @@ GemmArgs args(sht_mlp* m, int M, int N, int K, int epi) {
     return g;
 }
 
-// forward pass over B rows of X0; keep = store pre-activations
-cudaError_t forward(sht_mlp* m, int B, cudaStream_t s) {
+// forward pass over B rows of X0; keep = store the pre-activations (for the backward pass)
+cudaError_t forward(sht_mlp* m, int B, bool keep, cudaStream_t s) {
     cudaError_t e = cudaSuccess;
     const __nv_bfloat16* in = m->X0;
     int64_t ld_in = m->in_pad;
     for (int l = 0; l < 3 && e == cudaSuccess; ++l) {
         GemmArgs g = args(m, B, m->hidden, m->fan_in[l], EPI_BIAS_GELU);
-        g.out_f32 = m->Z[l];
+        g.out_f32 = keep ? m->Z[l] : nullptr;
         g.ld_f32 = m->hidden;
         g.out_bf16 = m->A[l];
         g.ld_bf16 = m->hidden;
@@ -519,6 +592,7 @@ int sht_mlp_create(int batch_capacity, uint64_t seed, int device, sht_mlp** out)
     if (e == cudaSuccess) e = alloc(&m->plainq, cap * NLC);
     if (e == cudaSuccess) e = alloc(&m->nfallback, 1);
     if (e == cudaSuccess) e = alloc(&m->partial, (cap / BIAS_ROWS + 1) * m->hidden);
+    if (e == cudaSuccess) e = alloc(&m->splitbuf, (size_t)sht_mlp::MAX_SPLIT * m->hidden * m->hidden);
     if (e == cudaSuccess && (e = alloc(&m->err, 1)) == cudaSuccess) e = cudaMemset(m->err, 0, 4);
     if (e == cudaSuccess) {          // identity normalisation until set
         std::vector<float> zero(m->nin, 0.f), one(m->nin, 1.f);
@@ -552,16 +626,14 @@ int sht_mlp_set_normalization(sht_mlp* m, const float* x_mean, const float* x_st
     return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_set_normalization");
 }
 
-int sht_mlp_train_step(sht_mlp* m, const float* x, const float* y, int B, float lr, void* stream) {
-    if (!m || !x || !y) return set_error(SHT_EINVAL, "sht_mlp_train_step: NULL argument");
-    if (B < 1 || B > m->cap) return set_error(SHT_EINVAL, "sht_mlp_train_step: batch outside 1 .. capacity");
-    DevGuard dg(m->device);
-    cudaStream_t s = (cudaStream_t)stream;
+namespace {
+// loss and gradients dW, db of every layer for the batch (x [B][33], y [B][16])
+cudaError_t backward(sht_mlp* m, const float* x, const float* y, int B, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(m->loss, 0, 4, s);
     const int64_t nx = (int64_t)B * m->in_pad;
     normalize_in_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, s>>>(x, m->nin, B, m->nin, m->xm, m->xs, m->X0,
                                                                      m->in_pad);
-    if (e == cudaSuccess) e = forward(m, B, s);
+    if (e == cudaSuccess) e = forward(m, B, true, s);
     const int64_t ny = (int64_t)B * m->nout;
     if (e == cudaSuccess)
         output_grad_kernel<<<(unsigned)((ny + 255) / 256), 256, 0, s>>>(m->Y, y, B, m->nout, m->ym, m->ys, m->dY,
@@ -573,12 +645,20 @@ int sht_mlp_train_step(sht_mlp* m, const float* x, const float* y, int B, float 
     int64_t ld_dz = m->nout;
     for (int l = 3; l >= 0 && e == cudaSuccess; --l) {
         const int fo = m->fan_out[l], fi = m->fan_in[l];
-        // dW[l] [fo][fi] = dz^T act[l]   (A = dz MN-major, B = act MN-major)
+        // dW[l] [fo][fi] = dz^T act[l]   (A = dz MN-major, B = act MN-major), K = B split
+        // over grid z into slices of >= 2 blocks of 64 rows, about one CTA per SM in all,
+        // partial products reduced in a fixed order (deterministic)
         GemmArgs gw = args(m, fo, fi, B, EPI_F32);
-        gw.out_f32 = m->dW[l];
+        const int tiles = ((fo + 127) / 128) * ((fi + 255) / 256);
+        const int ksplit = std::max(1, std::min(std::min((int)sht_mlp::MAX_SPLIT, 148 / tiles), (B + 127) / 128));
+        gw.out_f32 = m->splitbuf;
         gw.ld_f32 = fi;
-        e = gemm(dz, ld_dz, 1, act[l], ld_act[l], 1, gw, s);
+        gw.split_stride = (int64_t)fo * fi;
+        int nz = 1;
+        e = gemm(dz, ld_dz, 1, act[l], ld_act[l], 1, gw, s, ksplit, &nz);
         if (e != cudaSuccess) break;
+        split_reduce_kernel<<<(unsigned)(((int64_t)fo * fi + 255) / 256), 256, 0, s>>>(m->splitbuf, nz, fo, fi,
+                                                                                        m->dW[l], fi);
         const int P = (B + BIAS_ROWS - 1) / BIAS_ROWS;
         bias_partial_kernel<<<dim3((fo + 127) / 128, P), 128, 0, s>>>(dz, B, fo, ld_dz, m->partial);
         bias_final_kernel<<<(fo + 127) / 128, 128, 0, s>>>(m->partial, P, fo, m->db[l]);
@@ -593,6 +673,25 @@ int sht_mlp_train_step(sht_mlp* m, const float* x, const float* y, int B, float 
         dz = m->dZ[l - 1];
         ld_dz = m->hidden;
     }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e;
+}
+}  // namespace
+
+int sht_mlp_backward(sht_mlp* m, const float* x, const float* y, int B, void* stream) {
+    if (!m || !x || !y) return set_error(SHT_EINVAL, "sht_mlp_backward: NULL argument");
+    if (B < 1 || B > m->cap) return set_error(SHT_EINVAL, "sht_mlp_backward: batch outside 1 .. capacity");
+    DevGuard dg(m->device);
+    const cudaError_t e = backward(m, x, y, B, (cudaStream_t)stream);
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_backward");
+}
+
+int sht_mlp_train_step(sht_mlp* m, const float* x, const float* y, int B, float lr, void* stream) {
+    if (!m || !x || !y) return set_error(SHT_EINVAL, "sht_mlp_train_step: NULL argument");
+    if (B < 1 || B > m->cap) return set_error(SHT_EINVAL, "sht_mlp_train_step: batch outside 1 .. capacity");
+    DevGuard dg(m->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = backward(m, x, y, B, s);
     // Adam
     ++m->step;
     const float b1 = 0.9f, b2 = 0.999f;
@@ -617,7 +716,7 @@ int sht_mlp_infer(sht_mlp* m, const float* x, float* y, int B, void* stream) {
     const int64_t nx = (int64_t)B * m->in_pad;
     normalize_in_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, s>>>(x, m->nin, B, m->nin, m->xm, m->xs, m->X0,
                                                                      m->in_pad);
-    cudaError_t e = forward(m, B, s);
+    cudaError_t e = forward(m, B, false, s);
     const int64_t ny = (int64_t)B * m->nout;
     if (e == cudaSuccess)
         denormalize_kernel<<<(unsigned)((ny + 255) / 256), 256, 0, s>>>(m->Y, B, m->nout, m->ym, m->ys, y, m->nout);
@@ -635,10 +734,15 @@ int sht_mlp_loss(sht_mlp* m, float* loss) {
 
 int sht_mlp_params(sht_mlp* m, int layer, float* w, float* b, int set) {
     if (!m || layer < 0 || layer >= 4) return set_error(SHT_EINVAL, "sht_mlp_params: bad layer");
+    if (set < 0 || set > 2) return set_error(SHT_EINVAL, "sht_mlp_params: mode must be 0 (get), 1 (set) or 2 (gradients)");
     DevGuard dg(m->device);
     const size_t nw = (size_t)m->fan_out[layer] * m->fan_in[layer];
     cudaError_t e = cudaSuccess;
-    if (set) {
+    if (set == 2) {            // gradients of the last backward pass
+        e = cudaDeviceSynchronize();
+        if (e == cudaSuccess && w) e = cudaMemcpy(w, m->dW[layer], nw * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && b) e = cudaMemcpy(b, m->db[layer], m->fan_out[layer] * 4, cudaMemcpyDeviceToHost);
+    } else if (set) {
         if (w) e = cudaMemcpy(m->W[layer], w, nw * 4, cudaMemcpyHostToDevice);
         if (e == cudaSuccess && b) e = cudaMemcpy(m->b[layer], b, m->fan_out[layer] * 4, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) to_bf16_kernel<<<(unsigned)((nw + 255) / 256), 256>>>(m->W[layer], m->Wb[layer], nw);
@@ -655,23 +759,27 @@ int sht_column_emulate(sht_mlp* m, const float* temp, const float* humid, const 
                        float* dhumid, unsigned flags, int32_t* nfallback, void* stream) {
     if (!m || !temp || !humid || !u || !v || !surface_pressure || !dtemp || !dhumid)
         return set_error(SHT_EINVAL, "sht_column_emulate: NULL argument");
-    if (ncol < 0 || ncol > m->cap || ld < ncol)
-        return set_error(SHT_EINVAL, "sht_column_emulate: DimensionMismatch: ncol outside capacity or ld < ncol");
+    if (ncol < 0 || ld < ncol) return set_error(SHT_EINVAL, "sht_column_emulate: DimensionMismatch: ld < ncol");
     if (ncol == 0) return SHT_OK;
     DevGuard dg(m->device);
     cudaStream_t s = (cudaStream_t)stream;
-    gather_columns_kernel<<<(ncol + 127) / 128, 128, 0, s>>>(temp, humid, u, v, surface_pressure, ld, ncol,
-                                                             m->colbuf);
-    int rc = sht_mlp_infer(m, m->colbuf, m->ybuf, ncol, stream);
-    if (rc != SHT_OK) return rc;
-    cudaError_t e = launch_column_physics(temp, humid, surface_pressure, ld, ncol, (float)dt, m->plainT, m->plainq,
-                                          ncol, false, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(m->nfallback, 0, 4, s);
-    if (e == cudaSuccess)
-        scatter_columns_kernel<<<(ncol + 127) / 128, 128, 0, s>>>(m->colbuf, m->xm, m->xs, (float)z_max, m->ybuf,
-                                                                  m->plainT, m->plainq, ld, ncol, dtemp, dhumid,
-                                                                  (flags & SHT_ADD) ? 1 : 0, m->nfallback);
-    if (e == cudaSuccess) e = cudaGetLastError();
+    cudaError_t e = cudaMemsetAsync(m->nfallback, 0, 4, s);
+    // chunks of the network's batch capacity
+    for (int c0 = 0; c0 < ncol && e == cudaSuccess; c0 += m->cap) {
+        const int nc = std::min(m->cap, ncol - c0);
+        gather_columns_kernel<<<(nc + 127) / 128, 128, 0, s>>>(temp + c0, humid + c0, u + c0, v + c0,
+                                                               surface_pressure + c0, ld, nc, m->colbuf);
+        const int rc = sht_mlp_infer(m, m->colbuf, m->ybuf, nc, stream);
+        if (rc != SHT_OK) return rc;
+        e = launch_column_physics(temp + c0, humid + c0, surface_pressure + c0, ld, nc, (float)dt, m->plainT,
+                                  m->plainq, nc, false, s);
+        if (e == cudaSuccess)
+            scatter_columns_kernel<<<(nc + 127) / 128, 128, 0, s>>>(m->colbuf, m->xm, m->xs, (float)z_max, m->ybuf,
+                                                                    m->plainT, m->plainq, ld, nc, dtemp + c0,
+                                                                    dhumid + c0, (flags & SHT_ADD) ? 1 : 0,
+                                                                    m->nfallback);
+        if (e == cudaSuccess) e = cudaGetLastError();
+    }
     if (e == cudaSuccess && nfallback) {
         e = cudaMemcpyAsync(nfallback, m->nfallback, 4, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -51,6 +51,34 @@ def column_physics_(dtemp, dhumid, temp, humid, surface_pressure, *, dt=1200.0, 
     return dtemp, dhumid
 
 
+def synthetic_columns(ncol: int, seed: int = 0, device=None):
+    """Seeded columns standing in for model-generated states (there is no dynamical core
+    here), generated on the GPU: latitude-dependent surface temperature with a
+    tropospheric lapse rate, relative humidity 0.2 .. 1.05 decreasing upward, a zonal jet
+    with noise, log surface pressure near 1e5 Pa. Returns temp, humid, u, v [8, ncol] and
+    surface_pressure [ncol], float32 (the same distribution as the tests' numpy columns).
+    Saturation humidity by Clausius-Clapeyron (SpeedyWeather/src/dynamics/atmosphere.jl:138-157)."""
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev).manual_seed(seed)
+    f64 = torch.float64
+    half = torch.linspace(0, 1, NLAYERS + 1, dtype=f64, device=dev)
+    full = (0.5 * (half[1:] + half[:-1]))[:, None]
+    U = lambda *shape: torch.rand(*shape, generator=g, device=dev, dtype=f64)      # noqa: E731
+    N = lambda *shape: torch.randn(*shape, generator=g, device=dev, dtype=f64)     # noqa: E731
+    r_dry, r_vap = 1000 * 8.3145 / 28.9649, 1000 * 8.3145 / 18.0153
+    lat = torch.asin(2 * U(ncol) - 1)
+    ps = 1e5 * torch.exp(0.02 * N(ncol))
+    Ts = 302 - 45 * torch.sin(lat) ** 2 + 3 * N(ncol)
+    T = Ts[None, :] * full ** (r_dry * 0.0065 / 9.81) + 1.5 * N(NLAYERS, ncol)
+    T = torch.maximum(T, 195.0 + 2 * N(NLAYERS, ncol))
+    rh = (0.5 + 0.55 * U(ncol))[None, :] * (0.25 + 0.75 * full ** 1.5) * (0.85 + 0.3 * U(NLAYERS, ncol))
+    qsat = (r_dry / r_vap) * 610.78 * torch.exp(2501.0e3 / r_vap * (1 / 273.15 - 1 / T)) / (ps[None, :] * full)
+    q = torch.clamp(rh, 0.02, 1.08) * qsat
+    u = 30 * torch.sin(2 * lat)[None, :] * (1.2 - full) + 5 * N(NLAYERS, ncol)
+    v = 4 * N(NLAYERS, ncol)
+    return tuple(a.float().contiguous() for a in (T, q, u, v, ps))
+
+
 def columns_as_rows(temp, humid, u, v, surface_pressure):
     """[ncol, 33] network inputs: temp, humid, u, v on the 8 layers, then log ps (torch)."""
     return torch.cat([temp.T, humid.T, u.T, v.T, torch.log(surface_pressure)[:, None]], dim=1).contiguous()
@@ -85,6 +113,31 @@ class ColumnEmulator:
         _f32(y, "y", (x.shape[0], NOUT))
         check(lib.sht_mlp_train_step(self._m, x.data_ptr(), y.data_ptr(), x.shape[0], float(lr), _stream(x)))
 
+    def backward(self, x, y):
+        """Loss and gradients over (x, y) without an update; returns the loss."""
+        _f32(x, "x", (x.shape[0], NIN))
+        _f32(y, "y", (x.shape[0], NOUT))
+        check(lib.sht_mlp_backward(self._m, x.data_ptr(), y.data_ptr(), x.shape[0], _stream(x)))
+        return self.loss()
+
+    def gradients(self, layer):
+        """(dW [out][in], db [out]) of the last backward pass, FP32 numpy."""
+        w, b = self._layer_arrays(layer)
+        check(lib.sht_mlp_params(self._m, layer, w.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), 2))
+        return w, b
+
+    def _layer_arrays(self, layer):
+        fo = [256, 256, 256, NOUT][layer]
+        fi = [64, 256, 256, 256][layer]
+        return np.zeros((fo, fi), np.float32), np.zeros(fo, np.float32)
+
+    def set_params(self, layer, w, b):
+        """Upload FP32 parameters of one layer (w [out][in], b [out])."""
+        w0, b0 = self._layer_arrays(layer)
+        w = np.ascontiguousarray(w, dtype=np.float32).reshape(w0.shape)
+        b = np.ascontiguousarray(b, dtype=np.float32).reshape(b0.shape)
+        check(lib.sht_mlp_params(self._m, layer, w.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), 1))
+
     def loss(self) -> float:
         v = C.c_float(0)
         check(lib.sht_mlp_loss(self._m, C.byref(v)))
@@ -114,17 +167,16 @@ class ColumnEmulator:
         return y
 
     def params(self, layer):
-        fo = [256, 256, 256, NOUT][layer]
-        fi = [64, 256, 256, 256][layer]
-        w = np.zeros((fo, fi), np.float32)
-        b = np.zeros(fo, np.float32)
+        """(w [out][in], b [out]) FP32 master parameters of one layer, numpy."""
+        w, b = self._layer_arrays(layer)
         check(lib.sht_mlp_params(self._m, layer, w.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), 0))
         return w, b
 
     def parameterization_(self, dtemp, dhumid, temp, humid, u, v, surface_pressure, *, dt=1200.0, z_max=4.0,
-                          add=False) -> int:
+                          add=False, count=True):
         """The emulator as the column parameterization (fallback to the plain schemes outside
-        z_max standard deviations of the training inputs); returns the fallback count."""
+        z_max standard deviations of the training inputs); returns the fallback count
+        (count=True synchronises the stream), or None."""
         ncol = temp.shape[1]
         for n, t in (("temp", temp), ("humid", humid), ("u", u), ("v", v), ("dtemp", dtemp), ("dhumid", dhumid)):
             _f32(t, n, (NLAYERS, ncol))
@@ -132,9 +184,9 @@ class ColumnEmulator:
         nf = C.c_int32(0)
         check(lib.sht_column_emulate(self._m, temp.data_ptr(), humid.data_ptr(), u.data_ptr(), v.data_ptr(),
                                      surface_pressure.data_ptr(), ncol, ncol, float(dt), float(z_max),
-                                     dtemp.data_ptr(), dhumid.data_ptr(), _lib.ADD if add else 0, C.byref(nf),
-                                     _stream(temp)))
-        return int(nf.value)
+                                     dtemp.data_ptr(), dhumid.data_ptr(), _lib.ADD if add else 0,
+                                     C.byref(nf) if count else None, _stream(temp)))
+        return int(nf.value) if count else None
 
     def device_status(self) -> int:
         v = C.c_int32(0)
@@ -142,7 +194,7 @@ class ColumnEmulator:
         return int(v.value)
 
     def __del__(self):
-        if getattr(self, "_m", None) is not None:
+        if getattr(self, "_m", None) is not None and lib is not None:   # lib is None at interpreter exit
             lib.sht_mlp_destroy(self._m)
             self._m = None
 

@@ -76,6 +76,7 @@ SIGNATURES = {
     "sht_column_physics": (C.c_int, [_P, _P, _P, _I64, C.c_int, C.c_int, C.c_double, _P, _P, C.c_uint, _P]),
     "sht_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.c_int, C.POINTER(C.c_void_p)]),
     "sht_mlp_set_normalization": (C.c_int, [_P, _P, _P, _P, _P]),
+    "sht_mlp_backward": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "sht_mlp_train_step": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, _P]),
     "sht_mlp_loss": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "sht_mlp_infer": (C.c_int, [_P, _P, _P, C.c_int, _P]),

@@ -46,3 +46,54 @@ def test_float32_mode_tracks_float64():
     for x, y in zip(a, b):
         same = np.all(np.isclose(x, y, rtol=1e-3, atol=1e-3 * np.abs(x).max()), axis=1)
         assert same.mean() > 0.99
+
+
+def _random_params(seed):
+    rng = np.random.default_rng(seed)
+    shapes = [(256, 64), (256, 256), (256, 256), (16, 256)]
+    params = []
+    for i, (o, n) in enumerate(shapes):
+        w = rng.normal(0, np.sqrt(2.0 / n), (o, n))
+        if i == 0:
+            w[:, 33:] = 0.0
+        params.append((w, rng.normal(0, 0.1, o)))
+    return params
+
+
+def test_mlp_backward_finite_differences():
+    """The FP64 restatement of the emulator's backward pass against central differences
+    of its own loss on a few entries of every layer's weights and biases."""
+    rng = np.random.default_rng(7)
+    params = _random_params(1)
+    xn = rng.normal(size=(48, 33))
+    yn = rng.normal(size=(48, 16))
+    _, grads = C.mlp_backward(params, xn, yn, bf16=False)
+    h = 1e-6
+    for layer in range(4):
+        w, b = params[layer]
+        for _ in range(4):
+            i, j = rng.integers(w.shape[0]), rng.integers(33 if layer == 0 else w.shape[1])
+            for arr, g in ((w, grads[layer][0][i, j]), (b, grads[layer][1][i])):
+                idx = (i, j) if arr.ndim == 2 else (i,)
+                old = arr[idx]
+                arr[idx] = old + h
+                lp = C.mlp_backward(params, xn, yn, bf16=False)[0]
+                arr[idx] = old - h
+                lm = C.mlp_backward(params, xn, yn, bf16=False)[0]
+                arr[idx] = old
+                fd = (lp - lm) / (2 * h)
+                assert abs(fd - g) <= 1e-6 * max(1e-3, abs(g)) + 1e-9, (layer, idx, fd, g)
+
+
+def test_bf16_round():
+    a = np.array([1.0, 1.00390625, 1.005859375, -3.1415926, 65504.0, 1e-30], np.float32)
+    r = C.bf16_round(a)
+    import torch
+    ref = torch.tensor(a).to(torch.bfloat16).float().numpy()
+    np.testing.assert_array_equal(r, ref.astype(np.float64))
+    # BF16 rounding of the forward pass stays close to the exact one
+    params = _random_params(2)
+    xn = np.random.default_rng(3).normal(size=(32, 33))
+    y1, _ = C.mlp_forward(params, xn, bf16=True)
+    y0, _ = C.mlp_forward(params, xn, bf16=False)
+    assert np.linalg.norm(y1 - y0) / np.linalg.norm(y0) < 3e-2

@@ -157,3 +157,60 @@ def test_emulator_parameterization_and_fallback(sp, trained):
     err = np.linalg.norm(gT[:, n // 4:] - ref) / np.linalg.norm(ref)
     print("emulator vs plain physics (relative L2 of dT/dt):", err, "fallbacks:", nf)
     assert err < 0.5
+
+
+def test_mlp_gradients_vs_oracle(sp):
+    """sht_mlp_backward against the oracle's backward pass with BF16 rounding at the
+    kernels' storage points (relative Frobenius error per gradient < 5e-3), on a ragged
+    batch of 1000 rows; identity normalisation so both see the same inputs."""
+    rng = np.random.default_rng(5)
+    shapes = [(256, 64), (256, 256), (256, 256), (16, 256)]
+    params = []
+    em = sp.ColumnEmulator(1024, seed=0)
+    for i, (o, n) in enumerate(shapes):
+        w = rng.normal(0, np.sqrt(2.0 / n), (o, n)).astype(np.float32)
+        if i == 0:
+            w[:, 33:] = 0.0
+        b = rng.normal(0, 0.1, o).astype(np.float32)
+        em.set_params(i, w, b)
+        params.append((w.astype(np.float64), b.astype(np.float64)))
+    em.set_normalization(np.zeros(33), np.ones(33), np.zeros(16), np.ones(16))
+    B = 1000
+    x = rng.normal(size=(B, 33)).astype(np.float32)
+    y = rng.normal(size=(B, 16)).astype(np.float32)
+    loss = em.backward(to_dev(x), to_dev(y))
+    ref_loss, ref = CO.mlp_backward(params, x.astype(np.float64), y.astype(np.float64), bf16=True)
+    _, exact = CO.mlp_backward(params, x.astype(np.float64), y.astype(np.float64), bf16=False)
+    assert abs(loss - ref_loss) <= 1e-4 * ref_loss
+    for layer in range(4):
+        dw, db = em.gradients(layer)
+        for g, r, e in ((dw, ref[layer][0], exact[layer][0]), (db, ref[layer][1], exact[layer][1])):
+            rel = np.linalg.norm(g - r) / np.linalg.norm(r)
+            print(f"layer {layer} grad {g.shape}: vs BF16-rounded oracle {rel:.2e}, vs exact FP64 "
+                  f"{np.linalg.norm(g - e) / np.linalg.norm(e):.2e}")
+            assert rel < 5e-3
+    assert em.device_status() == 0
+
+
+def test_emulator_chunks_beyond_capacity(sp, trained):
+    """20 000 columns through an emulator of capacity 8192 (three chunks) equal the two
+    halves run separately, bit for bit (rows of the network are independent)."""
+    import torch
+    em = trained[0]
+    n = 20000
+    T, q, u, v, ps = (a.cuda() for a in (torch.tensor(np.ascontiguousarray(c.T if c.ndim == 2 else c))
+                                         for c in CO.synthetic_columns(n, seed=123)))
+    dT = torch.zeros((8, n), device="cuda")
+    dq = torch.zeros((8, n), device="cuda")
+    nf = em.parameterization_(dT, dq, T, q, u, v, ps)
+    h = n // 2
+    parts = []
+    for sl in (slice(0, h), slice(h, n)):
+        a = torch.zeros((8, h), device="cuda")
+        b = torch.zeros((8, h), device="cuda")
+        nfp = em.parameterization_(a, b, *(t[:, sl].contiguous() for t in (T, q, u, v)), ps[sl].contiguous())
+        parts.append((a, b, nfp))
+    torch.cuda.synchronize()
+    assert nf == parts[0][2] + parts[1][2]
+    assert torch.equal(dT, torch.cat([parts[0][0], parts[1][0]], dim=1))
+    assert torch.equal(dq, torch.cat([parts[0][1], parts[1][1]], dim=1))
