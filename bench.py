@@ -9,7 +9,9 @@ total round trips of all ranks divided by the slowest rank's time.
 Reports the headline precision (the fastest Legendre arithmetic whose round trip
 stays within 1e-5 relative error of the FP64 oracle) and every variant, the
 roofline of the dominant kernel, an end-to-end number through the public API with
-host buffers, clocks sampled during the timed region, and the CPU baseline.
+host buffers (coefficients in page-locked host memory, copied in and out inside the
+transforms, overlapped with the work over chunks of 16 layers), clocks sampled during
+the timed region, and the CPU baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -60,11 +62,19 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        time.sleep(0.3)
+        # the timed region starts once the sampler has written its first line (or after 5 s)
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < 5.0:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *a):
@@ -150,11 +160,21 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import sht_oracle as O
     from sht_cpu import CpuTransform, max_threads
-    sample = args.ref_sample_layers
-    cp = CpuTransform(1, NLAT_HALF, T, T, sample)
-    c = O.random_coeffs(O.Spectrum(T, T), sample, seed=0).T.astype(np.complex64)
-    g = np.empty((sample, cp.npoints), np.float32)
-    a = np.empty((sample, cp.nlm), np.complex64)
+    # each step: one round trip of `sample` layers (1 .. --ref-sample-layers), sized from a
+    # calibration round trip so that the K + W steps take about --ref-seconds in all
+    top = args.ref_sample_layers
+    cp = CpuTransform(1, NLAT_HALF, T, T, top)
+    c = O.random_coeffs(O.Spectrum(T, T), top, seed=0).T.astype(np.complex64)
+    g = np.empty((top, cp.npoints), np.float32)
+    a = np.empty((top, cp.nlm), np.complex64)
+    t0 = time.perf_counter()
+    cp.synthesize(c, g)
+    cp.analyze(g, a)
+    per_layer = (time.perf_counter() - t0) / top
+    sample = int(max(1, min(top, args.ref_seconds / max(1, args.steps + args.warmup) / per_layer)))
+    if sample < top:
+        cp = CpuTransform(1, NLAT_HALF, T, T, sample)
+        c, g, a = np.ascontiguousarray(c[:sample]), g[:sample], a[:sample]
     for _ in range(args.warmup):
         cp.synthesize(c, g)
         cp.analyze(g, a)
@@ -508,14 +528,21 @@ def run_ours(args):
     clocks = clk.summary()
     value = world * args.steps / secs
 
-    # end to end through the public API with host buffers (pinned H2D in, D2H of the result)
+    # end to end through the public API with host buffers: the coefficients go in from
+    # page-locked host memory and come back to it inside the transforms (sht_synthesize_host /
+    # sht_analyze_host), one round trip per chunk of 16 layers so that the copy in of the
+    # next chunk and the copy out of the previous one overlap the work of the current one;
+    # S.host_wait() makes the step end after its last copy to the host
     host_out = torch.empty((LAYERS, spec.nlm), dtype=torch.complex64).pin_memory()
+    E2E_CHUNK = 16
+    S.set_host_chunk(E2E_CHUNK)
 
     def e2e_step():
-        lt.data.copy_(host_c, non_blocking=True)
-        st.transform_(field, lt, S)
-        st.transform_(out, field, S)
-        host_out.copy_(out.data, non_blocking=True)
+        for k0 in range(0, LAYERS, E2E_CHUNK):
+            f = st.Field(field.data[k0:k0 + E2E_CHUNK], S.grid)
+            st.transform_(f, st.LowerTriangularArray(host_c[k0:k0 + E2E_CHUNK], spec), S)
+            st.transform_(st.LowerTriangularArray(host_out[k0:k0 + E2E_CHUNK], spec), f, S)
+        S.host_wait()
 
     for _ in range(args.warmup):
         e2e_step()
@@ -573,8 +600,8 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000, help="timed steps (default: ~1 s at T511 x 64)")
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3", "fp16x3", "bf16x5"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -585,6 +612,8 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="only W + K round trips of one precision (default bf16x3), for profilers")
     ap.add_argument("--ref-sample-layers", type=int, default=16)
+    ap.add_argument("--ref-seconds", type=float, default=90.0,
+                    help="reference arm: CPU seconds for all steps (sets the layers per step)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -128,6 +128,26 @@ SHT_API int sht_synthesize(sht_plan* plan, const void* coeffs, int64_t ldc, floa
 SHT_API int sht_analyze(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, int64_t ldc,
                 int K, unsigned flags, void* stream);
 
+/* Coefficients in HOST memory (page-locked for overlap), field on the device: the
+ * transforms above with the host <-> device copies that on_architecture performs in the
+ * reference (LowerTriangularArrays/src/lower_triangular_array.jl:905-910, used as in
+ * SpeedyWeather/test/GPU/spectral_transform.jl:104-105) folded into the call and
+ * pipelined over chunks of layers (sht_plan_set_host_chunk; default 16): each chunk's
+ * copy runs on a copy stream of the plan into one of two device staging slots, so the
+ * copy of chunk i + 1 overlaps the transform of chunk i, and the copies of one call
+ * overlap the work of the next. Stream-ordered on `stream`, except that the copies to
+ * the host complete on the plan's copy stream: sht_host_wait(plan, stream) makes
+ * `stream` wait for all of them (synchronising `stream` afterwards means the host
+ * arrays are written). coeffs_host of sht_synthesize_host may be reused once `stream`
+ * has passed the call. The first call allocates the staging slots (2 x 2 chunks of
+ * nlm complex values). sht_analyze_host accepts no SHT_ADD. */
+SHT_API int sht_plan_set_host_chunk(sht_plan* plan, int layers);
+SHT_API int sht_synthesize_host(sht_plan* plan, const void* coeffs_host, int64_t ldc, float* grid, int64_t ldg,
+                                int K, unsigned flags, void* stream);
+SHT_API int sht_analyze_host(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs_host, int64_t ldc,
+                             int K, unsigned flags, void* stream);
+SHT_API int sht_host_wait(sht_plan* plan, void* stream);
+
 /* Split stages, for callers that batch their own Fourier or Legendre work.
  * The Fourier scratch is the plan's own. sht_legendre_synthesis writes it,
  * sht_fourier_synthesis reads it; sht_fourier_analysis writes it,

@@ -25,8 +25,20 @@ cudaError_t launch_legendre_analysis_tc(const Plan& p, float2* coeffs, int64_t l
 
 using namespace sht;
 
+// Host-buffer transforms (sht_synthesize_host / sht_analyze_host): device staging slots
+// for chunks of layers, the plan's copy streams and the events ordering them.
+struct HostPipe {
+    int chunk = 0;                            // layers per chunk
+    float2* in_slot[2] = {};                  // [chunk][nlm] coefficients on their way in
+    float2* out_slot[2] = {};                 // [chunk][nlm] coefficients on their way out
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
+    int in_next = 0, out_next = 0;            // slot used by the next chunk
+};
+
 struct sht_plan {
     Plan p;
+    HostPipe host;
 };
 
 namespace {
@@ -565,9 +577,25 @@ int sht_plan_create(const sht_desc* desc, sht_plan** out) {
     return SHT_OK;
 }
 
+static void release_host(HostPipe& h) {
+    if (h.copy_in) cudaStreamSynchronize(h.copy_in);
+    if (h.copy_out) cudaStreamSynchronize(h.copy_out);
+    for (int i = 0; i < 2; ++i) {
+        if (h.in_slot[i]) cudaFree(h.in_slot[i]);
+        if (h.out_slot[i]) cudaFree(h.out_slot[i]);
+        cudaEvent_t* ev[] = {&h.in_ready[i], &h.in_free[i], &h.out_ready[i], &h.out_free[i]};
+        for (cudaEvent_t* e : ev)
+            if (*e) cudaEventDestroy(*e);
+    }
+    if (h.copy_in) cudaStreamDestroy(h.copy_in);
+    if (h.copy_out) cudaStreamDestroy(h.copy_out);
+    h = HostPipe{};
+}
+
 int sht_plan_destroy(sht_plan* plan) {
     if (!plan) return SHT_OK;
     DeviceGuard g(plan->p.device);
+    release_host(plan->host);
     release(plan->p);
     delete plan;
     return SHT_OK;
@@ -732,6 +760,116 @@ int sht_analyze(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, in
     if (e != cudaSuccess) return cuda_fail(e, "sht_analyze (Fourier)");
     return finish(legendre_analysis(plan->p, (float2*)coeffs, ldc, K, (flags & SHT_ADD) != 0, s),
                   "sht_analyze (Legendre)");
+}
+
+// ---- host-buffer transforms -------------------------------------------------------
+namespace {
+constexpr int kDefaultHostChunk = 16;
+
+cudaError_t host_prepare(sht_plan* plan, int chunk) {
+    HostPipe& h = plan->host;
+    chunk = std::max(1, std::min(chunk, std::max(1, plan->p.d.nlayers)));
+    if (h.chunk == chunk) return cudaSuccess;
+    release_host(h);
+    h.chunk = chunk;
+    const size_t bytes = (size_t)chunk * plan->p.nlm * sizeof(float2);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        e = cudaMalloc((void**)&h.in_slot[i], bytes);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&h.out_slot[i], bytes);
+        cudaEvent_t* ev[] = {&h.in_ready[i], &h.in_free[i], &h.out_ready[i], &h.out_free[i]};
+        for (cudaEvent_t* q : ev)
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(q, cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h.copy_in, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h.copy_out, cudaStreamNonBlocking);
+    if (e != cudaSuccess) release_host(h);
+    return e;
+}
+}  // namespace
+
+int sht_plan_set_host_chunk(sht_plan* plan, int layers) {
+    if (!plan) return fail(SHT_EINVAL, "sht_plan_set_host_chunk: NULL plan");
+    if (layers < 1) return fail(SHT_EINVAL, "sht_plan_set_host_chunk: layers must be >= 1");
+    DeviceGuard g(plan->p.device);
+    const cudaError_t e = host_prepare(plan, layers);
+    return e == cudaSuccess ? SHT_OK : cuda_fail(e, "sht_plan_set_host_chunk");
+}
+
+int sht_synthesize_host(sht_plan* plan, const void* coeffs_host, int64_t ldc, float* grid, int64_t ldg, int K,
+                        unsigned flags, void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_synthesize_host")) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, "sht_synthesize_host")) != SHT_OK) return rc;
+    if ((rc = check_ldg(plan->p, ldg, "sht_synthesize_host")) != SHT_OK) return rc;
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(coeffs_host) || !ok_ptr(grid)) return fail(SHT_EINVAL, "sht_synthesize_host: NULL array");
+    DeviceGuard g(plan->p.device);
+    cudaError_t e = plan->host.chunk ? cudaSuccess : host_prepare(plan, kDefaultHostChunk);
+    if (e != cudaSuccess) return cuda_fail(e, "sht_synthesize_host (staging)");
+    HostPipe& h = plan->host;
+    const Plan& p = plan->p;
+    cudaStream_t s = (cudaStream_t)stream;
+    const float2* src = static_cast<const float2*>(coeffs_host);
+    for (int k0 = 0; k0 < K && e == cudaSuccess; k0 += h.chunk) {
+        const int c = std::min(h.chunk, K - k0);
+        const int i = h.in_next;
+        h.in_next ^= 1;
+        // the slot's previous chunk has been read by its synthesis
+        e = cudaStreamWaitEvent(h.copy_in, h.in_free[i], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(h.in_slot[i], p.nlm * sizeof(float2), src + (int64_t)k0 * ldc, ldc * sizeof(float2),
+                                  p.nlm * sizeof(float2), c, cudaMemcpyHostToDevice, h.copy_in);
+        if (e == cudaSuccess) e = cudaEventRecord(h.in_ready[i], h.copy_in);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, h.in_ready[i], 0);
+        if (e == cudaSuccess) e = legendre_synthesis(p, h.in_slot[i], p.nlm, c, s);
+        if (e == cudaSuccess) e = launch_fft_synthesis(p, grid + (int64_t)k0 * ldg, ldg, c, flags, s);
+        if (e == cudaSuccess) e = cudaEventRecord(h.in_free[i], s);
+    }
+    return finish(e, "sht_synthesize_host");
+}
+
+int sht_analyze_host(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs_host, int64_t ldc, int K,
+                     unsigned flags, void* stream) {
+    int rc;
+    if ((rc = check_call(plan, K, "sht_analyze_host")) != SHT_OK) return rc;
+    if ((rc = check_ldc(plan->p, ldc, "sht_analyze_host")) != SHT_OK) return rc;
+    if ((rc = check_ldg(plan->p, ldg, "sht_analyze_host")) != SHT_OK) return rc;
+    if (flags & SHT_ADD) return fail(SHT_EINVAL, "sht_analyze_host: SHT_ADD into host memory is not supported");
+    if (K == 0) return SHT_OK;
+    if (!ok_ptr(coeffs_host) || !ok_ptr(grid)) return fail(SHT_EINVAL, "sht_analyze_host: NULL array");
+    DeviceGuard g(plan->p.device);
+    cudaError_t e = plan->host.chunk ? cudaSuccess : host_prepare(plan, kDefaultHostChunk);
+    if (e != cudaSuccess) return cuda_fail(e, "sht_analyze_host (staging)");
+    HostPipe& h = plan->host;
+    const Plan& p = plan->p;
+    cudaStream_t s = (cudaStream_t)stream;
+    float2* dst = static_cast<float2*>(coeffs_host);
+    for (int k0 = 0; k0 < K && e == cudaSuccess; k0 += h.chunk) {
+        const int c = std::min(h.chunk, K - k0);
+        const int i = h.out_next;
+        h.out_next ^= 1;
+        // the slot's previous chunk has reached the host
+        e = cudaStreamWaitEvent(s, h.out_free[i], 0);
+        if (e == cudaSuccess) e = launch_fft_analysis(p, grid + (int64_t)k0 * ldg, ldg, c, s);
+        if (e == cudaSuccess) e = legendre_analysis(p, h.out_slot[i], p.nlm, c, false, s);
+        if (e == cudaSuccess) e = cudaEventRecord(h.out_ready[i], s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(h.copy_out, h.out_ready[i], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(dst + (int64_t)k0 * ldc, ldc * sizeof(float2), h.out_slot[i], p.nlm * sizeof(float2),
+                                  p.nlm * sizeof(float2), c, cudaMemcpyDeviceToHost, h.copy_out);
+        if (e == cudaSuccess) e = cudaEventRecord(h.out_free[i], h.copy_out);
+    }
+    return finish(e, "sht_analyze_host");
+}
+
+int sht_host_wait(sht_plan* plan, void* stream) {
+    if (!plan) return fail(SHT_EINVAL, "sht_host_wait: NULL plan");
+    if (!plan->host.chunk) return SHT_OK;
+    DeviceGuard g(plan->p.device);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent((cudaStream_t)stream, plan->host.out_free[i], 0);
+    return finish(e, "sht_host_wait");
 }
 
 int sht_synthesize_adjoint(sht_plan* plan, const float* grid_bar, int64_t ldg, void* coeffs_bar, int64_t ldc, int K,

@@ -47,6 +47,10 @@ SIGNATURES = {
                                   C.POINTER(C.c_int32)]),
     "sht_synthesize": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
     "sht_analyze": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
+    "sht_plan_set_host_chunk": (C.c_int, [_P, C.c_int]),
+    "sht_synthesize_host": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
+    "sht_analyze_host": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
+    "sht_host_wait": (C.c_int, [_P, _P]),
     "sht_legendre_synthesis": (C.c_int, [_P, _P, _I64, C.c_int, _P]),
     "sht_fourier_synthesis": (C.c_int, [_P, _P, _I64, C.c_int, C.c_uint, _P]),
     "sht_fourier_analysis": (C.c_int, [_P, _P, _I64, C.c_int, _P]),

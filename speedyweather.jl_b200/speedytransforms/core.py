@@ -193,8 +193,11 @@ class LowerTriangularArray:
         return f"LowerTriangularArray({self.spectrum}, K={self.nlayers})"
 
 
-def _ld_and_k(t: torch.Tensor, width: int, what: str):
-    if not t.is_cuda:
+def _ld_and_k(t: torch.Tensor, width: int, what: str, host: bool = False):
+    if host:
+        if t.is_cuda:
+            raise ValueError(f"{what} must live in host memory")
+    elif not t.is_cuda:
         raise ValueError(f"{what} must live on a CUDA device")
     if t.dim() == 1:
         if t.stride(0) != 1:
@@ -212,14 +215,14 @@ def _stream_ptr(device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
 
 
-def _coeff_arg(lta: LowerTriangularArray, S, what):
+def _coeff_arg(lta: LowerTriangularArray, S, what, host: bool = False):
     if not isinstance(lta, LowerTriangularArray):
         raise TypeError(f"{what} must be a LowerTriangularArray")
     if lta.data.dtype != torch.complex64:
         raise TypeError(f"{what}: coefficients must be complex64 (NF = Float32)")
     if lta.spectrum != S.spectrum:
         raise DimensionMismatch(f"SpectralTransform for {S.spectrum} and {what} on {lta.spectrum} do not match")
-    return _ld_and_k(lta.data, S.spectrum.nlm, what)
+    return _ld_and_k(lta.data, S.spectrum.nlm, what, host)
 
 
 def _field_arg(f: Field, S, what):
@@ -311,6 +314,15 @@ class SpectralTransform:
         v = C.c_int32(0)
         check(lib.sht_device_status(self._plan, C.byref(v)))
         return int(v.value)
+
+    def host_wait(self):
+        """Make the current stream wait for the copies of host-memory coefficients that
+        earlier transforms issued (synchronise it afterwards to read them)."""
+        check(lib.sht_host_wait(self._plan, _stream_ptr(self.device)))
+
+    def set_host_chunk(self, layers: int):
+        """Layers per chunk of the host-memory transforms (allocates the staging slots)."""
+        check(lib.sht_plan_set_host_chunk(self._plan, int(layers)))
 
     def autotune(self, nlayers: int | None = None):
         """Time the FP32 Legendre kernels at ``nlayers`` layers for each tile width and
@@ -445,26 +457,35 @@ def _check_k(S, K, *others):
 
 def transform_(out, inp, S: SpectralTransform, *, unscale_coslat: bool = False, add: bool = False):
     """transform!(out, in, S): synthesis if ``out`` is a Field, analysis if it is a
-    LowerTriangularArray (spectral_transform.jl:515-531, 579-593)."""
+    LowerTriangularArray (spectral_transform.jl:515-531, 579-593). Coefficients may live
+    in host memory (page-locked for overlap; the field on the device): the copies then
+    run inside the call, pipelined over chunks of layers on the plan's copy streams
+    (sht_synthesize_host / sht_analyze_host); host results are complete after
+    ``S.host_wait()`` and a synchronisation of the current stream."""
     dev = S.device
     if isinstance(S, MatrixSpectralTransform):
         return _matrix_transform_(out, inp, S, unscale_coslat=unscale_coslat, add=add)
     if isinstance(out, Field) and isinstance(inp, LowerTriangularArray):
         ldg, K = _field_arg(out, S, "field")
-        ldc, K2 = _coeff_arg(inp, S, "coeffs")
+        host = isinstance(inp.data, torch.Tensor) and not inp.data.is_cuda
+        ldc, K2 = _coeff_arg(inp, S, "coeffs", host)
         _check_k(S, K, K2)
         flags = (_lib.UNSCALE_COSLAT if unscale_coslat else 0) | (_lib.ADD if add else 0)
-        check(lib.sht_synthesize(S.handle, inp.data.data_ptr(), ldc, out.data.data_ptr(), ldg, K, flags,
-                                 _stream_ptr(dev)))
+        fn = lib.sht_synthesize_host if host else lib.sht_synthesize
+        check(fn(S.handle, inp.data.data_ptr(), ldc, out.data.data_ptr(), ldg, K, flags, _stream_ptr(dev)))
         return out
     if isinstance(out, LowerTriangularArray) and isinstance(inp, Field):
         if unscale_coslat:
             raise TypeError("unscale_coslat applies to spectral-to-grid transforms only")
-        ldc, K = _coeff_arg(out, S, "coeffs")
+        host = isinstance(out.data, torch.Tensor) and not out.data.is_cuda
+        ldc, K = _coeff_arg(out, S, "coeffs", host)
         ldg, K2 = _field_arg(inp, S, "field")
         _check_k(S, K, K2)
-        check(lib.sht_analyze(S.handle, inp.data.data_ptr(), ldg, out.data.data_ptr(), ldc, K,
-                              _lib.ADD if add else 0, _stream_ptr(dev)))
+        if host and add:
+            raise TypeError("add=True needs device coefficients")
+        fn = lib.sht_analyze_host if host else lib.sht_analyze
+        check(fn(S.handle, inp.data.data_ptr(), ldg, out.data.data_ptr(), ldc, K, _lib.ADD if add else 0,
+                 _stream_ptr(dev)))
         return out
     raise TypeError("transform_(out, in, S) needs (Field, LowerTriangularArray) or (LowerTriangularArray, Field)")
 
