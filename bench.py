@@ -352,7 +352,7 @@ def run_column_emulator(args):
         return sp.columns_as_rows(T, q, u, v, ps), torch.cat([dT.T, dq.T], dim=1).contiguous()
 
     x, y = rows(sp.synthetic_columns(ntrain, seed=0, device=device))
-    em = sp.ColumnEmulator(batch, seed=0, device=device)
+    em = sp.ColumnEmulator(max(batch, ncol), seed=0, device=device)
     em.fit_normalization(x, y)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     g = torch.Generator(device=device).manual_seed(0)
