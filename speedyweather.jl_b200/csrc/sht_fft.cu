@@ -512,6 +512,14 @@ __device__ __forceinline__ void put_pieces(uint8_t* dst, int64_t piece_stride, c
 // / 2 for the transform; for the adjoint of the synthesis the rfft adjoint scale
 // (1 for m = 0 and the Nyquist frequency, 2 otherwise; SpeedyTransformsEnzymeExt.jl:33-57)
 // / 2, times 1/cos(lat) when the synthesis unscaled by it.
+// image row of one order for one ring (analysis epilogue of tensor-core plans)
+struct EpiRow {
+    int64_t e;        // byte offset of the row in the E tile, without the column chunk
+    int32_t o_tiles;  // tiles from the E tile to the O tile
+    int32_t r8;       // swizzle phase (row mod 8)
+};
+static_assert(sizeof(EpiRow) == 16, "16 bytes per order fit the spare Stockham buffer");
+
 __device__ __forceinline__ float ana_weight(const RingDesc& rd, int m, int adjoint, int unscale) {
     if (!adjoint) return 0.5f * rd.domega;
     const float sm = (m == 0 || 2 * m == rd.n) ? 1.f : 2.f;
@@ -594,6 +602,20 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
         const int gbeg = cbeg / 8, ngr = (cend + 7) / 8 - gbeg;
         const Div dngr = mkdiv(ngr);
         const int j = item.x;
+        // per order: byte offset of this ring's row in the E tile (all but the column
+        // chunk), distance to the O tile and the row's swizzle phase, computed once with
+        // all table loads in flight, into the Stockham buffer the result does not occupy
+        // (16 bytes per order <= its C ldx float2 since ldx >= 2 (mt + 1) and C >= 1)
+        EpiRow* rows = reinterpret_cast<EpiRow*>(Z == X ? Y : X);
+        const int64_t piece_span = (int64_t)(img.fp16 ? 2 : img.npieces) * img.tile_bytes;
+        for (int m = threadIdx.x; m < nm; m += blockDim.x) {
+            const int jj = j - img.j0[m];
+            const int r = jj % 64;
+            const int64_t t0 = img.tile_base[m] + jj / 64;
+            rows[m] = EpiRow{t0 * piece_span + (r / 8) * 1024 + (r % 8) * 128, img.njt[m] * (img.fp16 ? 2 : img.npieces),
+                             r % 8};
+        }
+        __syncthreads();
         for (int w = threadIdx.x; w < ngr * nm; w += blockDim.x) {
             const int m = quo(w, dngr);
             const int g = gbeg + (w - m * ngr);
@@ -620,21 +642,20 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
                     mask |= 3u << (2 * t);
                 }
             }
-            const int jj = j - img.j0[m];
-            const int r = jj % 64;
             // column block of 64 (8 KB apart), 8-row group, row, swizzled 16-byte chunk
-            const int64_t row_off = (int64_t)(g / 8) * 8192 + (r / 8) * 1024 + (r % 8) * 128 + (((g % 8) ^ (r % 8)) * 16);
-            uint8_t* base = reinterpret_cast<uint8_t*>(img.base) + row_off;
-            const int64_t t0 = img.tile_base[m] + jj / 64;
+            const EpiRow ro = rows[m];
+            uint8_t* eb = reinterpret_cast<uint8_t*>(img.base) + ro.e + (int64_t)(g / 8) * 8192 +
+                          (((g % 8) ^ ro.r8) * 16);
+            const int64_t odist = (int64_t)ro.o_tiles * img.tile_bytes;
             if (img.fp16) {
-                put_pieces<2, true>(base + t0 * 2 * img.tile_bytes, img.tile_bytes, ev, mask);
-                put_pieces<2, true>(base + (t0 + img.njt[m]) * 2 * img.tile_bytes, img.tile_bytes, ov, mask);
+                put_pieces<2, true>(eb, img.tile_bytes, ev, mask);
+                put_pieces<2, true>(eb + odist, img.tile_bytes, ov, mask);
             } else if (img.npieces == 2) {
-                put_pieces<2, false>(base + t0 * 2 * img.tile_bytes, img.tile_bytes, ev, mask);
-                put_pieces<2, false>(base + (t0 + img.njt[m]) * 2 * img.tile_bytes, img.tile_bytes, ov, mask);
+                put_pieces<2, false>(eb, img.tile_bytes, ev, mask);
+                put_pieces<2, false>(eb + odist, img.tile_bytes, ov, mask);
             } else {
-                put_pieces<3, false>(base + t0 * 3 * img.tile_bytes, img.tile_bytes, ev, mask);
-                put_pieces<3, false>(base + (t0 + img.njt[m]) * 3 * img.tile_bytes, img.tile_bytes, ov, mask);
+                put_pieces<3, false>(eb, img.tile_bytes, ev, mask);
+                put_pieces<3, false>(eb + odist, img.tile_bytes, ov, mask);
             }
         }
         return;
