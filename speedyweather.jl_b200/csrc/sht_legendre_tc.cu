@@ -53,7 +53,7 @@ namespace sht {
 
 namespace {
 
-constexpr int TC_THREADS = 192;
+constexpr int TC_THREADS = 320;     // producer warp, MMA warp, 8 epilogue warps
 constexpr int BLK = 64;                     // Legendre box edge (rows x rings)
 constexpr int BOX_BYTES = BLK * BLK * 2;    // 8 KB
 constexpr int A_PIECE_BYTES = 2 * BOX_BYTES;
@@ -158,16 +158,40 @@ __device__ __forceinline__ int item_steps(const TcDev& t, const TcItem& it) {
     return SYN ? t.nkt[it.m] : t.njt[it.m];
 }
 
+// A CTA's items with their step counts and data-image tile bases, fetched by all its
+// threads at once before the roles start (shared memory), so the producer does not wait
+// on dependent global loads at the start of every item.
+struct ItemInfo {
+    TcItem it;
+    int64_t tb;       // image tile index of (m, par, step 0)
+    int32_t nsteps;
+    int32_t pad;
+};
+constexpr int TC_ITEM_CACHE = 128;
+constexpr int TC_ITEM_BYTES = TC_ITEM_CACHE * (int)sizeof(ItemInfo);
+
+template <bool SYN>
+__device__ __forceinline__ ItemInfo item_info(const TcDev& t, const TcItem& it) {
+    ItemInfo f;
+    f.it = it;
+    f.nsteps = item_steps<SYN>(t, it);
+    f.tb = SYN ? t.syn_tile_base[it.m] + (int64_t)it.par * t.nkt[it.m]
+               : t.ana_tile_base[it.m] + (int64_t)it.par * t.njt[it.m];
+    f.pad = 0;
+    return f;
+}
+
 template <bool SYN>
 __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_cols, int K, uint32_t taddr, int r,
-                               float2* four, float2* coeffs, int64_t ldc, int add, bool good, bool accumulate) {
+                               int cb, float2* four, float2* coeffs, int64_t ldc, int add, bool good, bool accumulate) {
+    // this warp's column chunks: cb, cb + 64, ... (the other warp of its lane quarter takes the rest)
     const int m = it.m, par = it.par, tile = it.tile;
     const float mscale = t.fp16 ? ldexpf(1.f, t.mexp[m] - F16_TOP) : 1.f;
     if (SYN && t.matrix) {
         const int row = tile * 128 + r;
         const bool valid = good && row < t.mrows;
         const float rs = (valid && t.row_scale) ? t.row_scale[row] : 1.f;
-        for (int c0 = 0; c0 < nt_cols; c0 += 32) {
+        for (int c0 = cb; c0 < nt_cols; c0 += 64) {
             float v[32];
             tmem_ld32(taddr + c0, v);
             if (!valid) continue;
@@ -188,7 +212,7 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
         const int j = t.j0[m] + tile * 128 + r;
         const bool valid = good && j < t.nh && m <= t.rings[j].mt;
         float2* dst = valid ? four + ((t.rings[j].gofs + m) * 2 + par) * K : nullptr;
-        for (int c0 = 0; c0 < nt_cols; c0 += 32) {
+        for (int c0 = cb; c0 < nt_cols; c0 += 64) {
             float v[32];
             tmem_ld32(taddr + c0, v);
             if (!valid) continue;
@@ -215,7 +239,7 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
         const int i = tile * 128 + r;
         const bool valid = good && i < t.rows[m] && m + 2 * i + par < t.lmax;
         const int64_t lmo = t.lm_off[m];
-        for (int c0 = 0; c0 < nt_cols; c0 += 32) {
+        for (int c0 = cb; c0 < nt_cols; c0 += 64) {
             float v[32];
             tmem_ld32(taddr + c0, v);
             if (!valid) continue;
@@ -256,9 +280,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + (size_t)stages * stage_bytes);
     uint64_t* empty_bar = full_bar + stages;
     uint64_t* accf = empty_bar + stages;             // accumulator a ready   (tcgen05.commit)
-    uint64_t* acce = accf + 2;                       // accumulator a drained (128 epilogue threads)
+    uint64_t* acce = accf + 2;                       // accumulator a drained (256 epilogue threads)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acce + 2);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    ItemInfo* info = reinterpret_cast<ItemInfo*>(smem + (size_t)stages * stage_bytes + 256);
+    {   // this CTA's items ix = blockIdx.x + i gridDim.x, the first TC_ITEM_CACHE of them
+        const int n_my = (int)blockIdx.x < nitems ? (nitems - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+        for (int i = threadIdx.x; i < min(n_my, TC_ITEM_CACHE); i += blockDim.x)
+            info[i] = item_info<SYN>(t, items[blockIdx.x + i * gridDim.x]);
+    }
+    auto get = [&](int i, int ix) { return i < TC_ITEM_CACHE ? info[i] : item_info<SYN>(t, items[ix]); };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; ++s) {
@@ -267,7 +298,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&accf[a], 1);
-            mbar_init(&acce[a], 128);
+            mbar_init(&acce[a], 256);
         }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -290,13 +321,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int64_t col_off = SYN ? (int64_t)ct * 256 * 128 : (int64_t)ct * 4 * BOX_BYTES;
         int g = 0;
         bool ok = true;
-        for (int ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ix += gridDim.x) {
-            const TcItem it = items[ix];
-            const int m = it.m, par = it.par, tile = it.tile;
-            const int nsteps = item_steps<SYN>(t, it);
+        for (int i = 0, ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ++i, ix += gridDim.x) {
+            const ItemInfo f = get(i, ix);
+            const int m = f.it.m, par = f.it.par, tile = f.it.tile;
+            const int nsteps = f.nsteps;
             const CUtensorMap* map = t.maps + (2 * m + par);
-            const int64_t tb = SYN ? t.syn_tile_base[m] + (int64_t)par * t.nkt[m]
-                                   : t.ana_tile_base[m] + (int64_t)par * t.njt[m];
+            const int64_t tb = f.tb;
             for (int ks = 0; ks < nsteps; ++ks, ++g) {
                 const int s = g % stages;
                 if (g >= stages && !mbar_wait(&empty_bar[s], ((g / stages) - 1) & 1)) {
@@ -332,9 +362,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const uint32_t idesc = idesc_f16(t.fp16 ? 0u : 1u, SYN ? 1u : 0u, SYN ? 0u : 1u, (uint32_t)nt_cols);
         int g = 0, ti = 0;
         bool ok = true;
-        for (int ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ix += gridDim.x) {
-            const TcItem it = items[ix];
-            const int nsteps = item_steps<SYN>(t, it);
+        for (int i = 0, ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ++i, ix += gridDim.x) {
+            const ItemInfo f = get(i, ix);
+            const int nsteps = f.nsteps;
             if (nsteps == 0) continue;
             const int kch = t.kchunk > 0 ? t.kchunk : nsteps;
           for (int ks0 = 0; ks0 < nsteps && ok; ks0 += kch) {
@@ -383,22 +413,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (ti > 0 && !mbar_wait(&accf[(ti - 1) & 1], ((ti - 1) / 2) & 1)) atomicExch(t.err, 6);
     } else if (warp >= 2) {
         // ------------------------------------------------ epilogue
-        const int quarter = warp % 4;
+        // warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows r); the two warps of a lane
+        // quarter take alternate 32-column chunks
+        const int quarter = warp % 4, half = (warp - 2) / 4;
         const int r = quarter * 32 + lane;
         int ti = 0;
-        for (int ix = blockIdx.x; ix < nitems; ix += gridDim.x) {
-            const TcItem it = items[ix];
-            if (item_steps<SYN>(t, it) == 0) {      // analysis of an order no ring carries: zeros
+        for (int q = 0, ix = blockIdx.x; ix < nitems; ++q, ix += gridDim.x) {
+            const ItemInfo f = get(q, ix);
+            const TcItem it = f.it;
+            if (f.nsteps == 0) {      // analysis of an order no ring carries: zeros
                 if (!SYN && !add && !*abort_flag) {
                     const int i = it.tile * 128 + r;
                     if (i < t.rows[it.m] && it.m + 2 * i + it.par < t.lmax)
-                        for (int c = 0; c < nt_cols && ct * 256 + c < 2 * K; c += 2)
+                        for (int c = 2 * half; c < nt_cols && ct * 256 + c < 2 * K; c += 4)
                             coeffs[(int64_t)((ct * 256 + c) / 2) * ldc + t.lm_off[it.m] + 2 * i + it.par] =
                                 make_float2(0.f, 0.f);
                 }
                 continue;
             }
-            const int nsteps = item_steps<SYN>(t, it);
+            const int nsteps = f.nsteps;
             const int kch = t.kchunk > 0 ? t.kchunk : nsteps;
             bool ok = true;
             for (int ks0 = 0; ks0 < nsteps; ks0 += kch) {
@@ -411,8 +444,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 tc_fence_after();
                 const uint32_t taddr = tmem + (uint32_t)(a * acc_cols) + ((uint32_t)(quarter * 32) << 16);
-                epilogue_store<SYN>(t, it, ct, nt_cols, K, taddr, r, four, coeffs, ldc, add, ok && !*abort_flag,
-                                    ks0 > 0);
+                epilogue_store<SYN>(t, it, ct, nt_cols, K, taddr, r, 32 * half, four, coeffs, ldc, add,
+                                    ok && !*abort_flag, ks0 > 0);
                 tc_fence_before();
                 mbar_arrive(&acce[a]);
                 ++ti;
@@ -577,9 +610,9 @@ TcDev make_dev(const Plan& p) {
 
 int smem_for(int npa, int npb, int nt_cols, int& stages) {
     const int stage_bytes = npa * A_PIECE_BYTES + npb * nt_cols * 128;
-    const int budget = 227 * 1024 - 1024 - 256;      // alignment slack + barriers
+    const int budget = 227 * 1024 - 1024 - 256 - TC_ITEM_BYTES;   // alignment slack, barriers, item table
     stages = std::min(4, budget / stage_bytes);
-    return 1024 + stages * stage_bytes + 256;
+    return 1024 + stages * stage_bytes + 256 + TC_ITEM_BYTES;
 }
 
 }  // namespace
