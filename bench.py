@@ -405,7 +405,7 @@ def run_column_emulator(args):
             "plain_physics_grids_per_s": 1.0 / t_plain, "plain_physics_ms": t_plain * 1e3,
             "validation": {"rel_l2_dtemp": rel(dT, pT), "rel_l2_dhumid": rel(dq, pq),
                            "fallback_fraction": nf / ncol},
-            "gpu_launches_per_grid": 10}
+            "gpu_launches_per_grid": 1}
     print(json.dumps(line))
     return 0
 

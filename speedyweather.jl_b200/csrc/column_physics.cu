@@ -15,34 +15,16 @@
 // constants (atmosphere.jl:14-73).
 #include <cmath>
 
-#include "sht_internal.h"
+#include "column_physics.cuh"
 
 namespace sht {
 int set_error(int code, const char* msg);
 }
 
 using namespace sht;
+using namespace sht::colphys;
 
 namespace {
-
-constexpr int NL = SHT_COLUMN_LAYERS;
-constexpr float MOL_MASS_DRY = 28.9649f, MOL_MASS_VAPOR = 18.0153f, CP = 1004.0f, R_GAS = 8.3145f;
-constexpr float R_DRY = 1000.f * R_GAS / MOL_MASS_DRY, R_VAPOR = 1000.f * R_GAS / MOL_MASS_VAPOR;
-constexpr float EPS = R_DRY / R_VAPOR, MU_VIRT = (1.f - EPS) / EPS;
-constexpr float RHO_WATER = 1000.f, LV = 2501.0e3f, LF = 3.3e5f, E0 = 610.78f, T0 = 273.15f, GRAVITY = 9.81f;
-constexpr float RH_THRESHOLD = 0.95f, REEVAPORATION = 30.f, FREEZING = 263.f, MELTING = 278.f, COND_TIME = 3.f;
-constexpr float CONV_TIME = 4.f * 3600.f, CONV_RH = 0.7f;
-
-struct Levels {
-    float half[NL + 1], full[NL], dsig[NL];
-    float dgeo_half[NL], dgeo_full[NL];   // geopotential integration coefficients (geopotential.jl:36-60)
-    float dry_ratio[NL];                  // (full[k] / full[k + 1])^kappa
-};
-
-__device__ __forceinline__ float qsat(float T, float p) {
-    return EPS * E0 * expf(LV / R_VAPOR * (1.f / T0 - 1.f / T)) / p;
-}
-__device__ __forceinline__ float tvirt(float T, float q) { return T * (1.f + MU_VIRT * q); }
 
 __global__ void column_physics_kernel(const float* __restrict__ temp, const float* __restrict__ humid,
                                       const float* __restrict__ ps_, int64_t ld, int ncol, float dt, const Levels L,
@@ -54,117 +36,8 @@ __global__ void column_physics_kernel(const float* __restrict__ temp, const floa
     for (int k = 0; k < NL; ++k) {
         T[k] = temp[(int64_t)k * ld + ij];
         q[k] = humid[(int64_t)k * ld + ij];
-        dT[k] = dq[k] = 0.f;
     }
-    const float ps = ps_[ij];
-
-    // ---- large-scale condensation (large_scale_condensation.jl:84-160) ----
-    {
-        float rain = 0.f, snow = 0.f;
-        const float g_rho = GRAVITY * RHO_WATER, lv_cp = LV / CP, lf_cp = LF / CP, cp_lf = CP / LF;
-#pragma unroll
-        for (int k = 0; k < NL; ++k) {
-            const float qs = qsat(T[k], L.full[k] * ps);
-            const float dq_cond = qs * RH_THRESHOLD - q[k];
-            if (dq_cond < 0.f || snow > 0.f || rain > 0.f) {
-                const float dp_grho = L.dsig[k] * ps / g_rho;
-                const float dp_dtgrho = dp_grho / dt;
-                const float dtgrho_dp = 1.f / dp_dtgrho;
-                const float melt = fminf(snow, cp_lf * fmaxf(T[k] - MELTING, 0.f) * dp_dtgrho);
-                snow -= melt;
-                rain += melt;
-                const float dT_melt = -lf_cp * (melt * dtgrho_dp);
-                const float evap = fminf(REEVAPORATION * fmaxf(qs - q[k], 0.f), 1.f) * rain;
-                rain -= evap;
-                float dqk = fminf(0.f, dq_cond) + evap * dtgrho_dp;
-                const float Tn = T[k] + dt * dT_melt;
-                const float dqsat_dT = qs * RH_THRESHOLD * lv_cp / (R_VAPOR * Tn * Tn);
-                dqk /= (1.f + lv_cp * dqsat_dT) * COND_TIME * dt;
-                float dTk = -lv_cp * dqk;
-                const float dq_rain = fminf(0.f, dqk);
-                float r = dp_grho * -dq_rain, s = 0.f;
-                if (T[k] < FREEZING) {
-                    s = r;
-                    r = 0.f;
-                }
-                rain += r;
-                snow += s;
-                if (s > 0.f) dTk -= lf_cp * dq_rain;
-                dq[k] += dqk;
-                dT[k] += dTk;
-            }
-        }
-    }
-
-    // ---- convection (convection.jl:33-253) ----
-    {
-        float phi[NL];                                  // geopotential, flat orography
-        float Tv = tvirt(T[NL - 1], q[NL - 1]);
-        phi[NL - 1] = Tv * L.dgeo_full[NL - 1];
-#pragma unroll
-        for (int k = NL - 2; k >= 0; --k) {
-            const float Tv_below = Tv;
-            Tv = tvirt(T[k], q[k]);
-            phi[k] = phi[k + 1] + Tv_below * L.dgeo_half[k + 1] + Tv * L.dgeo_full[k];
-        }
-        float Tref[NL], qref[NL];
-        float Tp = T[NL - 1], qp = q[NL - 1];
-        Tref[NL - 1] = Tp;
-        bool saturated = false, buoyant = true;
-        int k = NL - 1;
-        float Tvp = tvirt(Tp, qp);
-        while (buoyant && k > 0) {
-            --k;
-            float Tdry = 0.f;
-            if (!saturated) {
-                Tdry = Tp * L.dry_ratio[k];
-                saturated = qp >= qsat(Tdry, L.full[k] * ps);
-            }
-            if (saturated) {
-                const float om = 1.f - qp;
-                const float A = qp * LV / (om * om * R_DRY);
-                const float B = qp * LV * LV / (om * om * CP * R_VAPOR);
-                const float gam = (1.f + A / Tvp) / (1.f + B / (Tp * Tp));
-                Tp = Tp - (phi[k] - phi[k + 1]) / CP * gam;
-                qp = qsat(Tp, L.full[k] * ps);
-            } else {
-                Tp = Tdry;
-            }
-            Tref[k] = Tp;
-            Tvp = tvirt(Tp, qp);
-            buoyant = Tvp > tvirt(T[k], q[k]);
-        }
-        const int lzb = k + (buoyant ? 0 : 1);
-        float Pq = 0.f, PT = 0.f;
-        for (int j = lzb; j < NL; ++j) {
-            qref[j] = qsat(Tref[j], ps * L.full[j]) * CONV_RH;
-            Pq += (q[j] - qref[j]) * L.dsig[j];
-            PT -= (T[j] - Tref[j]) * L.dsig[j];
-        }
-        const bool deep = Pq > 0.f && PT > 0.f;
-        const bool shallow = Pq <= 0.f && PT > 0.f;
-        if (deep || shallow) {
-            const float dsig_lzb = L.half[NL] - L.half[lzb];
-            if (deep) {
-                const float dTr = (PT - Pq * LV / CP) / dsig_lzb;
-                for (int j = lzb; j < NL; ++j) Tref[j] -= dTr;
-            } else {
-                float Qref = 0.f;
-                for (int j = lzb; j < NL; ++j) Qref -= qref[j] * L.dsig[j];
-                const float fq = 1.f - Pq / Qref;
-                const float dTr = PT / dsig_lzb;
-                for (int j = lzb; j < NL; ++j) {
-                    qref[j] *= fq;
-                    Tref[j] -= dTr;
-                }
-            }
-            const float tau_inv = 1.f / CONV_TIME;
-            for (int j = lzb; j < NL; ++j) {
-                dT[j] -= (T[j] - Tref[j]) * tau_inv;
-                dq[j] -= (q[j] - qref[j]) * tau_inv;
-            }
-        }
-    }
+    column_tendencies(T, q, ps_[ij], dt, L, dT, dq);
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
         float* a = dtemp + (int64_t)k * ldo + ij;
@@ -178,7 +51,10 @@ __global__ void column_physics_kernel(const float* __restrict__ temp, const floa
 
 namespace sht {
 // sigma levels and geopotential coefficients (FP64, rounded once)
-void column_levels(float* half, float* full, float* dsig, float* dgeo_half, float* dgeo_full, float* dry_ratio) {
+Levels column_levels() {
+    Levels L;
+    float *half = L.half, *full = L.full, *dsig = L.dsig, *dgeo_half = L.dgeo_half, *dgeo_full = L.dgeo_full,
+          *dry_ratio = L.dry_ratio;
     double h[NL + 1], f[NL];
     for (int k = 0; k <= NL; ++k) h[k] = (double)k / NL;
     for (int k = 0; k < NL; ++k) f[k] = 0.5 * (h[k] + h[k + 1]);
@@ -191,12 +67,12 @@ void column_levels(float* half, float* full, float* dsig, float* dgeo_half, floa
         dgeo_full[k] = (float)(r_dry * std::log(h[k + 1] / f[k]));
         dry_ratio[k] = k + 1 < NL ? (float)std::pow(f[k] / f[k + 1], kappa) : 1.f;
     }
+    return L;
 }
 
 cudaError_t launch_column_physics(const float* temp, const float* humid, const float* ps, int64_t ld, int ncol,
                                   float dt, float* dtemp, float* dhumid, int64_t ldo, bool add, cudaStream_t s) {
-    Levels L;
-    column_levels(L.half, L.full, L.dsig, L.dgeo_half, L.dgeo_full, L.dry_ratio);
+    const Levels L = column_levels();
     if (ncol <= 0) return cudaSuccess;
     column_physics_kernel<<<(ncol + 127) / 128, 128, 0, s>>>(temp, humid, ps, ld, ncol, dt, L, dtemp, dhumid, ldo,
                                                               add ? 1 : 0);

@@ -33,6 +33,7 @@
 #include <random>
 #include <vector>
 
+#include "column_physics.cuh"
 #include "sht_internal.h"
 #include "tc_ptx.cuh"
 
@@ -392,48 +393,271 @@ __global__ void to_bf16_kernel(const float* __restrict__ w, __nv_bfloat16* __res
     if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
 }
 
-// Column emulator glue: gather inputs [ncol][33] from layer-major fields, and scatter the
-// outputs back (emulator where every normalised input lies within z_max, plain physics
-// otherwise).
+// ---- the emulator as one kernel ----------------------------------------------------
+// One CTA per 128 columns: the inputs are gathered from the layer-major fields,
+// normalised and written as BF16 straight into the K-major 128-byte-swizzled activation
+// tile in shared memory; the four layers run on tcgen05 with the weights streamed by TMA
+// (three 32 KB stages, 13 blocks of 64 input features in all) and the accumulator in
+// TMEM; after each hidden layer 8 epilogue warps add the bias, apply GELU and write the
+// BF16 activations back into the tile in place (the layer's MMAs have completed), so no
+// activation leaves the SM. The output layer is de-normalised and written into the
+// tendency fields; columns outside the training range get the plain physics instead.
 constexpr int NLC = SHT_COLUMN_LAYERS;
-__global__ void gather_columns_kernel(const float* __restrict__ T, const float* __restrict__ q,
-                                      const float* __restrict__ u, const float* __restrict__ v,
-                                      const float* __restrict__ ps, int64_t ld, int ncol, float* __restrict__ x) {
-    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ij >= ncol) return;
-    float* r = x + (int64_t)ij * (4 * NLC + 1);
-#pragma unroll
-    for (int k = 0; k < NLC; ++k) {
-        r[k] = T[(int64_t)k * ld + ij];
-        r[NLC + k] = q[(int64_t)k * ld + ij];
-        r[2 * NLC + k] = u[(int64_t)k * ld + ij];
-        r[3 * NLC + k] = v[(int64_t)k * ld + ij];
-    }
-    r[4 * NLC] = logf(ps[ij]);
+constexpr int F_THREADS = 320;                       // producer warp, MMA warp, 8 epilogue warps
+constexpr int F_STAGES = 3;
+constexpr int F_W_STAGE = 4 * G_BOX_BYTES;           // 256 rows x 64 features
+constexpr int F_ACT_BYTES = 4 * 2 * G_BOX_BYTES;     // 128 rows x 256 features (4 blocks of 16 KB)
+constexpr int F_TAIL = 128 + 256;                    // barriers, inside flags [2][128]
+constexpr int F_SMEM = 1024 + F_ACT_BYTES + F_STAGES * F_W_STAGE + F_TAIL;
+
+struct FusedArgs {
+    const float *T, *q, *u, *v, *ps;
+    int64_t ld;
+    int ncol;
+    const float *xm, *xs, *ym, *ys;
+    const float* bias[4];
+    float zmax, dt;
+    colphys::Levels L;
+    float *dT, *dq;
+    int add;
+    int32_t* nfallback;
+    int32_t* err;
+};
+
+// byte offset of feature k (< 256) of row r (< 128) in the K-major SWIZZLE_128B tile
+__device__ __forceinline__ uint32_t act_off(int r, int k) {
+    return (uint32_t)((k >> 6) * (2 * G_BOX_BYTES) + r * 128 + ((((k & 63) >> 3) ^ (r & 7)) << 4) + ((k & 7) << 1));
 }
-__global__ void scatter_columns_kernel(const float* __restrict__ x, const float* __restrict__ mean,
-                                       const float* __restrict__ stdv, float zmax, const float* __restrict__ y,
-                                       const float* __restrict__ dT_plain, const float* __restrict__ dq_plain,
-                                       int64_t ld, int ncol, float* __restrict__ dT, float* __restrict__ dq, int add,
-                                       int* __restrict__ nfallback) {
-    // dT_plain, dq_plain: [layer][ncol]
-    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ij >= ncol) return;
-    const float* r = x + (int64_t)ij * (4 * NLC + 1);
-    bool inside = true;
-    for (int c = 0; c < 4 * NLC + 1; ++c) inside = inside && fabsf((r[c] - mean[c]) / stdv[c]) <= zmax;
-    if (!inside) atomicAdd(nfallback, 1);
-    const float* yo = y + (int64_t)ij * 2 * NLC;
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
+           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__global__ void __launch_bounds__(F_THREADS, 1)
+    mlp_fused_kernel(const __grid_constant__ CUtensorMap w0, const __grid_constant__ CUtensorMap w1,
+                     const __grid_constant__ CUtensorMap w2, const __grid_constant__ CUtensorMap w3,
+                     const FusedArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* act = smem;
+    uint8_t* wst = smem + F_ACT_BYTES;
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(wst + F_STAGES * F_W_STAGE);
+    uint64_t* empty_bar = full_bar + F_STAGES;
+    uint64_t* acc_bar = empty_bar + F_STAGES;         // layer l accumulated (phase l)
+    uint64_t* act_bar = acc_bar + 1;                  // input of layer l in the tile (phase l)
+    uint64_t* mma_bar = act_bar + 1;                  // every issued MMA complete
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    uint8_t* inside = reinterpret_cast<uint8_t*>(full_bar) + 128;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int col0 = blockIdx.x * 128;
+    const int nrow = min(128, a.ncol - col0);
+    const int nkb[4] = {1, 4, 4, 4}, nbox[4] = {4, 4, 4, 1}, nout[4] = {256, 256, 256, 16};
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < F_STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        mbar_init(acc_bar, 1);
+        mbar_init(act_bar, 256);
+        mbar_init(mma_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(256u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---- producer: the weight blocks of the four layers in order
+        const CUtensorMap* maps[4] = {&w0, &w1, &w2, &w3};
+        int g = 0;
+        for (int l = 0; l < 4 && !*abort_flag; ++l)
+            for (int kb = 0; kb < nkb[l] && !*abort_flag; ++kb, ++g) {
+                const int s = g % F_STAGES;
+                if (g >= F_STAGES && !mbar_wait(&empty_bar[s], ((g / F_STAGES) - 1) & 1)) {
+                    *abort_flag = 1;
+                    atomicExch(a.err, 21);
+                    break;
+                }
+                uint8_t* st = wst + s * F_W_STAGE;
+                mbar_expect_tx(&full_bar[s], (uint32_t)(nbox[l] * G_BOX_BYTES));
+                for (int h = 0; h < nbox[l]; ++h) tma_load_2d(st + h * G_BOX_BYTES, maps[l], kb * G_BOX, h * G_BOX, &full_bar[s]);
+            }
+        for (int u = g - 1; u >= 0 && u >= g - F_STAGES; --u)   // no copy lands after the exit
+            if (!mbar_wait(&full_bar[u % F_STAGES], (u / F_STAGES) & 1)) atomicExch(a.err, 22);
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer: layer l once its input is in the tile
+        int g = 0;
+        bool ok = true;
+        for (int l = 0; l < 4 && ok; ++l) {
+            if (!mbar_wait(act_bar, l & 1)) {
+                *abort_flag = 1;
+                atomicExch(a.err, 23);
+                break;
+            }
+            tc_fence_after();
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)nout[l] >> 3) << 17) | ((128u >> 4) << 24);
+            for (int kb = 0; kb < nkb[l]; ++kb, ++g) {
+                const int s = g % F_STAGES;
+                if (!mbar_wait(&full_bar[s], (g / F_STAGES) & 1)) {
+                    *abort_flag = 1;
+                    atomicExch(a.err, 24);
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t sa = smem_u32(act + kb * 2 * G_BOX_BYTES), sb = smem_u32(wst + s * F_W_STAGE);
+                for (int kk = 0; kk < G_BOX / 16; ++kk)
+                    umma_f16(tmem, sdesc(sa + kk * 32, 16, 1024), sdesc(sb + kk * 32, 16, 1024), idesc,
+                             (kb | kk) ? 1u : 0u);
+                umma_commit(&empty_bar[s]);
+            }
+            if (ok) umma_commit(acc_bar);
+        }
+        umma_commit(mma_bar);
+        if (!mbar_wait(mma_bar, 0)) atomicExch(a.err, 25);
+    } else if (warp >= 2) {
+        const int et = threadIdx.x - 64;
+        {   // ---- gather: row r, features [32 kh, 32 kh + 32), normalised, BF16 into the tile
+            const int r = et & 127, kh = et >> 7;
+            const int64_t ij = col0 + r;
+            bool in = true;
+            uint32_t pk[16];
 #pragma unroll
-    for (int k = 0; k < NLC; ++k) {
-        const float a = inside ? yo[k] : dT_plain[(int64_t)k * ncol + ij];
-        const float b = inside ? yo[NLC + k] : dq_plain[(int64_t)k * ncol + ij];
-        float* pa = dT + (int64_t)k * ld + ij;
-        float* pb = dq + (int64_t)k * ld + ij;
-        *pa = add ? *pa + a : a;
-        *pb = add ? *pb + b : b;
+            for (int i = 0; i < 32; i += 2) {
+                float z2[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int c = 32 * kh + i + e;
+                    float z = 0.f;
+                    if (c < 4 * NLC + 1 && r < nrow) {
+                        float x;
+                        if (c < 4 * NLC) {
+                            const float* f = c < NLC ? a.T : c < 2 * NLC ? a.q : c < 3 * NLC ? a.u : a.v;
+                            x = f[(int64_t)(c % NLC) * a.ld + ij];
+                        } else {
+                            x = logf(a.ps[ij]);
+                        }
+                        z = (x - a.xm[c]) / a.xs[c];
+                        in = in && fabsf(z) <= a.zmax;
+                    }
+                    z2[e] = z;
+                }
+                pk[i / 2] = pack_bf16x2(z2[0], z2[1]);
+            }
+#pragma unroll
+            for (int c8 = 0; c8 < 4; ++c8)
+                *reinterpret_cast<uint4*>(act + act_off(r, 32 * kh + 8 * c8)) =
+                    make_uint4(pk[4 * c8], pk[4 * c8 + 1], pk[4 * c8 + 2], pk[4 * c8 + 3]);
+            // features 64 .. 255 of layer 1 stay unread (its K is 64)
+            inside[kh * 128 + r] = in ? 1 : 0;
+            fence_proxy_async();
+            mbar_arrive(act_bar);
+            asm volatile("bar.sync 1, 256;" ::: "memory");   // the flags, among the 8 epilogue warps
+        }
+        const int quarter = warp % 4, half = (warp - 2) / 4;
+        const int r = quarter * 32 + lane;
+        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
+        bool ok = true;
+        for (int l = 0; l < 3 && ok; ++l) {   // ---- hidden layers: bias, GELU, BF16 in place
+            ok = __all_sync(0xffffffffu, mbar_wait(acc_bar, l & 1));
+            if (!ok) {
+                *abort_flag = 1;
+                atomicExch(a.err, 26);
+                break;
+            }
+            tc_fence_after();
+            const float* bias = a.bias[l];
+            for (int c0 = 32 * half; c0 < 256; c0 += 64) {
+                float v[32];
+                tmem_ld32(taddr + c0, v);
+                uint32_t pk[16];
+#pragma unroll
+                for (int q2 = 0; q2 < 16; ++q2)
+                    pk[q2] = pack_bf16x2(gelu(v[2 * q2] + bias[c0 + 2 * q2]), gelu(v[2 * q2 + 1] + bias[c0 + 2 * q2 + 1]));
+#pragma unroll
+                for (int c8 = 0; c8 < 4; ++c8)
+                    *reinterpret_cast<uint4*>(act + act_off(r, c0 + 8 * c8)) =
+                        make_uint4(pk[4 * c8], pk[4 * c8 + 1], pk[4 * c8 + 2], pk[4 * c8 + 3]);
+            }
+            fence_proxy_async();
+            tc_fence_before();
+            mbar_arrive(act_bar);
+        }
+        if (ok) {   // ---- output layer (16 columns): de-normalise, or the plain physics outside the range
+            ok = __all_sync(0xffffffffu, mbar_wait(acc_bar, 1));
+            if (!ok) {
+                *abort_flag = 1;
+                atomicExch(a.err, 27);
+            }
+        }
+        if (ok && half == 0) {
+            tc_fence_after();
+            float v[32];
+            tmem_ld32(taddr, v);
+            if (r < nrow) {
+                const int64_t ij = col0 + r;
+                float dT[NLC], dq[NLC];
+                if (inside[r] && inside[128 + r]) {
+#pragma unroll
+                    for (int k = 0; k < NLC; ++k) {
+                        const float y0 = v[k] + a.bias[3][k], y1 = v[NLC + k] + a.bias[3][NLC + k];
+                        dT[k] = y0 * a.ys[k] + a.ym[k];
+                        dq[k] = y1 * a.ys[NLC + k] + a.ym[NLC + k];
+                    }
+                } else {
+                    float T[NLC], q[NLC];
+#pragma unroll
+                    for (int k = 0; k < NLC; ++k) {
+                        T[k] = a.T[(int64_t)k * a.ld + ij];
+                        q[k] = a.q[(int64_t)k * a.ld + ij];
+                    }
+                    colphys::column_tendencies(T, q, a.ps[ij], a.dt, a.L, dT, dq);
+                    atomicAdd(a.nfallback, 1);
+                }
+#pragma unroll
+                for (int k = 0; k < NLC; ++k) {
+                    float* pa = a.dT + (int64_t)k * a.ld + ij;
+                    float* pb = a.dq + (int64_t)k * a.ld + ij;
+                    *pa = a.add ? *pa + dT[k] : dT[k];
+                    *pb = a.add ? *pb + dq[k] : dq[k];
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
     }
 }
+
+cudaError_t fused_attributes() {
+    static std::mutex mu;
+    static std::vector<bool> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)done.size() <= dev) done.resize(dev + 1, false);
+    if (done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(mlp_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, F_SMEM);
+    if (e == cudaSuccess) done[dev] = true;
+    return e;
+}
+
 
 }  // namespace
 
@@ -455,9 +679,7 @@ struct sht_mlp {
     __nv_bfloat16* dY = nullptr;                    // [cap][nout]
     float *xm = nullptr, *xs = nullptr, *ym = nullptr, *ys = nullptr;   // normalisation
     float* loss = nullptr;
-    float* colbuf = nullptr;                        // [cap][nin]  gathered columns
-    float* ybuf = nullptr;                          // [cap][nout] de-normalised outputs
-    float *plainT = nullptr, *plainq = nullptr;     // [NLC][cap] plain-physics fallback
+    CUtensorMap wmap[NLAYER];                       // TMA maps of the BF16 weights (fused emulator kernel)
     int* nfallback = nullptr;
     float* partial = nullptr;                       // [cap / 256][hidden] bias-gradient partial sums
     static constexpr int MAX_SPLIT = 32;
@@ -497,8 +719,8 @@ void release(sht_mlp* m) {
         for (void* q : ps)
             if (q) cudaFree(q);
     }
-    void* ps[] = {m->X0, m->Y, m->dY, m->xm, m->xs, m->ym, m->ys, m->loss, m->colbuf, m->ybuf, m->plainT, m->plainq,
-                  m->nfallback, m->partial, m->splitbuf, m->err};
+    void* ps[] = {m->X0, m->Y, m->dY, m->xm, m->xs, m->ym, m->ys, m->loss, m->nfallback, m->partial, m->splitbuf,
+                  m->err};
     for (void* q : ps)
         if (q) cudaFree(q);
 }
@@ -586,10 +808,6 @@ int sht_mlp_create(int batch_capacity, uint64_t seed, int device, sht_mlp** out)
     if (e == cudaSuccess) e = alloc(&m->ym, m->nout);
     if (e == cudaSuccess) e = alloc(&m->ys, m->nout);
     if (e == cudaSuccess) e = alloc(&m->loss, 1);
-    if (e == cudaSuccess) e = alloc(&m->colbuf, cap * m->nin);
-    if (e == cudaSuccess) e = alloc(&m->ybuf, cap * m->nout);
-    if (e == cudaSuccess) e = alloc(&m->plainT, cap * NLC);
-    if (e == cudaSuccess) e = alloc(&m->plainq, cap * NLC);
     if (e == cudaSuccess) e = alloc(&m->nfallback, 1);
     if (e == cudaSuccess) e = alloc(&m->partial, (cap / BIAS_ROWS + 1) * m->hidden);
     if (e == cudaSuccess) e = alloc(&m->splitbuf, (size_t)sht_mlp::MAX_SPLIT * m->hidden * m->hidden);
@@ -601,6 +819,8 @@ int sht_mlp_create(int batch_capacity, uint64_t seed, int device, sht_mlp** out)
         cudaMemcpy(m->ym, zero.data(), m->nout * 4, cudaMemcpyHostToDevice);
         e = cudaMemcpy(m->ys, one.data(), m->nout * 4, cudaMemcpyHostToDevice);
     }
+    for (int l = 0; l < 4 && e == cudaSuccess; ++l)
+        if (!make_map(&m->wmap[l], m->Wb[l], m->fan_out[l], m->fan_in[l], m->fan_in[l])) e = cudaErrorInvalidValue;
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         release(m);
@@ -763,22 +983,33 @@ int sht_column_emulate(sht_mlp* m, const float* temp, const float* humid, const 
     if (ncol == 0) return SHT_OK;
     DevGuard dg(m->device);
     cudaStream_t s = (cudaStream_t)stream;
-    cudaError_t e = cudaMemsetAsync(m->nfallback, 0, 4, s);
-    // chunks of the network's batch capacity
-    for (int c0 = 0; c0 < ncol && e == cudaSuccess; c0 += m->cap) {
-        const int nc = std::min(m->cap, ncol - c0);
-        gather_columns_kernel<<<(nc + 127) / 128, 128, 0, s>>>(temp + c0, humid + c0, u + c0, v + c0,
-                                                               surface_pressure + c0, ld, nc, m->colbuf);
-        const int rc = sht_mlp_infer(m, m->colbuf, m->ybuf, nc, stream);
-        if (rc != SHT_OK) return rc;
-        e = launch_column_physics(temp + c0, humid + c0, surface_pressure + c0, ld, nc, (float)dt, m->plainT,
-                                  m->plainq, nc, false, s);
-        if (e == cudaSuccess)
-            scatter_columns_kernel<<<(nc + 127) / 128, 128, 0, s>>>(m->colbuf, m->xm, m->xs, (float)z_max, m->ybuf,
-                                                                    m->plainT, m->plainq, ld, nc, dtemp + c0,
-                                                                    dhumid + c0, (flags & SHT_ADD) ? 1 : 0,
-                                                                    m->nfallback);
-        if (e == cudaSuccess) e = cudaGetLastError();
+    cudaError_t e = fused_attributes();
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->nfallback, 0, 4, s);
+    if (e == cudaSuccess) {
+        FusedArgs fa{};
+        fa.T = temp;
+        fa.q = humid;
+        fa.u = u;
+        fa.v = v;
+        fa.ps = surface_pressure;
+        fa.ld = ld;
+        fa.ncol = ncol;
+        fa.xm = m->xm;
+        fa.xs = m->xs;
+        fa.ym = m->ym;
+        fa.ys = m->ys;
+        for (int l = 0; l < 4; ++l) fa.bias[l] = m->b[l];
+        fa.zmax = (float)z_max;
+        fa.dt = (float)dt;
+        fa.L = column_levels();
+        fa.dT = dtemp;
+        fa.dq = dhumid;
+        fa.add = (flags & SHT_ADD) ? 1 : 0;
+        fa.nfallback = m->nfallback;
+        fa.err = m->err;
+        mlp_fused_kernel<<<(ncol + 127) / 128, F_THREADS, F_SMEM, s>>>(m->wmap[0], m->wmap[1], m->wmap[2], m->wmap[3],
+                                                                       fa);
+        e = cudaGetLastError();
     }
     if (e == cudaSuccess && nfallback) {
         e = cudaMemcpyAsync(nfallback, m->nfallback, 4, cudaMemcpyDeviceToHost, s);

@@ -214,3 +214,27 @@ def test_emulator_chunks_beyond_capacity(sp, trained):
     assert nf == parts[0][2] + parts[1][2]
     assert torch.equal(dT, torch.cat([parts[0][0], parts[1][0]], dim=1))
     assert torch.equal(dq, torch.cat([parts[0][1], parts[1][1]], dim=1))
+
+
+def test_fused_emulator_matches_unfused(sp, trained):
+    """The one-kernel parameterization (gather, four tcgen05 layers, output) against the
+    emulator run as separate launches (sht_mlp_infer on the gathered columns), for
+    in-range columns, with the tendencies accumulated (add=True) onto nonzero fields."""
+    import torch
+    em = trained[0]
+    n = 3000                                             # ragged last tile of 128 columns
+    T, q, u, v, ps = (a.cuda() for a in (torch.tensor(np.ascontiguousarray(c.T if c.ndim == 2 else c))
+                                         for c in CO.synthetic_columns(n, seed=7)))
+    base_T = torch.randn((8, n), device="cuda")
+    base_q = torch.randn((8, n), device="cuda") * 1e-6
+    dT, dq = base_T.clone(), base_q.clone()
+    nf = em.parameterization_(dT, dq, T, q, u, v, ps, z_max=1e9, add=True)
+    assert nf == 0
+    x = sp.columns_as_rows(T, q, u, v, ps)
+    y = em.infer(x)
+    torch.cuda.synchronize()
+    refT = base_T + y[:, :8].T
+    refq = base_q + y[:, 8:].T
+    torch.testing.assert_close(dT, refT, rtol=1e-5, atol=1e-9)
+    torch.testing.assert_close(dq, refq, rtol=1e-5, atol=1e-12)
+    assert em.device_status() == 0
