@@ -328,11 +328,12 @@ SHT_API int sht_mlp_infer(sht_mlp* m, const float* x, float* y, int B, void* str
  * 33..63 zero, 256 otherwise; b [out]); set = 1 uploads, 0 downloads, 2 downloads the
  * gradients of the last backward pass (synchronises) */
 SHT_API int sht_mlp_params(sht_mlp* m, int layer, float* w, float* b, int set);
-/* The emulator as a parameterization: gathers the columns of layer-major fields
- * (x[k ld + ij]), runs the network, and writes its tendencies for columns whose every
- * normalised input lies within z_max of the training mean, the plain parameterizations'
- * (sht_column_physics, dt) otherwise; *nfallback (if not NULL; synchronises) counts the
- * latter. flags: SHT_ADD. Any ncol: columns beyond the batch capacity run in chunks. */
+/* The emulator as a parameterization, one fused kernel launch: gathers the columns of
+ * layer-major fields (x[k ld + ij]), runs the network, and writes its tendencies for
+ * columns whose every normalised input lies within z_max of the training mean, the plain
+ * parameterizations' (sht_column_physics, dt) otherwise; *nfallback (if not NULL;
+ * synchronises) counts the latter. flags: SHT_ADD. Any ncol (not bound by the batch
+ * capacity, which sizes training and sht_mlp_infer only). */
 SHT_API int sht_column_emulate(sht_mlp* m, const float* temp, const float* humid, const float* u, const float* v,
                                const float* surface_pressure, int64_t ld, int ncol, double dt, double z_max,
                                float* dtemp, float* dhumid, unsigned flags, int32_t* nfallback, void* stream);
