@@ -10,8 +10,8 @@ Reports the headline precision (the fastest Legendre arithmetic whose round trip
 stays within 1e-5 relative error of the FP64 oracle) and every variant, the
 roofline of the dominant kernel, an end-to-end number through the public API with
 host buffers (coefficients in page-locked host memory, copied in and out inside the
-transforms, overlapped with the work over chunks of 16 layers), clocks sampled during
-the timed region, and the CPU baseline.
+transforms, overlapped with the work over chunks of 16 layers; consecutive steps
+pipelined), clocks sampled during the timed region, and the CPU baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -528,30 +528,37 @@ def run_ours(args):
     clocks = clk.summary()
     value = world * args.steps / secs
 
-    # end to end through the public API with host buffers: the coefficients go in from
-    # page-locked host memory and come back to it inside the transforms (sht_synthesize_host /
-    # sht_analyze_host), one round trip per chunk of 16 layers so that the copy in of the
-    # next chunk and the copy out of the previous one overlap the work of the current one;
-    # S.host_wait() makes the step end after its last copy to the host
-    host_out = torch.empty((LAYERS, spec.nlm), dtype=torch.complex64).pin_memory()
+    # end to end through the public API with host buffers: every step copies its 64 layers
+    # of coefficients in from page-locked host memory and its results back into it, inside
+    # the transforms (sht_synthesize_host / sht_analyze_host), one round trip per chunk of
+    # 16 layers so that the copy in of the next chunk and the copy out of the previous one
+    # overlap the work of the current one. Steps are pipelined like a stream of requests
+    # (results alternate between two host buffers): the copies of step i + 1 overlap the
+    # tail of step i, and the timed region ends after the last step's last copy to the host
+    # (S.host_wait() before the end event).
+    host_outs = [torch.empty((LAYERS, spec.nlm), dtype=torch.complex64).pin_memory() for _ in range(2)]
     E2E_CHUNK = 16
     S.set_host_chunk(E2E_CHUNK)
+    e2e_state = {"step": 0}
 
     def e2e_step():
+        host_out = host_outs[e2e_state["step"] % 2]
+        e2e_state["step"] += 1
         for k0 in range(0, LAYERS, E2E_CHUNK):
             f = st.Field(field.data[k0:k0 + E2E_CHUNK], S.grid)
             st.transform_(f, st.LowerTriangularArray(host_c[k0:k0 + E2E_CHUNK], spec), S)
             st.transform_(st.LowerTriangularArray(host_out[k0:k0 + E2E_CHUNK], spec), f, S)
-        S.host_wait()
 
     for _ in range(args.warmup):
         e2e_step()
+    S.host_wait()
     torch.cuda.synchronize()
     barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
         e2e_step()
+    S.host_wait()
     e1.record()
     torch.cuda.synchronize()
     barrier(world)
