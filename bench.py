@@ -343,7 +343,7 @@ def run_column_emulator(args):
     import speedytransforms as st
     device = torch.device("cuda", 0)
     ncol = st.OctahedralGaussianGrid(48).npoints
-    ntrain, batch, epochs = 96 * ncol, 4096, 4
+    ntrain, batch, epochs = 96 * ncol, 4096, args.train_epochs
 
     def rows(cols):
         T, q, u, v, ps = cols
@@ -618,6 +618,7 @@ def main():
                          "column-emulator: the MLP parameterization at T63")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W + K round trips of one precision (default bf16x3), for profilers")
+    ap.add_argument("--train-epochs", type=int, default=4, help="column-emulator: training epochs")
     ap.add_argument("--ref-sample-layers", type=int, default=16)
     ap.add_argument("--ref-seconds", type=float, default=90.0,
                     help="reference arm: CPU seconds for all steps (sets the layers per step)")
