@@ -25,7 +25,7 @@ def setup(T, nh, K, precision="fp32", chunk=None):
     return S, spec, grid, coeffs
 
 
-@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3", "fp16x3", "bf16x5"])
 def test_synthesize_analyze_host_match_device(precision):
     K = 20
     S, spec, grid, coeffs = setup(63, 48, K, precision, chunk=8)      # chunks 8, 8, 4
