@@ -133,6 +133,16 @@ def barrier(world):
         dist.barrier()
 
 
+def broadcast_choice(obj, world):
+    """Rank 0's value on every rank (the headline precision: all ranks time the same one)."""
+    if world == 1:
+        return obj
+    import torch.distributed as dist
+    box = [obj]
+    dist.broadcast_object_list(box, src=0)
+    return box[0]
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -515,11 +525,7 @@ def run_ours(args):
           and variants[p].get("rel_err_synthesis", 0.0) <= ERR_BAR]
     ok = ok or list(transforms)
     head = max(ok, key=lambda p: variants[p].get("round_trips_per_s", 0.0))
-    if world > 1:
-        import torch.distributed as dist
-        obj = [head]
-        dist.broadcast_object_list(obj, src=0)
-        head = obj[0]
+    head = broadcast_choice(head, world)
     S = transforms[head]
 
     # the timed region proper
