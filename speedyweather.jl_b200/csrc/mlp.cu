@@ -276,17 +276,42 @@ cudaError_t gemm_attributes() {
     return e;
 }
 
+// Tensor maps of one network's buffers, reused across steps (encoding them costs host
+// time on every product otherwise); keyed by base, rows, columns and pitch
+struct MapCache {
+    struct Entry {
+        const void* base;
+        int64_t rows, cols, ld;
+        CUtensorMap map;
+    };
+    std::vector<Entry> e;
+};
+bool cached_map(MapCache* c, CUtensorMap* out, const void* base, int64_t rows, int64_t cols, int64_t ld) {
+    if (!c) return make_map(out, base, rows, cols, ld);
+    for (const auto& x : c->e)
+        if (x.base == base && x.rows == rows && x.cols == cols && x.ld == ld) {
+            *out = x.map;
+            return true;
+        }
+    if (c->e.size() >= 64) c->e.clear();
+    MapCache::Entry x{base, rows, cols, ld, {}};
+    if (!make_map(&x.map, base, rows, cols, ld)) return false;
+    c->e.push_back(x);
+    *out = x.map;
+    return true;
+}
+
 // C = A B with A [M][K] (a_mn = 0: stored [M][lda], K contiguous; 1: stored [K][lda],
 // M contiguous) and B [K][N] (b_mn = 0: stored [N][ldb]; 1: stored [K][ldb]).
 // ksplit > 1 (EPI_F32 only) splits K over grid z; slice z writes its partial product to
 // g.out_f32 + z g.split_stride, which the caller reduces.
 cudaError_t gemm(const __nv_bfloat16* A, int64_t lda, int a_mn, const __nv_bfloat16* B, int64_t ldb, int b_mn,
-                 GemmArgs g, cudaStream_t s, int ksplit = 1, int* nz_out = nullptr) {
+                 GemmArgs g, cudaStream_t s, int ksplit = 1, int* nz_out = nullptr, MapCache* cache = nullptr) {
     if (g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaSuccess;
     if ((lda * 2) % 16 || (ldb * 2) % 16) return cudaErrorInvalidValue;   // TMA row pitch
     CUtensorMap ma, mb;
-    const bool ok_a = a_mn ? make_map(&ma, A, g.K, g.M, lda) : make_map(&ma, A, g.M, g.K, lda);
-    const bool ok_b = b_mn ? make_map(&mb, B, g.K, g.N, ldb) : make_map(&mb, B, g.N, g.K, ldb);
+    const bool ok_a = a_mn ? cached_map(cache, &ma, A, g.K, g.M, lda) : cached_map(cache, &ma, A, g.M, g.K, lda);
+    const bool ok_b = b_mn ? cached_map(cache, &mb, B, g.K, g.N, ldb) : cached_map(cache, &mb, B, g.N, g.K, ldb);
     if (!ok_a || !ok_b) return cudaErrorInvalidValue;
     const cudaError_t ea = gemm_attributes();
     if (ea != cudaSuccess) return ea;
@@ -345,40 +370,51 @@ __global__ void output_grad_kernel(const float* __restrict__ Y, const float* __r
     for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
 }
-// db[n] = sum_b dZ[b][n] in two deterministic passes: partial[p][n] over rows
-// [256 p, 256 p + 256), then the partials in order
-constexpr int BIAS_ROWS = 256;
-__global__ void bias_partial_kernel(const __nv_bfloat16* __restrict__ dZ, int B, int N, int64_t ld,
-                                    float* __restrict__ partial) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    const int p = blockIdx.y;
-    if (n >= N) return;
-    float s = 0.f;
-    const int b1 = min(B, (p + 1) * BIAS_ROWS);
-    for (int b = p * BIAS_ROWS; b < b1; ++b) s += __bfloat162float(dZ[(int64_t)b * ld + n]);
-    partial[(int64_t)p * N + n] = s;
+// db[n] = sum_b dZ[b][n], deterministic in one pass: a block sums 32 columns, warp w the
+// rows w, w + 8, ... (lanes over consecutive columns: coalesced), then warp 0 adds the 8
+// partial sums in order
+__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dZ, int B, int N, int64_t ld,
+                                 float* __restrict__ db) {
+    __shared__ float part[8][32];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int n = blockIdx.x * 32 + lane;
+    float acc = 0.f;
+    if (n < N)
+        for (int b = warp; b < B; b += 8) acc += __bfloat162float(dZ[(int64_t)b * ld + n]);
+    part[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0 && n < N) {
+        float t = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) t += part[w][lane];
+        db[n] = t;
+    }
 }
-__global__ void bias_final_kernel(const float* __restrict__ partial, int P, int N, float* __restrict__ db) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    float s = 0.f;
-    for (int p = 0; p < P; ++p) s += partial[(int64_t)p * N + n];
-    db[n] = s;
-}
-// Adam (FP32 master, bias-corrected), then the BF16 copy
-__global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ grad, float* __restrict__ m,
-                            float* __restrict__ v, __nv_bfloat16* __restrict__ wb, int64_t n, float lr, float b1,
-                            float b2, float c1, float c2, float eps) {
+// Adam over all parameter tensors in one launch (per tensor: master, gradient, moments,
+// optional BF16 copy, length); thread i updates element i of the concatenation
+struct AdamSet {
+    float* w[8];
+    const float* g[8];
+    float* m[8];
+    float* v[8];
+    __nv_bfloat16* wb[8];
+    int64_t end[8];      // cumulative lengths
+    int count;
+};
+__global__ void adam_multi_kernel(const AdamSet set, float lr, float b1, float b2, float c1, float c2, float eps) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float g = grad[i];
-    const float mi = b1 * m[i] + (1.f - b1) * g;
-    const float vi = b2 * v[i] + (1.f - b2) * g * g;
-    m[i] = mi;
-    v[i] = vi;
-    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
-    w[i] = wi;
-    if (wb) wb[i] = __float2bfloat16_rn(wi);
+    if (i >= set.end[set.count - 1]) return;
+    int t = 0;
+    while (i >= set.end[t]) ++t;
+    const int64_t j = i - (t ? set.end[t - 1] : 0);
+    const float g = set.g[t][j];
+    const float mi = b1 * set.m[t][j] + (1.f - b1) * g;
+    const float vi = b2 * set.v[t][j] + (1.f - b2) * g * g;
+    set.m[t][j] = mi;
+    set.v[t][j] = vi;
+    const float wi = set.w[t][j] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    set.w[t][j] = wi;
+    if (set.wb[t]) set.wb[t][j] = __float2bfloat16_rn(wi);
 }
 // y[b][c] = Y[b][c] std[c] + mean[c]
 __global__ void denormalize_kernel(const float* __restrict__ Y, int B, int nout, const float* __restrict__ mean,
@@ -680,8 +716,8 @@ struct sht_mlp {
     float *xm = nullptr, *xs = nullptr, *ym = nullptr, *ys = nullptr;   // normalisation
     float* loss = nullptr;
     CUtensorMap wmap[NLAYER];                       // TMA maps of the BF16 weights (fused emulator kernel)
+    MapCache maps;                                  // TMA maps of the layer-by-layer products
     int* nfallback = nullptr;
-    float* partial = nullptr;                       // [cap / 256][hidden] bias-gradient partial sums
     static constexpr int MAX_SPLIT = 32;
     float* splitbuf = nullptr;                      // [MAX_SPLIT][256][256] split-K partial weight gradients
     int32_t* err = nullptr;
@@ -719,7 +755,7 @@ void release(sht_mlp* m) {
         for (void* q : ps)
             if (q) cudaFree(q);
     }
-    void* ps[] = {m->X0, m->Y, m->dY, m->xm, m->xs, m->ym, m->ys, m->loss, m->nfallback, m->partial, m->splitbuf,
+    void* ps[] = {m->X0, m->Y, m->dY, m->xm, m->xs, m->ym, m->ys, m->loss, m->nfallback, m->splitbuf,
                   m->err};
     for (void* q : ps)
         if (q) cudaFree(q);
@@ -747,7 +783,7 @@ cudaError_t forward(sht_mlp* m, int B, bool keep, cudaStream_t s) {
         g.out_bf16 = m->A[l];
         g.ld_bf16 = m->hidden;
         g.bias = m->b[l];
-        e = gemm(in, ld_in, 0, m->Wb[l], m->fan_in[l], 0, g, s);
+        e = gemm(in, ld_in, 0, m->Wb[l], m->fan_in[l], 0, g, s, 1, nullptr, &m->maps);
         in = m->A[l];
         ld_in = m->hidden;
     }
@@ -756,7 +792,7 @@ cudaError_t forward(sht_mlp* m, int B, bool keep, cudaStream_t s) {
     g.out_f32 = m->Y;
     g.ld_f32 = m->nout;
     g.bias = m->b[3];
-    return gemm(in, ld_in, 0, m->Wb[3], m->hidden, 0, g, s);
+    return gemm(in, ld_in, 0, m->Wb[3], m->hidden, 0, g, s, 1, nullptr, &m->maps);
 }
 }  // namespace
 
@@ -809,7 +845,6 @@ int sht_mlp_create(int batch_capacity, uint64_t seed, int device, sht_mlp** out)
     if (e == cudaSuccess) e = alloc(&m->ys, m->nout);
     if (e == cudaSuccess) e = alloc(&m->loss, 1);
     if (e == cudaSuccess) e = alloc(&m->nfallback, 1);
-    if (e == cudaSuccess) e = alloc(&m->partial, (cap / BIAS_ROWS + 1) * m->hidden);
     if (e == cudaSuccess) e = alloc(&m->splitbuf, (size_t)sht_mlp::MAX_SPLIT * m->hidden * m->hidden);
     if (e == cudaSuccess && (e = alloc(&m->err, 1)) == cudaSuccess) e = cudaMemset(m->err, 0, 4);
     if (e == cudaSuccess) {          // identity normalisation until set
@@ -875,13 +910,11 @@ cudaError_t backward(sht_mlp* m, const float* x, const float* y, int B, cudaStre
         gw.ld_f32 = fi;
         gw.split_stride = (int64_t)fo * fi;
         int nz = 1;
-        e = gemm(dz, ld_dz, 1, act[l], ld_act[l], 1, gw, s, ksplit, &nz);
+        e = gemm(dz, ld_dz, 1, act[l], ld_act[l], 1, gw, s, ksplit, &nz, &m->maps);
         if (e != cudaSuccess) break;
         split_reduce_kernel<<<(unsigned)(((int64_t)fo * fi + 255) / 256), 256, 0, s>>>(m->splitbuf, nz, fo, fi,
                                                                                         m->dW[l], fi);
-        const int P = (B + BIAS_ROWS - 1) / BIAS_ROWS;
-        bias_partial_kernel<<<dim3((fo + 127) / 128, P), 128, 0, s>>>(dz, B, fo, ld_dz, m->partial);
-        bias_final_kernel<<<(fo + 127) / 128, 128, 0, s>>>(m->partial, P, fo, m->db[l]);
+        bias_grad_kernel<<<(fo + 31) / 32, 256, 0, s>>>(dz, B, fo, ld_dz, m->db[l]);
         if (l == 0) break;
         // dZ[l-1] = (dz W[l]) * GELU'(Z[l-1])   (A = dz K-major, B = W[l] [fo][fi] MN-major)
         GemmArgs gd = args(m, B, fi, fo, EPI_GELU_BWD);
@@ -889,7 +922,7 @@ cudaError_t backward(sht_mlp* m, const float* x, const float* y, int B, cudaStre
         gd.ld_bf16 = m->hidden;
         gd.zin = m->Z[l - 1];
         gd.ld_z = m->hidden;
-        e = gemm(dz, ld_dz, 0, m->Wb[l], fi, 1, gd, s);
+        e = gemm(dz, ld_dz, 0, m->Wb[l], fi, 1, gd, s, 1, nullptr, &m->maps);
         dz = m->dZ[l - 1];
         ld_dz = m->hidden;
     }
@@ -916,12 +949,26 @@ int sht_mlp_train_step(sht_mlp* m, const float* x, const float* y, int B, float 
     ++m->step;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - std::pow(b1, (float)m->step), c2 = 1.f - std::pow(b2, (float)m->step);
-    for (int l = 0; l < 4 && e == cudaSuccess; ++l) {
-        const int64_t nw = (int64_t)m->fan_out[l] * m->fan_in[l];
-        adam_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(m->W[l], m->dW[l], m->mW[l], m->vW[l], m->Wb[l], nw, lr,
-                                                                 b1, b2, c1, c2, 1e-8f);
-        adam_kernel<<<(m->fan_out[l] + 255) / 256, 256, 0, s>>>(m->b[l], m->db[l], m->mb[l], m->vb[l], nullptr,
-                                                                m->fan_out[l], lr, b1, b2, c1, c2, 1e-8f);
+    if (e == cudaSuccess) {
+        AdamSet set{};
+        int64_t total = 0;
+        for (int l = 0; l < 4; ++l) {
+            const int64_t nw = (int64_t)m->fan_out[l] * m->fan_in[l];
+            set.w[2 * l] = m->W[l];
+            set.g[2 * l] = m->dW[l];
+            set.m[2 * l] = m->mW[l];
+            set.v[2 * l] = m->vW[l];
+            set.wb[2 * l] = m->Wb[l];
+            set.end[2 * l] = (total += nw);
+            set.w[2 * l + 1] = m->b[l];
+            set.g[2 * l + 1] = m->db[l];
+            set.m[2 * l + 1] = m->mb[l];
+            set.v[2 * l + 1] = m->vb[l];
+            set.wb[2 * l + 1] = nullptr;
+            set.end[2 * l + 1] = (total += m->fan_out[l]);
+        }
+        set.count = 8;
+        adam_multi_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(set, lr, b1, b2, c1, c2, 1e-8f);
         e = cudaGetLastError();
     }
     return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_mlp_train_step");
