@@ -783,14 +783,16 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kern
 
 // Persistent grouped launch over the (ring, chunk) items of many transforms: CTA b
 // takes the items b, b + gridDim.x, ... of the batch's list (task, ring, chunk).
+// (one instantiation per direction: a single body per kernel keeps the registers in bounds)
+template <bool SYN>
 __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_grouped_kernel(const FftView* __restrict__ views,
                                                                                  const GroupItem* __restrict__ items,
-                                                                                 int nitems, int synthesis) {
+                                                                                 int nitems) {
     extern __shared__ float2 sm[];
     for (int ix = blockIdx.x; ix < nitems; ix += gridDim.x) {
         const GroupItem it = items[ix];
         __syncthreads();                  // the previous item is done with shared memory
-        if (synthesis)
+        if (SYN)
             fft_synthesis_body(views[it.task], it.a, it.b, sm);
         else
             fft_analysis_body(views[it.task], it.a, it.b, sm);
@@ -822,7 +824,10 @@ cudaError_t launch_fft_grouped(const FftView* views, const GroupItem* items, int
                                int grid, cudaStream_t s) {
     if (nitems == 0) return cudaSuccess;
     const int g = std::max(1, std::min(nitems, grid));
-    fft_grouped_kernel<<<g, kFftThreads, smem, s>>>(views, items, nitems, synthesis ? 1 : 0);
+    if (synthesis)
+        fft_grouped_kernel<true><<<g, kFftThreads, smem, s>>>(views, items, nitems);
+    else
+        fft_grouped_kernel<false><<<g, kFftThreads, smem, s>>>(views, items, nitems);
     return cudaGetLastError();
 }
 
@@ -864,7 +869,10 @@ cudaError_t fft_set_smem(int bytes) {
     std::lock_guard<std::mutex> lock(mu);
     if (bytes <= current[dev]) return cudaSuccess;
     e = cudaFuncSetAttribute(fft_analysis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(fft_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fft_grouped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fft_grouped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(fft_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) current[dev] = bytes;
     return e;
