@@ -420,6 +420,54 @@ def run_column_emulator(args):
     return 0
 
 
+def run_dycore_step(args):
+    """The transforms of one time step of the primitive-equation wet model at T63 on the
+    octahedral grid with nlat = 96 and 8 layers, in the reference's order (transform.jl:117-191,
+    tendencies.jl:161-214): gradient, UV_from_vordiv, syntheses of 2, 4L+1 and 2L layers, the
+    analysis of 9L+1 layers, curl, divergences and a Laplacian. Timed as eager library calls
+    and as one CUDA graph replayed per step. Prints one JSON line (not the headline metric)."""
+    import torch
+    import speedytransforms as st
+    res = {}
+    for prec in ("fp32", "bf16x3"):
+        step = st.DycoreStep(T=63, nlat_half=48, L=8, precision=prec)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+        def timed(fn):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            ev[0].record()
+            for _ in range(args.steps):
+                fn()
+            ev[1].record()
+            torch.cuda.synchronize()
+            return ev[0].elapsed_time(ev[1]) / args.steps
+
+        t_eager = timed(step)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            step()
+        torch.cuda.current_stream().wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            step()
+        t_graph = timed(graph.replay)
+        res[prec] = {"eager_ms": t_eager, "graph_ms": t_graph}
+        del graph
+    best = min(res, key=lambda p: res[p]["graph_ms"])
+    line = {"metric": "dycore-step transforms/s (T63 octahedral nlat 96, 8 layers, primitive wet model)",
+            "value": 1e3 / res[best]["graph_ms"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res[best]["graph_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": best, "data": "synthetic",
+            "config": {"workload": "one time step's transforms and spectral operators, CUDA graph",
+                       "library_calls_per_step": 11},
+            "ms_per_step_by_precision": res}
+    print(json.dumps(line))
+    return 0
+
+
 def profile_run(args):
     """W + K round trips of one precision at the benchmark workload and nothing else:
     the command ncu wraps for the launch list and the per-kernel captures."""
@@ -619,9 +667,10 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3", "fp16x3", "bf16x5"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="t511", choices=["t511", "mixed-batch", "column-emulator"],
+    ap.add_argument("--workload", default="t511", choices=["t511", "mixed-batch", "column-emulator", "dycore-step"],
                     help="t511: the headline benchmark; mixed-batch: the grouped-launch comparison; "
-                         "column-emulator: the MLP parameterization at T63")
+                         "column-emulator: the MLP parameterization at T63; dycore-step: one time step's "
+                         "transforms at T63 L8, eager and as a CUDA graph")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W + K round trips of one precision (default bf16x3), for profilers")
     ap.add_argument("--train-epochs", type=int, default=4, help="column-emulator: training epochs")
@@ -638,6 +687,8 @@ def main():
         return run_mixed_batch(args)
     if args.workload == "column-emulator":
         return run_column_emulator(args)
+    if args.workload == "dycore-step":
+        return run_dycore_step(args)
     return run_ours(args)
 
 

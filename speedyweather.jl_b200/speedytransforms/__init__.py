@@ -50,3 +50,4 @@ from .core import (  # noqa: F401
 )
 
 __version__ = "0.1.0"
+from .dycore_step import DycoreStep  # noqa: F401,E402
