@@ -143,7 +143,10 @@ __device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P]) 
 // radices of earlier stages. Output in natural order after the last stage. A work
 // item is one butterfly position b for CT layers: its index arithmetic and twiddles
 // are shared by the layers. The first stage (Ns = 1) has no twiddles.
-constexpr int CT = 2;
+#ifndef SHT_FFT_CT
+#define SHT_FFT_CT 4
+#endif
+constexpr int CT = SHT_FFT_CT;
 
 template <int P, bool INV, bool FIRST>
 __device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y, int n, int ldx, int C, int Ns,

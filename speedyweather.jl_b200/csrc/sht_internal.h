@@ -12,7 +12,10 @@
 namespace sht {
 
 constexpr int kMaxFactors = 24;      // radices per ring FFT (n <= 2^24)
-constexpr int kPrimeGroup = 8;       // outputs per thread of a prime FFT stage
+#ifndef SHT_PRIME_GROUP
+#define SHT_PRIME_GROUP 8
+#endif
+constexpr int kPrimeGroup = SHT_PRIME_GROUP;   // outputs per thread of a prime FFT stage
 
 // Launch shape of the FFT kernels: threads per CTA, CTAs per SM, and the shared
 // memory one CTA may use (which bounds the layers per CTA).
