@@ -301,7 +301,7 @@ class SpectralTransform:
         self.norm_sphere = 2 * math.sqrt(math.pi)
 
     def __del__(self):
-        if getattr(self, "_plan", None) is not None:
+        if getattr(self, "_plan", None) is not None and lib is not None:   # lib is None at interpreter exit
             lib.sht_plan_destroy(self._plan)
             self._plan = None
 
@@ -370,7 +370,7 @@ class MatrixSpectralTransform:
         return int(v.value)
 
     def __del__(self):
-        if getattr(self, "_m", None) is not None:
+        if getattr(self, "_m", None) is not None and lib is not None:
             lib.sht_matrix_destroy(self._m)
             self._m = None
 
@@ -439,7 +439,7 @@ class Batch:
         return int(v.value)
 
     def __del__(self):
-        if getattr(self, "_b", None) is not None:
+        if getattr(self, "_b", None) is not None and lib is not None:
             lib.sht_batch_destroy(self._b)
             self._b = None
 
