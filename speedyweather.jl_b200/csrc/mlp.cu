@@ -12,16 +12,21 @@
 // -> 256 -> 256 -> 256 (GELU) -> 16 outputs (dT/dt and dq/dt on 8 layers, normalised).
 // Weights in BF16 (FP32 master copies and Adam moments for training), FP32 accumulate.
 //
-// Every matrix product is one launch of a tcgen05 GEMM: C[M x N] = A[M x K] B[K x N],
-// A and B row-major BF16 in global memory, each either K-major (K contiguous) or
-// MN-major (M or N contiguous), loaded by 2-D TMA boxes of 64 x 64 with 128-byte
-// swizzle into a ring of shared-memory stages; one elected thread issues
-// tcgen05.mma kind::f16 (M = 128, N <= 256) into a TMEM accumulator; four warps read it
-// (tcgen05.ld) and apply a fused epilogue:
+// Training and sht_mlp_infer: every matrix product is one launch of a tcgen05 GEMM,
+// C[M x N] = A[M x K] B[K x N], A and B row-major BF16 in global memory, each either
+// K-major (K contiguous) or MN-major (M or N contiguous), loaded by 2-D TMA boxes of
+// 64 x 64 with 128-byte swizzle into a ring of shared-memory stages; one elected thread
+// issues tcgen05.mma kind::f16 (M = 128, N <= 256) into a TMEM accumulator; eight warps
+// read it (tcgen05.ld), transpose 32 x 32 blocks through shared memory for coalesced
+// stores and apply a fused epilogue:
 //   forward hidden layer   Z = A W^T + b, A' = bf16(GELU(Z)) (Z kept for the backward)
 //   forward output layer   Y = A W^T + b
 //   backward data          dZ = bf16((dZ' W) * GELU'(Z))
-//   backward weights       dW = dZ^T A (FP32)
+//   backward weights       dW = dZ^T A (FP32; the batch split over the grid, partial
+//                          products reduced in a fixed order)
+// The emulator as a parameterization (sht_column_emulate) is one fused kernel instead:
+// gather, the four layers with the activations kept in shared memory, output and plain
+// physics fallback (mlp_fused_kernel below).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>

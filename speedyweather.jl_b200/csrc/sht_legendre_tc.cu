@@ -32,8 +32,9 @@
 //
 // A persistent CTA per SM computes a sequence of 128 x N output tiles (N <= 256 real
 // columns): warp 0 issues the copies, warp 1 owns the tensor memory (two
-// accumulators) and one of its threads issues the MMAs, warps 2-5 read the
-// accumulator (tcgen05.ld) and store while the next tile accumulates. Every wait is
+// accumulators) and one of its threads issues the MMAs, warps 2-9 (two per TMEM lane
+// quarter) read the accumulator (tcgen05.ld) and store while the next tile
+// accumulates. The CTA's items are read into shared memory once. Every wait is
 // bounded by a one-second global-timer limit; on expiry the CTA records an error
 // in the plan's status word, drains, frees its tensor memory and returns.
 #include <cuda.h>
