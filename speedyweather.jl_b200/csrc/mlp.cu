@@ -444,11 +444,12 @@ __global__ void to_bf16_kernel(const float* __restrict__ w, __nv_bfloat16* __res
 // activation leaves the SM. The output layer is de-normalised and written into the
 // tendency fields; columns outside the training range get the plain physics instead.
 constexpr int NLC = SHT_COLUMN_LAYERS;
-constexpr int F_THREADS = 320;                       // producer warp, MMA warp, 8 epilogue warps
+constexpr int F_THREADS = 576;                       // producer warp, MMA warp, 16 epilogue warps
+constexpr int F_EPI = F_THREADS - 64;                // epilogue threads
 constexpr int F_STAGES = 3;
 constexpr int F_W_STAGE = 4 * G_BOX_BYTES;           // 256 rows x 64 features
 constexpr int F_ACT_BYTES = 4 * 2 * G_BOX_BYTES;     // 128 rows x 256 features (4 blocks of 16 KB)
-constexpr int F_TAIL = 128 + 256;                    // barriers, inside flags [2][128]
+constexpr int F_TAIL = 128 + 512;                    // barriers, inside flags [4][128]
 constexpr int F_SMEM = 1024 + F_ACT_BYTES + F_STAGES * F_W_STAGE + F_TAIL;
 
 struct FusedArgs {
@@ -502,7 +503,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
             mbar_init(&empty_bar[s], 1);
         }
         mbar_init(acc_bar, 1);
-        mbar_init(act_bar, 256);
+        mbar_init(act_bar, F_EPI);
         mbar_init(mma_bar, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -569,17 +570,17 @@ __global__ void __launch_bounds__(F_THREADS, 1)
         if (!mbar_wait(mma_bar, 0)) atomicExch(a.err, 25);
     } else if (warp >= 2) {
         const int et = threadIdx.x - 64;
-        {   // ---- gather: row r, features [32 kh, 32 kh + 32), normalised, BF16 into the tile
+        {   // ---- gather: row r, features [16 kh, 16 kh + 16), normalised, BF16 into the tile
             const int r = et & 127, kh = et >> 7;
             const int64_t ij = col0 + r;
             bool in = true;
-            uint32_t pk[16];
+            uint32_t pk[8];
 #pragma unroll
-            for (int i = 0; i < 32; i += 2) {
+            for (int i = 0; i < 16; i += 2) {
                 float z2[2];
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    const int c = 32 * kh + i + e;
+                    const int c = 16 * kh + i + e;
                     float z = 0.f;
                     if (c < 4 * NLC + 1 && r < nrow) {
                         float x;
@@ -597,15 +598,17 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                 pk[i / 2] = pack_bf16x2(z2[0], z2[1]);
             }
 #pragma unroll
-            for (int c8 = 0; c8 < 4; ++c8)
-                *reinterpret_cast<uint4*>(act + act_off(r, 32 * kh + 8 * c8)) =
+            for (int c8 = 0; c8 < 2; ++c8)
+                *reinterpret_cast<uint4*>(act + act_off(r, 16 * kh + 8 * c8)) =
                     make_uint4(pk[4 * c8], pk[4 * c8 + 1], pk[4 * c8 + 2], pk[4 * c8 + 3]);
             // features 64 .. 255 of layer 1 stay unread (its K is 64)
             inside[kh * 128 + r] = in ? 1 : 0;
             fence_proxy_async();
             mbar_arrive(act_bar);
-            asm volatile("bar.sync 1, 256;" ::: "memory");   // the flags, among the 8 epilogue warps
+            asm volatile("bar.sync 1, %0;" ::"n"(F_EPI) : "memory");   // the flags, among the epilogue warps
         }
+        // warp w reads TMEM lanes 32 (w % 4) .. + 31; the four warps of a lane quarter take
+        // every fourth 32-column chunk
         const int quarter = warp % 4, half = (warp - 2) / 4;
         const int r = quarter * 32 + lane;
         const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
@@ -619,7 +622,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
             }
             tc_fence_after();
             const float* bias = a.bias[l];
-            for (int c0 = 32 * half; c0 < 256; c0 += 64) {
+            for (int c0 = 32 * half; c0 < 256; c0 += 128) {
                 float v[32];
                 tmem_ld32(taddr + c0, v);
                 uint32_t pk[16];
@@ -649,7 +652,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
             if (r < nrow) {
                 const int64_t ij = col0 + r;
                 float dT[NLC], dq[NLC];
-                if (inside[r] && inside[128 + r]) {
+                if (inside[r] && inside[128 + r] && inside[256 + r] && inside[384 + r]) {
 #pragma unroll
                     for (int k = 0; k < NLC; ++k) {
                         const float y0 = v[k] + a.bias[3][k], y1 = v[NLC + k] + a.bias[3][NLC + k];
