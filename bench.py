@@ -618,6 +618,21 @@ def run_ours(args):
     barrier(world)
     e2e_secs = reduce_max(e0.elapsed_time(e1) / 1e3, world, device)
     nbytes = host_c.numel() * 8
+    # the host link on this box: one plain copy of the step's coefficients each way (context
+    # for e2e, which the two copies bound)
+    dev_c = torch.empty_like(host_c, device=device)
+    link = {}
+    for name, fn in (("h2d_ms", lambda: dev_c.copy_(host_c, non_blocking=True)),
+                     ("d2h_ms", lambda: host_outs[0].copy_(dev_c, non_blocking=True))):
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(3):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        link[name] = e0.elapsed_time(e1) / 3
+    del dev_c
 
     # roofline of the dominant kernel (per-kernel CUDA events on the launching stream)
     stage_ms = time_stages(S, lt, field, out, reps=max(5, args.steps // 2))
@@ -643,7 +658,7 @@ def run_ours(args):
             "config": config({"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                               "precision": head}),
             "e2e": {"value": world * args.steps / e2e_secs, "unit": UNIT, "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": nbytes},
+                    "d2h_bytes_per_step": nbytes, "plain_copy_ms": link},
             "roofline": roofline, "clocks": clocks, "gpu_launches": launches_per_rt * args.steps,
             "variants": variants}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

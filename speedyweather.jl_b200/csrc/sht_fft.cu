@@ -788,7 +788,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kern
 // takes the items b, b + gridDim.x, ... of the batch's list (task, ring, chunk).
 // (one instantiation per direction: a single body per kernel keeps the registers in bounds)
 template <bool SYN>
-__global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_grouped_kernel(const FftView* __restrict__ views,
+__global__ void __launch_bounds__(kFftGroupThreads, kFftCtasPerSm) fft_grouped_kernel(const FftView* __restrict__ views,
                                                                                  const GroupItem* __restrict__ items,
                                                                                  int nitems) {
     extern __shared__ float2 sm[];
@@ -828,9 +828,9 @@ cudaError_t launch_fft_grouped(const FftView* views, const GroupItem* items, int
     if (nitems == 0) return cudaSuccess;
     const int g = std::max(1, std::min(nitems, grid));
     if (synthesis)
-        fft_grouped_kernel<true><<<g, kFftThreads, smem, s>>>(views, items, nitems);
+        fft_grouped_kernel<true><<<g, kFftGroupThreads, smem, s>>>(views, items, nitems);
     else
-        fft_grouped_kernel<false><<<g, kFftThreads, smem, s>>>(views, items, nitems);
+        fft_grouped_kernel<false><<<g, kFftGroupThreads, smem, s>>>(views, items, nitems);
     return cudaGetLastError();
 }
 

@@ -20,12 +20,13 @@ constexpr int kPrimeGroup = SHT_PRIME_GROUP;   // outputs per thread of a prime 
 // Launch shape of the FFT kernels: threads per CTA, CTAs per SM, and the shared
 // memory one CTA may use (which bounds the layers per CTA).
 #ifndef SHT_FFT_THREADS
-#define SHT_FFT_THREADS 256
+#define SHT_FFT_THREADS 384        // 2 x 12 warps per SM in 80 registers (256: 119 registers, 16 warps)
 #endif
 #ifndef SHT_FFT_CTAS_PER_SM
 #define SHT_FFT_CTAS_PER_SM 2
 #endif
 constexpr int kFftThreads = SHT_FFT_THREADS;
+constexpr int kFftGroupThreads = 256;   // grouped (batch) launches: their item loop needs more registers
 constexpr int kFftCtasPerSm = SHT_FFT_CTAS_PER_SM;
 constexpr int kFftSmemBudget = (227 * 1024) / SHT_FFT_CTAS_PER_SM - 1024;
 
