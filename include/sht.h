@@ -292,7 +292,7 @@ SHT_API int sht_matrix_destroy(sht_matrix* m);
  * sht_column_physics: large-scale condensation + simplified Betts-Miller convection
  * tendencies of ncol columns (replaces the column loops of
  * SpeedyWeather/src/parameterizations/large_scale_condensation.jl:55-178 and
- * SpeedyWeather/src/parameterizations/convection.jl:33-253, in the driver's order,
+ * SpeedyWeather/src/parameterizations/convection.jl:33-253, in the order of the column loop of
  * SpeedyWeather/src/parameterizations/tendencies.jl:3-90). Fields layer-major like a
  * Field{npoints, nlayers}: temp[k ld + ij] [K], humid [kg/kg], surface_pressure[ij] [Pa];
  * outputs dtemp [K/s], dhumid [kg/kg/s] (SHT_ADD accumulates, as the reference does).

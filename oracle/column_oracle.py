@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY: a numpy restatement of the reference's column
 parameterizations, used as the checker of the CUDA column-physics kernel and as the
-teacher and judge of the MLP emulator's tests. Never imported by the product path.
+teacher and the reference of the MLP emulator's tests. Never imported by the product path.
 
 Follows, per column (vectorised over columns; FP64 by default, FP32 with dtype=float32):
 * ImplicitCondensation: SpeedyWeather/src/parameterizations/large_scale_condensation.jl:55-178

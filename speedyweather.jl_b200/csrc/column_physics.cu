@@ -3,7 +3,7 @@
 //
 // Replaces the column loops of SpeedyWeather/src/parameterizations/large_scale_condensation.jl:55-178
 // (ImplicitCondensation) and SpeedyWeather/src/parameterizations/convection.jl:33-253
-// (BettsMillerConvection, pseudo_adiabat!), called per grid point ij by the driver
+// (BettsMillerConvection, pseudo_adiabat!), called per grid point ij by the column loop of
 // SpeedyWeather/src/parameterizations/tendencies.jl:3-90 in the order condensation,
 // convection (SpeedyWeather/src/models/primitive_wet.jl:123-136); both read the same
 // state and add to the tendencies. These are the fallback of the MLP emulator and the

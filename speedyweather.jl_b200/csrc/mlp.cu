@@ -5,7 +5,7 @@
 // large_scale_condensation.jl:55-178, convection.jl:33-253), called per column through
 // the parameterization interface parameterization!(ij, vars, p, model)
 // (SpeedyWeather/src/parameterizations/tendencies.jl:3-90). The plain parameterizations
-// (column_physics.cu) label the training columns, judge the emulator, and replace it
+// (column_physics.cu) label the training columns, evaluate the emulator, and replace it
 // for columns outside the range of its training inputs.
 //
 // Network: 33 inputs (T, q, u, v on 8 layers and log surface pressure, normalised)

@@ -152,7 +152,7 @@ def test_emulator_parameterization_and_fallback(sp, trained):
     gT, gq = dT.cpu().numpy(), dq.cpu().numpy()
     np.testing.assert_array_equal(gT[:, : n // 4], pT.cpu().numpy()[:, : n // 4])
     np.testing.assert_array_equal(gq[:, : n // 4], pq.cpu().numpy()[:, : n // 4])
-    # in range: the emulator, judged by the plain physics (relative RMS over the columns)
+    # in range: the emulator, compared with the plain physics (relative RMS over the columns)
     ref = pT.cpu().numpy()[:, n // 4:]
     err = np.linalg.norm(gT[:, n // 4:] - ref) / np.linalg.norm(ref)
     print("emulator vs plain physics (relative L2 of dT/dt):", err, "fallbacks:", nf)
