@@ -210,29 +210,60 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
         return;
     }
     if (SYN) {
+        // Lane r holds ring r's 32 columns (16 complex k) of a chunk. A warp transposes the
+        // chunk at float4 granularity with three shfl_xor stages so that one store instruction
+        // writes 4 rings x 128 contiguous bytes (whole L2 lines) instead of 16 bytes of each of
+        // 32 rings: after the exchange, float4 slot s of lane x is ring 4 s + (x & 3), complex
+        // pair x >> 2.
         const int j = t.j0[m] + tile * 128 + r;
         const bool valid = good && j < t.nh && m <= t.rings[j].mt;
         float2* dst = valid ? four + ((t.rings[j].gofs + m) * 2 + par) * K : nullptr;
+        const unsigned vm = __ballot_sync(0xffffffffu, valid);
+        const int lane = r % 32;
+        float2* rowp[8];
+#pragma unroll
+        for (int s = 0; s < 8; ++s)
+            rowp[s] = reinterpret_cast<float2*>(
+                __shfl_sync(0xffffffffu, reinterpret_cast<uintptr_t>(dst), 4 * s + (lane & 3)));
         for (int c0 = cb; c0 < nt_cols; c0 += 64) {
             float v[32];
             tmem_ld32(taddr + c0, v);
-            if (!valid) continue;
+            if (vm == 0) continue;
+            const int k0 = (ct * 256 + c0) / 2;
             if (t.fp16) {
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
-                    const float f = t.kscale_syn[min((ct * 256 + c0) / 2 + q, K - 1)].x;
+                    const float f = t.kscale_syn[min(k0 + q, K - 1)].x;
                     v[2 * q] = v[2 * q] * mscale * f;
                     v[2 * q + 1] = v[2 * q + 1] * mscale * f;
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 16; q += 2) {
-                const int k = (ct * 256 + c0) / 2 + q;
+            for (int i = 0; i < 3; ++i) {        // swap register bit i of the float4 index with lane bit 2 + i
+                const bool upper = (lane >> (2 + i)) & 1;
+#pragma unroll
+                for (int f = 0; f < 8; ++f) {
+                    if ((f >> i) & 1) continue;
+                    const int f1 = f | (1 << i);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const float send = upper ? v[4 * f + c] : v[4 * f1 + c];
+                        const float recv = __shfl_xor_sync(0xffffffffu, send, 1 << (2 + i));
+                        if (upper) v[4 * f + c] = recv;
+                        else v[4 * f1 + c] = recv;
+                    }
+                }
+            }
+            const int k = k0 + 2 * (lane >> 2);
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                if (!((vm >> (4 * s + (lane & 3))) & 1)) continue;
+                float2* d = rowp[s];
                 if (k + 1 < K && (K % 2) == 0) {    // 16-byte aligned: row * K and k even
-                    *reinterpret_cast<float4*>(dst + k) = make_float4(v[2 * q], v[2 * q + 1], v[2 * q + 2], v[2 * q + 3]);
+                    *reinterpret_cast<float4*>(d + k) = make_float4(v[4 * s], v[4 * s + 1], v[4 * s + 2], v[4 * s + 3]);
                 } else {
-                    if (k < K) dst[k] = make_float2(v[2 * q], v[2 * q + 1]);
-                    if (k + 1 < K) dst[k + 1] = make_float2(v[2 * q + 2], v[2 * q + 3]);
+                    if (k < K) d[k] = make_float2(v[4 * s], v[4 * s + 1]);
+                    if (k + 1 < K) d[k + 1] = make_float2(v[4 * s + 2], v[4 * s + 3]);
                 }
             }
         }
