@@ -500,35 +500,73 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // coefficients [k][lm] complex FP32 -> per (m, p, kt, piece) K-major SWIZZLE_128B tiles
 // of nmax rows (columns c = 2k + re/im) x 64 parity rows (128 B).
 
-// Synthesis data image. One thread per (order m, 64-row block kt, 8-row chunk ib8,
-// layer k): it loads the 16 packed coefficients of its 8 rows (both parities, four
-// 16-byte loads; the 8 threads of a layer read 512 consecutive bytes) and writes, per
-// parity, real/imaginary column and piece, one whole 16-byte chunk of the swizzled
-// K-major tile: rows 8 ib8 .. 8 ib8 + 7 of column c = 2 k + ri. CTA: 8 chunks x 32
-// layers. Rows past the order's last coefficient are written as zeros.
+// Synthesis data image. CTA: order m, 64-row block kt, 32 layers. The CTA first stages
+// the 128 packed coefficients (both parities) of each of its layers in shared memory
+// with asynchronous copies, a warp copying 512 consecutive bytes per instruction (16-byte
+// copies where the run is 16-byte aligned, 8-byte copies otherwise; coefficients past the
+// order's last one staged as zeros). Then one thread per (8-row chunk ib8, layer k) reads
+// its 16 coefficients from shared memory and writes, per parity, real/imaginary column
+// and piece, one whole 16-byte chunk of the swizzled K-major tile: rows 8 ib8 .. 8 ib8 + 7
+// of column c = 2 k + ri (the 8 threads of a layer fill the tile row's 128 bytes).
+// Shared layout: per layer 8 runs of 16 coefficients, 144 bytes apart, so that the 8
+// threads of a layer read distinct banks.
+constexpr int IMG_RUN = 144;                 // bytes per staged run of 16 coefficients (128 + 16 pad)
+constexpr int IMG_LAYER = 8 * IMG_RUN;       // bytes per staged layer
+
+__device__ __forceinline__ void cp_async_16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_8(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+
 template <int NPB, bool F16>
 __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const float2* __restrict__ coeffs,
                                                         int64_t ldc, int K) {
+    __shared__ __align__(16) uint8_t stage[32 * IMG_LAYER];
     const int m = blockIdx.x;
     const int kt = blockIdx.y;
     if (kt >= t.nkt[m]) return;
-    const int ib8 = threadIdx.x & 7;
-    const int k = blockIdx.z * 32 + (threadIdx.x >> 3);
-    if (k >= K) return;
-    const int lmrem = t.lmax - m - 2 * BLK * kt - 16 * ib8;   // packed coefficients left from this chunk
-    const float2* src = coeffs + (int64_t)k * ldc + t.lm_off[m] + 2 * BLK * kt + 16 * ib8;
-    float2 v[16];
-    const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && lmrem >= 16;
-    if (vec) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const float4 f = __ldg(reinterpret_cast<const float4*>(src) + q);
-            v[2 * q] = make_float2(f.x, f.y);
-            v[2 * q + 1] = make_float2(f.z, f.w);
+    const int kbase = blockIdx.z * 32;
+    const int lmrem = t.lmax - m - 2 * BLK * kt;             // packed coefficients left from this block
+    const float2* src0 = coeffs + t.lm_off[m] + 2 * BLK * kt;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(stage);
+    const bool al16 = ((reinterpret_cast<uintptr_t>(src0) & 15) == 0) && ((ldc & 1) == 0);
+    if (al16) {
+        // 32 layers x 64 pairs of coefficients: lanes take consecutive pairs of a layer
+        for (int w = threadIdx.x; w < 32 * 64; w += 256) {
+            const int kl = w >> 6, e2 = w & 63, e = 2 * e2;
+            const uint32_t soff = kl * IMG_LAYER + (e >> 4) * IMG_RUN + (e & 15) * 8;
+            if (kbase + kl < K && e + 1 < lmrem)
+                cp_async_16(sbase + soff, src0 + (int64_t)(kbase + kl) * ldc + e);
+            else
+                *reinterpret_cast<float4*>(stage + soff) =
+                    make_float4(0.f, 0.f, 0.f, 0.f);   // past the order (or K), or half of the last pair below
+            if (kbase + kl < K && e < lmrem && e + 1 >= lmrem)
+                *reinterpret_cast<float2*>(stage + soff) = src0[(int64_t)(kbase + kl) * ldc + e];
         }
     } else {
+        for (int w = threadIdx.x; w < 32 * 128; w += 256) {
+            const int kl = w >> 7, e = w & 127;
+            const uint32_t soff = kl * IMG_LAYER + (e >> 4) * IMG_RUN + (e & 15) * 8;
+            if (kbase + kl < K && e < lmrem)
+                cp_async_8(sbase + soff, src0 + (int64_t)(kbase + kl) * ldc + e);
+            else
+                *reinterpret_cast<float2*>(stage + soff) = make_float2(0.f, 0.f);
+        }
+    }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    const int ib8 = threadIdx.x & 7;
+    const int k = kbase + (threadIdx.x >> 3);
+    if (k >= K) return;
+    float2 v[16];
+    const float4* run = reinterpret_cast<const float4*>(stage + (threadIdx.x >> 3) * IMG_LAYER + ib8 * IMG_RUN);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = q < lmrem ? __ldg(src + q) : make_float2(0.f, 0.f);
+    for (int q = 0; q < 8; ++q) {
+        const float4 f = run[q];
+        v[2 * q] = make_float2(f.x, f.y);
+        v[2 * q + 1] = make_float2(f.z, f.w);
     }
     if (F16) {
         const float sc = t.kscale_syn[k].y;
