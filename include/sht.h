@@ -352,6 +352,17 @@ SHT_API int sht_bf16_gemm(const void* A, int64_t lda, int a_mn, const void* B, i
  * No counterpart in the reference (its kernels have no waits). */
 SHT_API int sht_device_status(sht_plan* plan, int32_t* status);
 
+/* Failure-detection check of those waits (no counterpart in the reference): launches one
+ * CTA on the plan's device and stream whose thread waits, through the same bounded
+ * mbarrier wait as the tensor-core kernels, first for a phase it completes itself, then
+ * for a phase that nothing completes, each with a limit of limit_us microseconds
+ * (1 .. 1000000). The second wait expires as designed; the kernel stores
+ * SHT_STATUS_DIAG_EXPIRED in the plan's status word (SHT_STATUS_DIAG_FAILED if either wait
+ * misbehaved) and returns, leaving the context usable. Read it with sht_device_status. */
+#define SHT_STATUS_DIAG_EXPIRED 9
+#define SHT_STATUS_DIAG_FAILED 10
+SHT_API int sht_diag_wait_expiry(sht_plan* plan, int32_t limit_us, void* stream);
+
 /* Message of the last failed call on this thread ("" if none). */
 SHT_API const char* sht_last_error(void);
 

@@ -177,6 +177,8 @@ cudaError_t tc_matrix_create(TcMatrix** out, int precision, const float* const a
 void tc_matrix_destroy(TcMatrix* x);
 cudaError_t tc_matrix_apply(const TcMatrix* x, int which, const float* in, int64_t ld, float* out, int64_t ldo, int K,
                             const float* row_scale, int32_t* d_err, cudaStream_t st);
+// failure-detection check of the bounded mbarrier waits (sht_legendre_tc.cu)
+cudaError_t launch_wait_probe(int32_t* err, uint64_t limit_ns, cudaStream_t s);
 cudaError_t launch_column_physics(const float* temp, const float* humid, const float* ps, int64_t ld, int ncol,
                                   float dt, float* dtemp, float* dhumid, int64_t ldo, bool add, cudaStream_t s);
 cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, float mul);

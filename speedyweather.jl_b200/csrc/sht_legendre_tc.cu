@@ -685,7 +685,29 @@ int smem_for(int npa, int npb, int nt_cols, int& stages) {
     return 1024 + stages * stage_bytes + 256 + TC_ITEM_BYTES;
 }
 
+// Failure-detection check of the bounded waits. One thread waits through the routine of
+// the kernels' pipelines (mbar_wait_for), first for an mbarrier phase it completes itself
+// (must succeed), then for one that nothing completes (must expire after limit_ns). It
+// stores SHT_STATUS_DIAG_EXPIRED when both behave, SHT_STATUS_DIAG_FAILED otherwise, and
+// returns: nothing is in flight and the context stays usable.
+__global__ void wait_probe_kernel(int32_t* err, uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar[2];
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_arrive(&bar[0]);
+    const bool done = mbar_wait_for(&bar[0], 0, limit_ns);
+    const bool expired = !mbar_wait_for(&bar[1], 0, limit_ns);
+    atomicExch(err, done && expired ? SHT_STATUS_DIAG_EXPIRED : SHT_STATUS_DIAG_FAILED);
+}
+
 }  // namespace
+
+cudaError_t launch_wait_probe(int32_t* err, uint64_t limit_ns, cudaStream_t s) {
+    wait_probe_kernel<<<1, 32, 0, s>>>(err, limit_ns);
+    return cudaGetLastError();
+}
 
 int tc_supported() { return get_encoder() != nullptr; }
 

@@ -689,6 +689,15 @@ int sht_device_status(sht_plan* plan, int32_t* status) {
     return SHT_OK;
 }
 
+int sht_diag_wait_expiry(sht_plan* plan, int32_t limit_us, void* stream) {
+    if (!plan) return fail(SHT_EINVAL, "sht_diag_wait_expiry: NULL plan");
+    if (limit_us < 1 || limit_us > 1000000)
+        return fail(SHT_EINVAL, "sht_diag_wait_expiry: limit_us = %d outside 1 .. 1000000", (int)limit_us);
+    DeviceGuard g(plan->p.device);
+    const cudaError_t e = launch_wait_probe(plan->p.d_err, (uint64_t)limit_us * 1000u, (cudaStream_t)stream);
+    return e == cudaSuccess ? SHT_OK : cuda_fail(e, "sht_diag_wait_expiry");
+}
+
 int sht_legendre_synthesis(sht_plan* plan, const void* coeffs, int64_t ldc, int K, void* stream) {
     int rc;
     if ((rc = check_call(plan, K, "sht_legendre_synthesis")) != SHT_OK) return rc;

@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "libsht.so")
 
 SHT_OK, SHT_EINVAL, SHT_ECUDA, SHT_ENOMEM, SHT_EUNSUPPORTED = 0, 1, 2, 3, 4
+SHT_STATUS_DIAG_EXPIRED, SHT_STATUS_DIAG_FAILED = 9, 10     # device status words of sht_diag_wait_expiry
 GRID_FULL_GAUSSIAN, GRID_OCTAHEDRAL_GAUSSIAN = 0, 1
 PREC_FP32, PREC_BF16X3, PREC_FP16X3, PREC_BF16X5 = 0, 1, 2, 3
 SHORTCUTS = {"linear": 0, "quadratic": 1, "cubic": 2, "linquadcoslat2": 3, "lincubcoslat": 4}
@@ -61,6 +62,7 @@ SIGNATURES = {
     "sht_laplace": (C.c_int, [_P, _P, _P, _I64, C.c_int, C.c_uint, C.c_double, _P]),
     "sht_gradient": (C.c_int, [_P, _P, _P, _P, _I64, C.c_int, C.c_double, _P]),
     "sht_device_status": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "sht_diag_wait_expiry": (C.c_int, [_P, C.c_int32, _P]),
     "sht_analyze_static_scratch": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
     "sht_plan_autotune": (C.c_int, [_P, C.c_int, _P, C.POINTER(C.c_int32)]),
     "sht_synthesize_adjoint": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),

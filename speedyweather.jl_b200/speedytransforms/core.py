@@ -315,6 +315,13 @@ class SpectralTransform:
         check(lib.sht_device_status(self._plan, C.byref(v)))
         return int(v.value)
 
+    def diag_wait_expiry(self, limit_us: int = 20000):
+        """Failure-detection check of the tensor-core kernels' bounded waits: one thread
+        on the plan's device waits, through the same routine, for an mbarrier phase that
+        nothing completes and gives up after ``limit_us`` microseconds, storing
+        ``SHT_STATUS_DIAG_EXPIRED`` (9) in the status word that ``device_status`` reads."""
+        check(lib.sht_diag_wait_expiry(self._plan, int(limit_us), _stream_ptr(self.device)))
+
     def host_wait(self):
         """Make the current stream wait for the copies of host-memory coefficients that
         earlier transforms issued (synchronise it afterwards to read them)."""

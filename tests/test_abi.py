@@ -63,6 +63,7 @@ def test_argument_checks_of_the_newer_entry_points(lib):
     assert f.sht_analyze_host(None, None, 0, None, 0, 1, 0, None) == E
     assert f.sht_plan_set_host_chunk(None, 8) == E
     assert f.sht_host_wait(None, None) == E
+    assert f.sht_diag_wait_expiry(None, 1000, None) == E
     assert f.sht_column_physics(None, None, None, 10, 10, 7, 1200.0, None, None, 0, None) == E   # nlayers
     assert b"nlayers" in f.sht_last_error()
     assert f.sht_column_physics(None, None, None, 5, 10, 8, 1200.0, None, None, 0, None) == E    # ld < ncol
