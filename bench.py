@@ -468,6 +468,93 @@ def run_dycore_step(args):
     return 0
 
 
+def run_operators(args):
+    """The spectral operators (spectral_gradients.jl) at the T511 x 64 size, one degree more
+    than the order (lmax = mmax + 1, as the reference's vector operators need): curl,
+    divergence, UV_from_vordiv, Laplacian, inverse Laplacian and gradient, each timed alone
+    with CUDA events over `--steps` calls, three sets of 67 MB fields taken in turn so that
+    consecutive calls share no data through the L2.
+    Prints one JSON line (not the headline metric) with each kernel's achieved GB/s of
+    algorithmic bytes (fields read + written) against the measured HBM copy bandwidth."""
+    import torch
+    import speedytransforms as st
+    K = LAYERS
+    spec = st.Spectrum(T + 1, T)
+    S = st.SpectralTransform(spec, st.OctahedralGaussianGrid(NLAT_HALF), nlayers=K, precision="fp32")
+    g = torch.Generator(device="cuda").manual_seed(4)
+
+    def field():
+        return st.LowerTriangularArray(torch.randn((K, spec.nlm), dtype=torch.complex64, device="cuda",
+                                                   generator=g), spec)
+    # three sets of (u, v, out1, out2) used in turn: consecutive calls share no data (810 MB)
+    sets = [tuple(field() for _ in range(4)) for _ in range(3)]
+    turn = [0]
+
+    def nxt():
+        turn[0] = (turn[0] + 1) % len(sets)
+        return sets[turn[0]]
+    nbytes = K * spec.nlm * 8
+
+    def curl():
+        u, v, o1, _ = nxt()
+        st.curl_(o1, u, v, S, radius=6.371e6)
+
+    def div():
+        u, v, o1, _ = nxt()
+        st.divergence_(o1, u, v, S, radius=6.371e6)
+
+    def uv():
+        u, v, o1, o2 = nxt()
+        st.UV_from_vordiv_(o1, o2, u, v, S, radius=6.371e6)
+
+    def lap(inverse):
+        u, _, o1, _ = nxt()
+        st.laplace_(o1, u, S, inverse=inverse, radius=6.371e6)
+
+    def grad():
+        u, _, o1, o2 = nxt()
+        st.gradient_(o1, o2, u, S, radius=6.371e6)
+    ops = {   # name: (call, fields read + written per call)
+        "curl": (curl, 3),
+        "divergence": (div, 3),
+        "UV_from_vordiv": (uv, 4),
+        "laplace": (lambda: lap(False), 2),
+        "inverse_laplace": (lambda: lap(True), 2),
+        "gradient": (grad, 3),
+    }
+    peaks, peak_src = measured_peaks()
+    peak = peaks.get("hbm_gbs")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    res = {}
+    for name, (fn, nf) in ops.items():
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(args.steps):
+            fn()
+        ev[1].record()
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1]) / args.steps
+        gbs = nf * nbytes / (ms * 1e-3) / 1e9
+        res[name] = {"ms": ms, "algorithmic_bytes": nf * nbytes, "achieved_gbs": gbs,
+                     "frac_of_measured_hbm": (gbs / peak) if peak else None}
+    assert S.device_status() == 0
+    total = sum(r["ms"] for r in res.values())
+    line = {"metric": "spectral operators at T511 x 64 layers (lmax = mmax + 1 = 513), achieved HBM GB/s",
+            "value": sum(r["algorithmic_bytes"] for r in res.values()) / (total * 1e-3) / 1e9, "unit": "GB/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "peak_hbm_gbs": peak, "peak_source": peak_src,
+            "config": {"workload": "curl, divergence, UV_from_vordiv, laplace, inverse laplace, gradient "
+                                   "on [64][nlm] complex FP32 fields, each call timed alone",
+                       "nlm": spec.nlm, "layers": K, "field_mb": nbytes / 1e6,
+                       "l2": "three sets of fields in turn, so consecutive calls share no data (810 MB)"},
+            "by_operator": res}
+    print(json.dumps(line))
+    return 0
+
+
 def profile_run(args):
     """W + K round trips of one precision at the benchmark workload and nothing else:
     the command ncu wraps for the launch list and the per-kernel captures."""
@@ -682,10 +769,12 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3", "fp16x3", "bf16x5"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="t511", choices=["t511", "mixed-batch", "column-emulator", "dycore-step"],
+    ap.add_argument("--workload", default="t511",
+                    choices=["t511", "mixed-batch", "column-emulator", "dycore-step", "operators"],
                     help="t511: the headline benchmark; mixed-batch: the grouped-launch comparison; "
                          "column-emulator: the MLP parameterization at T63; dycore-step: one time step's "
-                         "transforms at T63 L8, eager and as a CUDA graph")
+                         "transforms at T63 L8, eager and as a CUDA graph; operators: the spectral "
+                         "operators at T511 x 64, GB/s per kernel")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W + K round trips of one precision (default bf16x3), for profilers")
     ap.add_argument("--train-epochs", type=int, default=4, help="column-emulator: training epochs")
@@ -704,6 +793,8 @@ def main():
         return run_column_emulator(args)
     if args.workload == "dycore-step":
         return run_dycore_step(args)
+    if args.workload == "operators":
+        return run_operators(args)
     return run_ours(args)
 
 
