@@ -708,9 +708,23 @@ def run_ours(args):
     # the host link on this box: one plain copy of the step's coefficients each way (context
     # for e2e, which the two copies bound)
     dev_c = torch.empty_like(host_c, device=device)
+    dev_c2 = torch.empty_like(host_c, device=device)
+    side = (torch.cuda.Stream(device=device), torch.cuda.Stream(device=device))
+
+    def duplex():   # one copy each way at once, on two streams: the bound of a pipelined step
+        cur = torch.cuda.current_stream()
+        for sx in side:
+            sx.wait_stream(cur)
+        with torch.cuda.stream(side[0]):
+            dev_c.copy_(host_c, non_blocking=True)
+        with torch.cuda.stream(side[1]):
+            host_outs[1].copy_(dev_c2, non_blocking=True)
+        for sx in side:
+            cur.wait_stream(sx)
     link = {}
     for name, fn in (("h2d_ms", lambda: dev_c.copy_(host_c, non_blocking=True)),
-                     ("d2h_ms", lambda: host_outs[0].copy_(dev_c, non_blocking=True))):
+                     ("d2h_ms", lambda: host_outs[0].copy_(dev_c, non_blocking=True)),
+                     ("both_ms", duplex)):
         fn()
         torch.cuda.synchronize()
         e0.record()
@@ -719,7 +733,7 @@ def run_ours(args):
         e1.record()
         torch.cuda.synchronize()
         link[name] = e0.elapsed_time(e1) / 3
-    del dev_c
+    del dev_c, dev_c2
 
     # roofline of the dominant kernel (per-kernel CUDA events on the launching stream)
     stage_ms = time_stages(S, lt, field, out, reps=max(5, args.steps // 2))
