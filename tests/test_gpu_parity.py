@@ -266,6 +266,48 @@ def test_laplace_gradient_match_oracle(st):
     assert O.rel_err(np_of(dx), rx) < TOL and O.rel_err(np_of(dy), ry) < TOL
 
 
+def test_operators_layer_groups_match_oracle(st):
+    """At T255 with 22 layers the operator kernels run several layers per thread (8 for
+    curl/divergence, the Laplacians and the gradient, 4 for UV_from_vordiv) with a partial
+    last group (22 = 8 + 8 + 6 = 5 x 4 + 2); outputs NaN-prefilled, every flag."""
+    import torch
+    K = 22
+    S, So = setup(st, 255, "octa", K, one_more=True)
+    sp = So.spectrum
+    rng = np.random.default_rng(8)
+    mk = lambda: rng.standard_normal((sp.nlm, K)) + 1j * rng.standard_normal((sp.nlm, K))
+    u, v, o = mk(), mk(), mk()
+
+    def nan_lta():
+        return st.LowerTriangularArray(torch.full((K, sp.nlm), complex(np.nan, np.nan), dtype=torch.complex64,
+                                                  device="cuda"), S.spectrum)
+    for fn, ofn in ((st.divergence_, O.divergence), (st.curl_, O.curl)):
+        for flip, add in ((False, False), (True, True)):
+            out = to_lta(st, S, o) if add else nan_lta()
+            fn(out, to_lta(st, S, u), to_lta(st, S, v), S, flipsign=flip, add=add, radius=6.371e6)
+            ref = ofn(sp, u, v, flipsign=flip, add=add, out=o.copy(), radius=6.371e6)
+            assert O.rel_err(np_of(out), ref) < TOL
+    U, V = nan_lta(), nan_lta()
+    st.UV_from_vordiv_(U, V, to_lta(st, S, u), to_lta(st, S, v), S, radius=6.371e6)
+    Ur, Vr = O.UV_from_vordiv(sp, u, v, radius=6.371e6)
+    assert O.rel_err(np_of(U), Ur) < TOL and O.rel_err(np_of(V), Vr) < TOL
+    U, V = nan_lta(), nan_lta()
+    st.UV_from_vor_(U, V, to_lta(st, S, u), S)
+    Ur, Vr = O.UV_from_vordiv(sp, u)
+    assert O.rel_err(np_of(U), Ur) < TOL and O.rel_err(np_of(V), Vr) < TOL
+    for inv in (False, True):
+        for flip, add in ((False, False), (True, True)):
+            out = to_lta(st, S, o) if add else nan_lta()
+            st.laplace_(out, to_lta(st, S, u), S, inverse=inv, flipsign=flip, add=add, radius=2.0)
+            ref = O.laplace(sp, u, inverse=inv, flipsign=flip, add=add, out=o.copy(), radius=2.0)
+            assert O.rel_err(np_of(out), ref) < TOL
+    dx, dy = nan_lta(), nan_lta()
+    st.gradient_(dx, dy, to_lta(st, S, u), S, radius=3.0)
+    rx, ry = O.gradient(sp, u, radius=3.0)
+    assert O.rel_err(np_of(dx), rx) < TOL and O.rel_err(np_of(dy), ry) < TOL
+    assert S.device_status() == 0
+
+
 def test_vordiv_uv_roundtrip_gpu(st):
     # spectral_gradients.jl tests :201-252 on the GPU path (Float32: rtol = 80 sqrt(eps(Float32)))
     import torch
