@@ -212,9 +212,9 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
     if (SYN) {
         // Lane r holds ring r's 32 columns (16 complex k) of a chunk. A warp transposes the
         // chunk at float4 granularity with three shfl_xor stages so that one store instruction
-        // writes 4 rings x 128 contiguous bytes (whole L2 lines) instead of 16 bytes of each of
-        // 32 rings: after the exchange, float4 slot s of lane x is ring 4 s + (x & 3), complex
-        // pair x >> 2.
+        // writes 4 rings x 128 contiguous bytes (whole 128-byte lines when K is a multiple of
+        // 16) instead of 16 bytes of each of 32 rings: after the exchange, float4 slot s of
+        // lane x is ring 4 s + (x & 3), complex pair x >> 2.
         const int j = t.j0[m] + tile * 128 + r;
         const bool valid = good && j < t.nh && m <= t.rings[j].mt;
         float2* dst = valid ? four + ((t.rings[j].gofs + m) * 2 + par) * K : nullptr;
