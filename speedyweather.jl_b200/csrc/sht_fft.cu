@@ -725,7 +725,52 @@ __device__ void fft_synthesis_body(const FftView& v, int ring, int chunk, float2
     const int nhalf = n / 2;   // highest source frequency
     // layer fastest across the lanes (a warp reads whole runs of C layers of a scratch
     // row), four items per thread in flight: the scratch reads are the latency
-    const int tot = C * (nhalf + 1);
+    if (svec) {
+        // staged rows, C even: an item is a pair of layers (16-byte loads of the row's run;
+        // one index division and one weight per two layers), same arithmetic per value
+        const int C2 = C / 2;
+        const int tot2 = C2 * (nhalf + 1);
+        const Div dC2 = mkdiv(C2);
+        const float4* Y4 = reinterpret_cast<const float4*>(Y);
+        for (int w0 = threadIdx.x; w0 < tot2; w0 += 4 * blockDim.x) {
+            float4 e[4], o[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int w = w0 + u * blockDim.x;
+                const int m = quo(w, dC2);
+                const int c2 = w - m * C2;
+                e[u] = o[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (w < tot2 && m <= rd.mt) {
+                    e[u] = Y4[m * C + c2];          // Y[2 m C + 2 c2], two layers
+                    o[u] = Y4[m * C + C2 + c2];     // Y[(2 m + 1) C + 2 c2]
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int w = w0 + u * blockDim.x;
+                if (w >= tot2) break;
+                const int m = quo(w, dC2);
+                const int c = 2 * (w - m * C2);
+                const float scale = syn_weight(rd, m, adj, unscale);
+                const bool selfconj = (m == 0) || (2 * m == n);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float2 eh = h ? make_float2(e[u].z, e[u].w) : make_float2(e[u].x, e[u].y);
+                    const float2 oh = h ? make_float2(o[u].z, o[u].w) : make_float2(o[u].x, o[u].y);
+                    const float2 gn = make_float2(__fmul_rn(scale, eh.x + oh.x), __fmul_rn(scale, eh.y + oh.y));
+                    const float2 gs = make_float2(__fmul_rn(scale, eh.x - oh.x), __fmul_rn(scale, eh.y - oh.y));
+                    float2* xr = X + (c + h) * ldx;
+                    if (selfconj) {
+                        xr[m] = make_float2(gn.x, gs.x);
+                    } else {
+                        xr[m] = make_float2(gn.x - gs.y, gn.y + gs.x);
+                        xr[n - m] = make_float2(gn.x + gs.y, gs.x - gn.y);
+                    }
+                }
+            }
+        }
+    }
+    const int tot = svec ? 0 : C * (nhalf + 1);
     const Div dC = mkdiv(C);
     for (int w0 = threadIdx.x; w0 < tot; w0 += 4 * blockDim.x) {
         float2 e[4], o[4];
@@ -736,14 +781,9 @@ __device__ void fft_synthesis_body(const FftView& v, int ring, int chunk, float2
             const int c = w - m * C;
             e[u] = o[u] = make_float2(0.f, 0.f);
             if (w < tot && m <= rd.mt) {
-                if (svec) {
-                    e[u] = Y[2 * m * C + c];
-                    o[u] = Y[(2 * m + 1) * C + c];
-                } else {
-                    const int64_t row = (rd.gofs + m) * 2;
-                    e[u] = four[row * K + k0 + c];
-                    o[u] = four[(row + 1) * K + k0 + c];
-                }
+                const int64_t row = (rd.gofs + m) * 2;
+                e[u] = four[row * K + k0 + c];
+                o[u] = four[(row + 1) * K + k0 + c];
             }
         }
 #pragma unroll
