@@ -537,7 +537,9 @@ __device__ __forceinline__ float syn_weight(const RingDesc& rd, int m, int adjoi
 }
 
 // grid -> Fourier scratch (E/O combinations weighted by the solid angle), one work
-// item (ring, layer chunk) of one transform
+// item (ring, layer chunk) of one transform. IMG: the tensor-core operand-image epilogue
+// is compiled in (the grouped batch launches, FP32 plans only, leave it out).
+template <bool IMG>
 __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2* sm) {
     const RingDesc* __restrict__ rings = v.rings;
     const float2* __restrict__ twiddle = v.twiddle;
@@ -597,7 +599,7 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
     const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G);
     const int adj = v.adjoint, unsc = v.unscale;
     const int nm = rd.mt + 1;
-    if (img.base != nullptr) {
+    if (IMG && img.base != nullptr) {
         // tensor-core operand: E (parity 0) and O (parity 1) split into 16-bit pieces,
         // written into the swizzled MN-major tile of (m, parity, ring block) at ring
         // row j - j0(m); 8 real columns (4 layers) form one 16-byte chunk
@@ -814,7 +816,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_analysis_kerne
                                                                                   const FftView v) {
     extern __shared__ float2 sm[];
     const int2 it = items[blockIdx.x];
-    fft_analysis_body(v, it.x, it.y, sm);
+    fft_analysis_body<true>(v, it.x, it.y, sm);
 }
 
 __global__ void __launch_bounds__(kFftThreads, kFftCtasPerSm) fft_synthesis_kernel(const int2* __restrict__ items,
@@ -838,7 +840,7 @@ __global__ void __launch_bounds__(kFftGroupThreads, kFftCtasPerSm) fft_grouped_k
         if (SYN)
             fft_synthesis_body(views[it.task], it.a, it.b, sm);
         else
-            fft_analysis_body(views[it.task], it.a, it.b, sm);
+            fft_analysis_body<false>(views[it.task], it.a, it.b, sm);
     }
 }
 
