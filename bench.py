@@ -749,6 +749,12 @@ def run_ours(args):
     if "flops" in alg[dom]:
         mult = 3 if head in ("bf16x3", "fp16x3") else 1
         roofline["legendre_tflops"] = alg[dom]["flops"] * mult / (stage_ms[dom] * 1e-3) / 1e12
+    # the whole round trip against HBM: each of Λ (both directions), the grid and the
+    # coefficients read once and written once, at the measured per-GPU round-trip rate
+    rt_bytes = 2 * (4 * alg["_lam_elems"] + S.grid.npoints * LAYERS * 4 + S.spectrum.nlm * LAYERS * 8)
+    rt_gbs = rt_bytes * (value / world) / 1e9
+    roofline["round_trip"] = {"algorithmic_bytes": rt_bytes, "achieved": rt_gbs, "unit": "GB/s",
+                              "frac": rt_gbs / peaks["hbm_gbs"]}
 
     # this library's kernels per round trip: FFT x 2 and Legendre x 2, plus the tensor-core
     # synthesis data image, plus for fp16 the two max-abs passes and their scale kernels
