@@ -246,7 +246,10 @@ __device__ __forceinline__ void prime_block(float (&ar)[GR], float (&ai)[GR], fl
     }
 }
 
-template <bool INV>
+// RAW (first stage of the analysis only): layer c's input is still the raw ring data at
+// X + c ldx (n northern floats, then n southern floats) instead of interleaved complex
+// values; the pass that forms u_b, v_b reads it in place.
+template <bool INV, bool RAW>
 __device__ void stage_prime(float2* __restrict__ X, float2* __restrict__ Y, int n, int ldx, int C, int Ns, int p,
                             const float2* __restrict__ G) {
     const int nb = n / p;
@@ -263,13 +266,26 @@ __device__ void stage_prime(float2* __restrict__ X, float2* __restrict__ Y, int 
         const int b = quo(w, dcols);
         const int col = w - b * cols;
         const int c = quo(col, dnb);
-        const float2* x = X + c * ldx + (col - c * nb);
-        if (b < h) {
-            const int qn = qb[b] * nb;
-            const float2 xq = x[qn], xm = x[n - qn];
-            UV[b * cols + col] = make_float4(xq.x + xm.x, xq.y + xm.y, xq.x - xm.x, xq.y - xm.y);
+        const int i0 = col - c * nb;
+        if (RAW) {
+            const float* raw = reinterpret_cast<const float*>(X + c * ldx);
+            if (b < h) {
+                const int qn = qb[b] * nb;
+                const float2 xq = make_float2(raw[i0 + qn], raw[n + i0 + qn]);
+                const float2 xm = make_float2(raw[i0 + n - qn], raw[2 * n + i0 - qn]);
+                UV[b * cols + col] = make_float4(xq.x + xm.x, xq.y + xm.y, xq.x - xm.x, xq.y - xm.y);
+            } else {
+                X0[col] = make_float2(raw[i0], raw[n + i0]);
+            }
         } else {
-            X0[col] = x[0];
+            const float2* x = X + c * ldx + i0;
+            if (b < h) {
+                const int qn = qb[b] * nb;
+                const float2 xq = x[qn], xm = x[n - qn];
+                UV[b * cols + col] = make_float4(xq.x + xm.x, xq.y + xm.y, xq.x - xm.x, xq.y - xm.y);
+            } else {
+                X0[col] = x[0];
+            }
         }
     }
     __syncthreads();
@@ -330,7 +346,7 @@ __device__ void stage_prime(float2* __restrict__ X, float2* __restrict__ Y, int 
 // Runs all stages; returns the buffer holding the result. G: the ring's prime tables.
 template <bool INV>
 __device__ float2* run_fft(float2* X, float2* Y, int n, int ldx, int C, const RingDesc& rd, const float2* W,
-                           const float2* G) {
+                           const float2* G, bool raw_first = false) {
     int Ns = 1;
     for (int s = 0; s < rd.nfac; ++s) {
         const int p = rd.fac[s];
@@ -339,7 +355,10 @@ __device__ float2* run_fft(float2* X, float2* Y, int n, int ldx, int C, const Ri
                 twiddle_pass<INV>(X, n, ldx, C, Ns, p, W);
                 __syncthreads();
             }
-            stage_prime<INV>(X, Y, n, ldx, C, Ns, p, G);     // result in X
+            if (!INV && raw_first && s == 0)
+                stage_prime<INV, true>(X, Y, n, ldx, C, Ns, p, G);    // result in X
+            else
+                stage_prime<INV, false>(X, Y, n, ldx, C, Ns, p, G);   // result in X
             G += 3 * prime_hpad(p);
             __syncthreads();
             Ns *= p;
@@ -562,9 +581,13 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
     float2* Y = X + C * ldx;
     // Ring values of the C layers land raw in Y (layer c at Y + c ldx: n northern, then
     // n southern floats) by asynchronous copies issued together with the twiddles,
-    // then are interleaved into X. Unaligned layouts take the register path.
+    // then are interleaved into X. When the first stage is a prime p > 8 they land raw
+    // in X instead and that stage reads them in place (no interleave pass). Unaligned
+    // layouts take the register path.
     const bool avec = ((ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(grid) & 15) == 0) &&
                       ((rd.off_north & 3) == 0) && ((rd.off_south & 3) == 0) && ((n & 3) == 0);
+    const bool raw_first = avec && rd.nfac > 0 && rd.fac[0] > 8;
+    float2* const land = raw_first ? X : Y;
     copy_twiddles_async(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
     const int n4 = n >> 2;
     if (avec) {
@@ -575,12 +598,14 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
             const int hs = r >= n4 ? 1 : 0;
             const int i4 = r - hs * n4;
             const float* src = grid + (int64_t)(k0 + c) * ldg + (hs ? rd.off_south : rd.off_north) + 4 * i4;
-            cp_async16(reinterpret_cast<float*>(Y + c * ldx) + hs * n + 4 * i4, src);
+            cp_async16(reinterpret_cast<float*>(land + c * ldx) + hs * n + 4 * i4, src);
         }
     }
     cp_async_wait_all();
     __syncthreads();
-    if (avec) {
+    if (raw_first) {
+        // the prime stage reads the raw layout (visible after the barrier above)
+    } else if (avec) {
         const Div dn4 = mkdiv(n4);
         for (int w = threadIdx.x; w < C * n4; w += blockDim.x) {
             const int c = quo(w, dn4);
@@ -595,8 +620,8 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
     } else {
         load_rings(X, grid, ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn);
     }
-    __syncthreads();
-    const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G);
+    if (!raw_first) __syncthreads();
+    const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G, raw_first);
     const int adj = v.adjoint, unsc = v.unscale;
     const int nm = rd.mt + 1;
     if (IMG && img.base != nullptr) {
