@@ -148,7 +148,9 @@ __device__ __forceinline__ void dft_small(const float2 (&v)[P], float2 (&y)[P]) 
 #endif
 constexpr int CT = SHT_FFT_CT;
 
-template <int P, bool INV, bool FIRST>
+// RAW (FIRST only, analysis): the input of layer c is the raw ring data at X + c ldx
+// (n northern floats, then n southern floats).
+template <int P, bool INV, bool FIRST, bool RAW = false>
 __device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y, int n, int ldx, int C, int Ns,
                             const float2* __restrict__ W) {
     const int nb = n / P;
@@ -171,8 +173,14 @@ __device__ void stage_small(const float2* __restrict__ X, float2* __restrict__ Y
             if (c >= C) break;
             const float2* x = X + c * ldx + b;
             float2 v[P];
+            if (RAW) {
+                const float* raw = reinterpret_cast<const float*>(X + c * ldx) + b;
 #pragma unroll
-            for (int r = 0; r < P; ++r) v[r] = (FIRST || r == 0) ? x[r * nb] : twmul<INV>(x[r * nb], tw[r]);
+                for (int r = 0; r < P; ++r) v[r] = make_float2(raw[r * nb], raw[n + r * nb]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < P; ++r) v[r] = (FIRST || r == 0) ? x[r * nb] : twmul<INV>(x[r * nb], tw[r]);
+            }
             float2 y[P];
             dft_small<P, INV>(v, y);
             float2* yo = Y + c * ldx + (b - k) * P + k;
@@ -363,6 +371,15 @@ __device__ float2* run_fft(float2* X, float2* Y, int n, int ldx, int C, const Ri
             __syncthreads();
             Ns *= p;
             continue;
+        } else if (!INV && raw_first && s == 0) {
+            switch (p) {
+                case 2: stage_small<2, INV, true, true>(X, Y, n, ldx, C, Ns, W); break;
+                case 3: stage_small<3, INV, true, true>(X, Y, n, ldx, C, Ns, W); break;
+                case 4: stage_small<4, INV, true, true>(X, Y, n, ldx, C, Ns, W); break;
+                case 5: stage_small<5, INV, true, true>(X, Y, n, ldx, C, Ns, W); break;
+                case 7: stage_small<7, INV, true, true>(X, Y, n, ldx, C, Ns, W); break;
+                default: stage_small<8, INV, true, true>(X, Y, n, ldx, C, Ns, W); break;
+            }
         } else if (Ns == 1) {
             switch (p) {
                 case 2: stage_small<2, INV, true>(X, Y, n, ldx, C, Ns, W); break;
@@ -581,12 +598,12 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
     float2* Y = X + C * ldx;
     // Ring values of the C layers land raw in Y (layer c at Y + c ldx: n northern, then
     // n southern floats) by asynchronous copies issued together with the twiddles,
-    // then are interleaved into X. When the first stage is a prime p > 8 they land raw
-    // in X instead and that stage reads them in place (no interleave pass). Unaligned
-    // layouts take the register path.
+    // then are interleaved into X. In the aligned case they land raw in X instead and the
+    // first FFT stage reads them in place (no interleave pass). Unaligned layouts take the
+    // register path.
     const bool avec = ((ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(grid) & 15) == 0) &&
                       ((rd.off_north & 3) == 0) && ((rd.off_south & 3) == 0) && ((n & 3) == 0);
-    const bool raw_first = avec && rd.nfac > 0 && rd.fac[0] > 8;
+    const bool raw_first = avec && rd.nfac > 0;
     float2* const land = raw_first ? X : Y;
     copy_twiddles_async(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
     const int n4 = n >> 2;
