@@ -504,16 +504,28 @@ __device__ __forceinline__ void store_rings(float* __restrict__ grid, int64_t ld
         }
     }
 }
-template <bool F16>
-__device__ __forceinline__ uint32_t piece_bits(float& r) {
+
+// The next 16-bit piece (bf16 or fp16, round to nearest) of two reals r0 (low half) and
+// r1 (high half), one paired rounding; the residuals r -= piece are formed only when
+// another piece follows.
+template <bool F16, bool RESIDUAL>
+__device__ __forceinline__ uint32_t piece_bits2(float& r0, float& r1) {
     if (F16) {
-        const __half h = __float2half_rn(r);
-        r -= __half2float(h);
-        return __half_as_ushort(h);
+        const __half2 h = __floats2half2_rn(r0, r1);
+        if (RESIDUAL) {
+            const float2 b = __half22float2(h);
+            r0 -= b.x;
+            r1 -= b.y;
+        }
+        return *reinterpret_cast<const uint32_t*>(&h);
     }
-    const __nv_bfloat16 h = __float2bfloat16_rn(r);
-    r -= __bfloat162float(h);
-    return __bfloat16_as_ushort(h);
+    const __nv_bfloat162 h = __floats2bfloat162_rn(r0, r1);
+    if (RESIDUAL) {
+        const float2 b = __bfloat1622float2(h);
+        r0 -= b.x;
+        r1 -= b.y;
+    }
+    return *reinterpret_cast<const uint32_t*>(&h);
 }
 
 // Writes the 16-bit pieces (bf16 or fp16) of 8 reals as one 16-byte chunk per piece
@@ -527,8 +539,7 @@ __device__ __forceinline__ void put_pieces(uint8_t* dst, int64_t piece_stride, c
         float r0 = v[2 * h], r1 = v[2 * h + 1];
 #pragma unroll
         for (int q = 0; q < NP; ++q) {
-            const uint32_t b0 = piece_bits<F16>(r0);
-            w[q][h] = b0 | (piece_bits<F16>(r1) << 16);
+            w[q][h] = q + 1 < NP ? piece_bits2<F16, true>(r0, r1) : piece_bits2<F16, false>(r0, r1);
         }
     }
 #pragma unroll
