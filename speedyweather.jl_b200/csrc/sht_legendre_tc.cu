@@ -145,6 +145,28 @@ __device__ __forceinline__ uint32_t piece_bits(float& r) {
     r -= __bfloat162float(h);
     return __bfloat16_as_ushort(h);
 }
+// The next pieces of two reals r0 (low half) and r1 (high half) with one paired rounding
+// (the same bits as piece_bits on each); the residuals are formed only when another piece
+// follows.
+template <bool F16, bool RESIDUAL>
+__device__ __forceinline__ uint32_t piece_bits2(float& r0, float& r1) {
+    if (F16) {
+        const __half2 h = __floats2half2_rn(r0, r1);
+        if (RESIDUAL) {
+            const float2 b = __half22float2(h);
+            r0 -= b.x;
+            r1 -= b.y;
+        }
+        return *reinterpret_cast<const uint32_t*>(&h);
+    }
+    const __nv_bfloat162 h = __floats2bfloat162_rn(r0, r1);
+    if (RESIDUAL) {
+        const float2 b = __bfloat1622float2(h);
+        r0 -= b.x;
+        r1 -= b.y;
+    }
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
 
 // ---------------------------------------------------------------- the GEMM kernel
 // SYN: A = Lam^T (MN-major), B = synthesis image (K-major), D -> Fourier scratch.
@@ -587,8 +609,7 @@ __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const flo
                 float r1 = ri ? v[2 * (2 * h + 1) + par].y : v[2 * (2 * h + 1) + par].x;
 #pragma unroll
                 for (int q = 0; q < NPB; ++q) {
-                    const uint32_t b0 = piece_bits<F16>(r0);
-                    w[q][h] = b0 | (piece_bits<F16>(r1) << 16);
+                    w[q][h] = q + 1 < NPB ? piece_bits2<F16, true>(r0, r1) : piece_bits2<F16, false>(r0, r1);
                 }
             }
             const int64_t off = (int64_t)(c / 8) * 1024 + (c % 8) * 128 + ((ib8 ^ (c % 8)) * 16);
@@ -1020,8 +1041,7 @@ __global__ void __launch_bounds__(256) matrix_image_kernel(const float* __restri
         float r0 = v[2 * h], r1 = v[2 * h + 1];
 #pragma unroll
         for (int q = 0; q < NPB; ++q) {
-            const uint32_t b0 = piece_bits<F16>(r0);
-            w[q][h] = b0 | (piece_bits<F16>(r1) << 16);
+            w[q][h] = q + 1 < NPB ? piece_bits2<F16, true>(r0, r1) : piece_bits2<F16, false>(r0, r1);
         }
     }
     const int64_t off = (int64_t)(n / 8) * 1024 + (n % 8) * 128 + ((ib8 ^ (n % 8)) * 16);
