@@ -183,9 +183,10 @@ SHT_API int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p, 
                  double radius, void* stream);
 
 /* Grid to spectral analysis that allocates nothing, for callers that cannot call
- * cudaMalloc where they transform (inside a CUDA-graph capture they do not own,
- * under a fixed start-up memory pool, or in a runtime that forbids allocation
- * after initialisation). It has no counterpart in the reference.
+ * cudaMalloc where they transform: a host that hands out device memory only from a
+ * fixed pool reserved at start-up, or a runtime that forbids allocation once it is
+ * initialised (an allocation there can fail, or stall every stream of the device).
+ * It has no counterpart in the reference.
  * Same arguments and result as sht_analyze on an SHT_PREC_FP32 plan (FP32 Fourier
  * and Legendre stages); the Fourier coefficients between the two kernels live in a
  * fixed 8 MiB __device__ array of the library instead of the plan's scratch, which
@@ -193,8 +194,10 @@ SHT_API int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p, 
  * Limit: scratch rows x 2 x K x 8 bytes <= 8 MiB (octahedral T63: K <= 223, T127: K <= 59,
  * T255: K <= 15);
  * larger calls return SHT_EINVAL. The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any stream
- * capture. All calls share the array: calls that overlap on the GPU (different
+ * device address (cudaGetSymbolAddress) and keeps it for the life of the process;
+ * make that first call before any stream capture, and do not use the entry point
+ * after a cudaDeviceReset of that device (the kept address would be stale). All
+ * calls share the array: calls that overlap on the GPU (different
  * streams, threads or plans) race and must be serialised by the caller. Every
  * location the Legendre kernel reads is written by the Fourier kernel of the same
  * call, so nothing needs clearing between calls.

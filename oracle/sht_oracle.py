@@ -18,9 +18,9 @@ It restates, in plain numpy float64, what SpeedyTransforms computes:
   Legendre shortcut, normalised associated Legendre polynomials;
 * synthesis ``transform!(field, coeffs, S)``: Legendre
   (``SpeedyTransforms/src/legendre.jl:38-101``) then inverse real FFT per ring
-  (``SpeedyTransforms/src/fourier.jl:439-474``);
+  (``SpeedyTransforms/src/fourier.jl:215-250``);
 * analysis ``transform!(coeffs, field, S)``: real FFT per ring
-  (``SpeedyTransforms/src/fourier.jl:353-390``) then Legendre with quadrature
+  (``SpeedyTransforms/src/fourier.jl:129-166``) then Legendre with quadrature
   (``SpeedyTransforms/src/legendre.jl:131-195``);
 * the spectral operators (``SpeedyTransforms/src/spectral_gradients.jl``) with the
   factors of ``SpeedyTransforms/src/gradient_arrays.jl``.

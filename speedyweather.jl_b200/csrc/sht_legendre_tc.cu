@@ -30,11 +30,23 @@
 //   coefficients for the synthesis, the FFT kernel for the analysis) directly as
 //   swizzled shared-memory images in global memory and loaded with 1-D bulk copies.
 //
-// A persistent CTA per SM computes a sequence of 128 x N output tiles (N <= 256 real
-// columns): warp 0 issues the copies, warp 1 owns the tensor memory (two
-// accumulators) and one of its threads issues the MMAs, warps 2-9 (two per TMEM lane
-// quarter) read the accumulator (tcgen05.ld) and store while the next tile
-// accumulates. The CTA's items are read into shared memory once. Every wait is
+// A persistent CTA per SM computes a sequence of 128 x N output tiles (N <= 128 real
+// columns for the transforms, <= 256 for dense matrices): warp 0 issues the copies,
+// warp 1 owns the tensor memory and one of its threads issues the MMAs, warps 2-9 (two
+// per TMEM lane quarter) read the accumulator (tcgen05.ld) and store while the next
+// tile accumulates.
+//
+// Accumulation. The tensor core adds each MMA's products to its FP32 accumulator with
+// truncation, not rounding to nearest: every update loses on average half a unit in
+// the last place of the accumulator, always toward zero. Over the long same-sign sums
+// of the transforms (the l = 0 coefficient sums all rings; the synthesis of a field
+// with a large mean sums the same sign over l) these losses add up to a bias (measured
+// at T511: the a_00 error pointed toward zero in 98 % of layers, and made up ~70 % of
+// the squared error of every split form). The transforms therefore give each tile two
+// accumulators: one for the leading product (piece 0 x piece 0) and one for all the
+// cross products, which are 2^-8 (bf16) or 2^-11 (fp16) smaller, so their truncation
+// is negligible; the epilogue adds the two in FP32 with rounding to nearest. The large
+// accumulator then takes one update per 16-deep step instead of 3 (5 for BF16X5). The CTA's items are read into shared memory once. Every wait is
 // bounded by a one-second global-timer limit; on expiry the CTA records an error
 // in the plan's status word, drains, frees its tensor memory and returns.
 #include <cuda.h>
@@ -58,6 +70,9 @@ constexpr int TC_THREADS = 320;     // producer warp, MMA warp, 8 epilogue warps
 constexpr int BLK = 64;                     // Legendre box edge (rows x rings)
 constexpr int BOX_BYTES = BLK * BLK * 2;    // 8 KB
 constexpr int A_PIECE_BYTES = 2 * BOX_BYTES;
+// Column tile of the transforms' GEMMs: two buffers of two accumulators of up to 128
+// FP32 columns fill the 512 columns of tensor memory.
+constexpr int kTcTileCols = 128;
 
 struct TcItem {
     int32_t m, par, tile, pad;
@@ -204,9 +219,22 @@ __device__ __forceinline__ ItemInfo item_info(const TcDev& t, const TcItem& it) 
     return f;
 }
 
+// 32 columns of the tile at TMEM address taddr: the leading-product accumulator plus,
+// with xoff > 0, the cross-product accumulator xoff columns further (rounded FP32 sum)
+__device__ __forceinline__ void acc_ld32(uint32_t taddr, uint32_t xoff, float (&v)[32]) {
+    tmem_ld32(taddr, v);
+    if (xoff) {
+        float w[32];
+        tmem_ld32(taddr + xoff, w);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] = __fadd_rn(v[i], w[i]);
+    }
+}
+
 template <bool SYN>
-__device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_cols, int K, uint32_t taddr, int r,
-                               int cb, float2* four, float2* coeffs, int64_t ldc, int add, bool good, bool accumulate) {
+__device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int ctw, int nt_cols, int K, uint32_t taddr,
+                               uint32_t xoff, int r, int cb, float2* four, float2* coeffs, int64_t ldc, int add,
+                               bool good, bool accumulate) {
     // this warp's column chunks: cb, cb + 64, ... (the other warp of its lane quarter takes the rest)
     const int m = it.m, par = it.par, tile = it.tile;
     const float mscale = t.fp16 ? ldexpf(1.f, t.mexp[m] - F16_TOP) : 1.f;
@@ -216,11 +244,11 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
         const float rs = (valid && t.row_scale) ? t.row_scale[row] : 1.f;
         for (int c0 = cb; c0 < nt_cols; c0 += 64) {
             float v[32];
-            tmem_ld32(taddr + c0, v);
+            acc_ld32(taddr + c0, xoff, v);
             if (!valid) continue;
 #pragma unroll
             for (int q = 0; q < 32; ++q) {
-                const int n = ct * 256 + c0 + q;
+                const int n = ct * ctw + c0 + q;
                 if (n >= K) break;
                 float x = v[q];
                 if (t.fp16) x = x * mscale * t.kscale_syn[n].x;
@@ -249,9 +277,9 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
                 __shfl_sync(0xffffffffu, reinterpret_cast<uintptr_t>(dst), 4 * s + (lane & 3)));
         for (int c0 = cb; c0 < nt_cols; c0 += 64) {
             float v[32];
-            tmem_ld32(taddr + c0, v);
+            acc_ld32(taddr + c0, xoff, v);
             if (vm == 0) continue;
-            const int k0 = (ct * 256 + c0) / 2;
+            const int k0 = (ct * ctw + c0) / 2;
             if (t.fp16) {
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
@@ -295,11 +323,11 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
         const int64_t lmo = t.lm_off[m];
         for (int c0 = cb; c0 < nt_cols; c0 += 64) {
             float v[32];
-            tmem_ld32(taddr + c0, v);
+            acc_ld32(taddr + c0, xoff, v);
             if (!valid) continue;
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
-                const int k = (ct * 256 + c0) / 2 + q;
+                const int k = (ct * ctw + c0) / 2 + q;
                 if (k >= K) break;
                 float2* d = coeffs + (int64_t)k * ldc + lmo + 2 * i + par;
                 float2 val = make_float2(v[2 * q], v[2 * q + 1]);
@@ -321,12 +349,15 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int nt_
 
 template <bool SYN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    legendre_tc_kernel(const TcDev t, const TcItem* __restrict__ items, int nitems, int K, int nt_cols, int stages,
-                       uint32_t acc_cols, float2* __restrict__ four, float2* __restrict__ coeffs, int64_t ldc,
-                       int add) {
+    legendre_tc_kernel(const TcDev t, const TcItem* __restrict__ items, int nitems, int K, int ctw, int nt_cols,
+                       int stages, uint32_t acc_cols, int split, float2* __restrict__ four, float2* __restrict__ coeffs,
+                       int64_t ldc, int add) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const int ct = blockIdx.y;                       // column tile (256 columns)
+    const int ct = blockIdx.y;                       // column tile (ctw columns)
+    // per item buffer: the leading-product accumulator, then (split) the cross-product one
+    const uint32_t buf_cols = (split ? 2u : 1u) * acc_cols;
+    const uint32_t xoff = split ? acc_cols : 0u;
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const int a_bytes = t.npa * A_PIECE_BYTES;
     const int b_piece_bytes = nt_cols * 128;
@@ -359,7 +390,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(2 * acc_cols)
+                     "r"(2 * buf_cols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -372,7 +403,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ------------------------------------------------ producer
         const int64_t img_tile_bytes = SYN ? t.syn_tile_bytes : t.ana_tile_bytes;
         const uint8_t* img = reinterpret_cast<const uint8_t*>(SYN ? t.syn_img : t.ana_img);
-        const int64_t col_off = SYN ? (int64_t)ct * 256 * 128 : (int64_t)ct * 4 * BOX_BYTES;
+        const int64_t col_off = SYN ? (int64_t)ct * ctw * 128 : (int64_t)ct * (ctw / 64) * BOX_BYTES;
         int g = 0;
         bool ok = true;
         for (int i = 0, ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ++i, ix += gridDim.x) {
@@ -430,7 +461,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             tc_fence_after();
-            const uint32_t dacc = tmem + (uint32_t)(a * acc_cols);
+            const uint32_t dacc = tmem + (uint32_t)a * buf_cols;
             for (int ks = ks0; ks < min(nsteps, ks0 + kch); ++ks, ++g) {
                 const int s = g % stages;
                 if (!mbar_wait(&full_bar[s], (g / stages) & 1)) {
@@ -444,6 +475,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 for (int kk = 0; kk < BLK / 16; ++kk) {
                     for (int q = 0; q < t.nprod; ++q) {
                         const int pa = (t.prod >> (4 * q)) & 3, pb = (t.prod >> (4 * q + 2)) & 3;
+                        // product 0 is piece 0 x piece 0 (the leading one); with split the
+                        // others go to the cross accumulator, whose first write is product 1
+                        const bool cross = split && q > 0;
+                        const uint32_t dst = cross ? dacc + xoff : dacc;
+                        const bool first = ks == ks0 && kk == 0 && q == (cross ? 1 : 0);
                         const uint32_t aa = st + pa * A_PIECE_BYTES;
                         const uint32_t bb = st + a_bytes + pb * b_piece_bytes;
                         uint64_t da, db;
@@ -454,7 +490,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                             da = sdesc(aa + kk * 32, 16, 1024);
                             db = sdesc(bb + kk * 2048, BOX_BYTES, 1024);
                         }
-                        umma_f16(dacc, da, db, idesc, (ks != ks0 || kk || q) ? 1u : 0u);
+                        umma_f16(dst, da, db, idesc, first ? 0u : 1u);
                     }
                 }
                 umma_commit(&empty_bar[s]);      // frees the stage once these MMAs complete
@@ -479,8 +515,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (!SYN && !add && !*abort_flag) {
                     const int i = it.tile * 128 + r;
                     if (i < t.rows[it.m] && it.m + 2 * i + it.par < t.lmax)
-                        for (int c = 2 * half; c < nt_cols && ct * 256 + c < 2 * K; c += 4)
-                            coeffs[(int64_t)((ct * 256 + c) / 2) * ldc + t.lm_off[it.m] + 2 * i + it.par] =
+                        for (int c = 2 * half; c < nt_cols && ct * ctw + c < 2 * K; c += 4)
+                            coeffs[(int64_t)((ct * ctw + c) / 2) * ldc + t.lm_off[it.m] + 2 * i + it.par] =
                                 make_float2(0.f, 0.f);
                 }
                 continue;
@@ -497,8 +533,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     atomicExch(t.err, 3);
                 }
                 tc_fence_after();
-                const uint32_t taddr = tmem + (uint32_t)(a * acc_cols) + ((uint32_t)(quarter * 32) << 16);
-                epilogue_store<SYN>(t, it, ct, nt_cols, K, taddr, r, 32 * half, four, coeffs, ldc, add,
+                const uint32_t taddr = tmem + (uint32_t)a * buf_cols + ((uint32_t)(quarter * 32) << 16);
+                epilogue_store<SYN>(t, it, ct, ctw, nt_cols, K, taddr, xoff, r, 32 * half, four, coeffs, ldc, add,
                                     ok && !*abort_flag, ks0 > 0);
                 tc_fence_before();
                 mbar_arrive(&acce[a]);
@@ -513,7 +549,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 1) {
         __syncwarp();
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * acc_cols)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * buf_cols)
                      : "memory");
     }
 }
@@ -751,8 +787,9 @@ cudaError_t tc_prepare(Plan& p) {
         return cudaErrorNotSupported;
     }
     const int nh = p.nh, mmax = p.mmax;
-    // image columns: whole 256-column tiles once a call can need more than one
-    s->nmax = 2 * p.d.nlayers <= 256 ? (2 * p.d.nlayers + 63) / 64 * 64 : (2 * p.d.nlayers + 255) / 256 * 256;
+    // image columns: whole column tiles (kTcTileCols) once a call can need more than one
+    s->nmax = 2 * p.d.nlayers <= kTcTileCols ? (2 * p.d.nlayers + 63) / 64 * 64
+                                             : (2 * p.d.nlayers + kTcTileCols - 1) / kTcTileCols * kTcTileCols;
 
     // --- Legendre pieces [m][p][piece][i][j - j0] with row pitch rounded to 8 rings ---
     std::vector<int32_t> nr(mmax), pitch(mmax), nkt(mmax), njt(mmax);
@@ -992,12 +1029,13 @@ cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, in
     e = cudaGetLastError();
     if (e != cudaSuccess || s.n_syn_items == 0) return e;
     const int ncols = 2 * K;
-    const int nct = (ncols + 255) / 256;
-    const int nt_cols = std::min(256, (ncols + 63) / 64 * 64);
+    const int nct = (ncols + kTcTileCols - 1) / kTcTileCols;
+    const int nt_cols = std::min(kTcTileCols, (ncols + 63) / 64 * 64);
     int stages;
     const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
     legendre_tc_kernel<true><<<dim3(std::min(s.n_syn_items, s.nsm), nct), TC_THREADS, smem, st>>>(
-        t, s.d_syn_items, s.n_syn_items, K, nt_cols, stages, tmem_cols_for(nt_cols), p.d_four, nullptr, 0, 0);
+        t, s.d_syn_items, s.n_syn_items, K, kTcTileCols, nt_cols, stages, tmem_cols_for(nt_cols), 1, p.d_four, nullptr,
+        0, 0);
     return cudaGetLastError();
 }
 
@@ -1222,7 +1260,7 @@ cudaError_t tc_matrix_apply(const TcMatrix* x, int which, const float* in, int64
     int stages;
     const int smem = smem_for(x->npa, x->npb, nt_cols, stages);
     legendre_tc_kernel<true><<<dim3(std::min(m.nitems, x->nsm), nct), TC_THREADS, smem, st>>>(
-        t, m.d_items, m.nitems, K, nt_cols, stages, tmem_cols_for(nt_cols), nullptr, nullptr, 0, 0);
+        t, m.d_items, m.nitems, K, 256, nt_cols, stages, tmem_cols_for(nt_cols), 0, nullptr, nullptr, 0, 0);
     return cudaGetLastError();
 }
 
@@ -1242,13 +1280,13 @@ cudaError_t launch_legendre_analysis_tc(const Plan& p, float2* coeffs, int64_t l
     if (s.n_ana_items == 0) return cudaSuccess;
     const TcDev t = make_dev(p);
     const int ncols = 2 * K;
-    const int nct = (ncols + 255) / 256;
-    const int nt_cols = std::min(256, (ncols + 63) / 64 * 64);
+    const int nct = (ncols + kTcTileCols - 1) / kTcTileCols;
+    const int nt_cols = std::min(kTcTileCols, (ncols + 63) / 64 * 64);
     int stages;
     const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
     legendre_tc_kernel<false><<<dim3(std::min(s.n_ana_items, s.nsm), nct), TC_THREADS, smem, st>>>(
-        t, s.d_ana_items, s.n_ana_items, K, nt_cols, stages, tmem_cols_for(nt_cols), nullptr, coeffs, ldc,
-        add ? 1 : 0);
+        t, s.d_ana_items, s.n_ana_items, K, kTcTileCols, nt_cols, stages, tmem_cols_for(nt_cols), 1, nullptr, coeffs,
+        ldc, add ? 1 : 0);
     return cudaGetLastError();
 }
 

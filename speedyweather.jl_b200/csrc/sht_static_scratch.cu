@@ -1,9 +1,9 @@
 // Grid -> spectral analysis for callers that cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc on the path where they transform: code
-// running inside a CUDA-graph capture they do not control, a host with a
-// fixed-size memory pool handed out at start-up, or a runtime that forbids
-// allocation after initialisation. sht_analyze_static_scratch lets them run the
+// Some callers cannot call cudaMalloc on the path where they transform: a host
+// whose device memory is a fixed-size pool handed out at start-up, or a runtime
+// that forbids allocation once initialised (an allocation there can fail, or
+// stall every stream of the device). sht_analyze_static_scratch lets them run the
 // analysis without any allocation: the Fourier coefficients that pass between
 // the Fourier and the Legendre kernel live in a file-scope __device__ array of
 // fixed size (kStaticScratchBytes) instead of the plan's scratch. The plan itself
@@ -30,8 +30,10 @@ namespace {
 constexpr size_t kStaticScratchBytes = size_t(8) << 20;
 __device__ __align__(256) float2 g_static_scratch[kStaticScratchBytes / sizeof(float2)];
 
-// Device address of g_static_scratch, looked up once per device. In host code the
-// name g_static_scratch is only a host-side stand-in, never a device address.
+// Device address of g_static_scratch, looked up once per device (on the first call,
+// with that device current) and kept for the life of the process; a cudaDeviceReset
+// would make it stale, so the entry point is not for use across one. In host code
+// the name g_static_scratch is only a host-side stand-in, never a device address.
 constexpr int kMaxDevices = 128;
 std::mutex g_mutex;
 float2* g_addr[kMaxDevices] = {};
