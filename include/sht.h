@@ -182,6 +182,36 @@ SHT_API int sht_laplace(sht_plan* plan, void* out, const void* alms, int64_t ldc
 SHT_API int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p, int64_t ldc, int K,
                  double radius, void* stream);
 
+/* Several spectral operators in one kernel launch (no counterpart in the reference, whose
+ * time step calls curl!, divergence!, ∇²! ... one by one: SpeedyWeather/src/dynamics/
+ * tendencies.jl:161-214, 585-594). Each sht_op is one of the calls above with the same
+ * arguments and the same result bit for bit; a thread applies the ops to its (lm, layer)
+ * in list order, so several ops accumulating (SHT_ADD) into the same output give the
+ * result of the separate calls in that order. Rules, checked (SHT_EINVAL otherwise): at
+ * most SHT_MAX_OPS ops; an op's inputs must not overlap any output of the batch; outputs
+ * that overlap must be the same array (same pointer and ldc). radius as in the single
+ * calls; b is v for curl/divergence, div for UV_from_vordiv (may be NULL), unused otherwise;
+ * out2 is V for UV_from_vordiv, dpdy for the gradient, unused otherwise. */
+#define SHT_OP_CURL 0
+#define SHT_OP_DIVERGENCE 1
+#define SHT_OP_LAPLACE 2          /* flags SHT_INVERSE: the inverse Laplacian */
+#define SHT_OP_GRADIENT 3
+#define SHT_OP_UV_FROM_VORDIV 4
+#define SHT_MAX_OPS 16
+typedef struct sht_op {
+    int32_t kind;
+    uint32_t flags;             /* SHT_ADD, SHT_FLIPSIGN, SHT_INVERSE as in the single calls */
+    void* out;
+    void* out2;
+    const void* a;
+    const void* b;
+    int64_t ldc;
+    int32_t K;
+    int32_t pad;
+    double radius;
+} sht_op;
+SHT_API int sht_operators(sht_plan* plan, const sht_op* ops, int nops, void* stream);
+
 /* Grid to spectral analysis that allocates nothing, for callers that cannot call
  * cudaMalloc where they transform: a host that hands out device memory only from a
  * fixed pool reserved at start-up, or a runtime that forbids allocation once it is

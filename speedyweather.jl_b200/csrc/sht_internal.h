@@ -202,6 +202,7 @@ cudaError_t launch_uv_from_vordiv(const Plan& p, float2* U, float2* V, const flo
                                   const float2* div, int64_t ldc, int K, float radius, cudaStream_t s);
 cudaError_t launch_laplace(const Plan& p, float2* out, const float2* in, int64_t ldc, int K,
                            bool inverse, bool flipsign, bool add, float scale, cudaStream_t s);
+cudaError_t launch_operators(const Plan& p, const sht_op* ops, int nops, cudaStream_t s);
 cudaError_t launch_gradient(const Plan& p, float2* dpdx, float2* dpdy, const float2* in, int64_t ldc,
                             int K, float inv_radius, cudaStream_t s);
 

@@ -976,6 +976,64 @@ int sht_gradient(sht_plan* plan, void* dpdx, void* dpdy, const void* p_, int64_t
                   "sht_gradient");
 }
 
+int sht_operators(sht_plan* plan, const sht_op* ops, int nops, void* stream) {
+    const char* what = "sht_operators";
+    if (!plan) return fail(SHT_EINVAL, "%s: plan is NULL", what);
+    if (nops < 0 || nops > SHT_MAX_OPS) return fail(SHT_EINVAL, "%s: %d ops (at most %d)", what, nops, SHT_MAX_OPS);
+    if (nops == 0) return SHT_OK;
+    if (!ops) return fail(SHT_EINVAL, "%s: ops is NULL", what);
+    const Plan& p = plan->p;
+    // byte range of an array of K layers with leading dimension ldc
+    auto range = [&](const void* ptr, int64_t ldc, int K) {
+        const uintptr_t b = reinterpret_cast<uintptr_t>(ptr);
+        return std::make_pair(b, b + (uintptr_t)(((int64_t)(K - 1) * ldc + p.nlm) * 8));
+    };
+    auto overlap = [](std::pair<uintptr_t, uintptr_t> x, std::pair<uintptr_t, uintptr_t> y) {
+        return x.first < y.second && y.first < x.second;
+    };
+    struct Arr {
+        const void* ptr;
+        int64_t ldc;
+        std::pair<uintptr_t, uintptr_t> r;
+    };
+    std::vector<Arr> outs, ins;
+    for (int j = 0; j < nops; ++j) {
+        const sht_op& o = ops[j];
+        int rc = ops_check(plan, o.ldc, o.K, what, {o.out, o.a});
+        if (rc != SHT_OK) return rc;
+        if (o.K == 0) continue;
+        const bool two_out = o.kind == SHT_OP_GRADIENT || o.kind == SHT_OP_UV_FROM_VORDIV;
+        switch (o.kind) {
+            case SHT_OP_CURL:
+            case SHT_OP_DIVERGENCE:
+                if (!o.b) return fail(SHT_EINVAL, "%s: op %d: NULL array", what, j);
+                break;
+            case SHT_OP_LAPLACE:
+                break;
+            case SHT_OP_GRADIENT:
+            case SHT_OP_UV_FROM_VORDIV:
+                if (!o.out2) return fail(SHT_EINVAL, "%s: op %d: NULL array", what, j);
+                break;
+            default:
+                return fail(SHT_EINVAL, "%s: op %d: unknown kind %d", what, j, o.kind);
+        }
+        if (!(o.radius > 0.0)) return fail(SHT_EINVAL, "%s: op %d: radius must be positive", what, j);
+        outs.push_back({o.out, o.ldc, range(o.out, o.ldc, o.K)});
+        if (two_out) outs.push_back({o.out2, o.ldc, range(o.out2, o.ldc, o.K)});
+        ins.push_back({o.a, o.ldc, range(o.a, o.ldc, o.K)});
+        if (o.b && o.kind != SHT_OP_LAPLACE && o.kind != SHT_OP_GRADIENT) ins.push_back({o.b, o.ldc, range(o.b, o.ldc, o.K)});
+    }
+    for (const Arr& x : ins)
+        for (const Arr& y : outs)
+            if (overlap(x.r, y.r)) return fail(SHT_EINVAL, "%s: an input overlaps an output of the batch", what);
+    for (size_t i = 0; i < outs.size(); ++i)
+        for (size_t k = i + 1; k < outs.size(); ++k)
+            if (overlap(outs[i].r, outs[k].r) && (outs[i].ptr != outs[k].ptr || outs[i].ldc != outs[k].ldc))
+                return fail(SHT_EINVAL, "%s: overlapping outputs must be the same array", what);
+    DeviceGuard g(p.device);
+    return finish(launch_operators(p, ops, nops, (cudaStream_t)stream), what);
+}
+
 }  // extern "C"
 
 namespace sht {

@@ -10,7 +10,7 @@ SpeedyTransforms/src/spectral_gradients.jl) over the C ABI of libsht.so:
   ``transform(in, S)`` allocates;
 * operators ``curl_``, ``divergence_``, ``UV_from_vor_``, ``UV_from_vordiv_``,
   ``laplace_`` (``∇²!``), ``inverse_laplace_`` (``∇⁻²!``), ``gradient_`` (``∇!``)
-  and their allocating forms;
+  and their allocating forms; ``Operators`` -- several of them in one kernel launch;
 * ``MatrixSpectralTransform`` -- the dense-matrix transforms (cuBLAS FP32 or tcgen05);
 * ``Batch`` -- many transforms in one grouped launch per stage, CUDA-graph capture;
 * ``spec2grid_pullback_``, ``grid2spec_pullback_`` -- the adjoints of the transforms.
@@ -25,6 +25,7 @@ from .core import (  # noqa: F401
     LowerTriangularArray,
     MatrixSpectralTransform,
     OctahedralGaussianGrid,
+    Operators,
     SpectralTransform,
     Spectrum,
     UV_from_vor,

@@ -32,6 +32,16 @@ class ShtInfo(C.Structure):
                 ("table_bytes", C.c_int64)]
 
 
+class ShtOp(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("flags", C.c_uint32), ("out", C.c_void_p), ("out2", C.c_void_p),
+                ("a", C.c_void_p), ("b", C.c_void_p), ("ldc", C.c_int64), ("K", C.c_int32), ("pad", C.c_int32),
+                ("radius", C.c_double)]
+
+
+OP_CURL, OP_DIVERGENCE, OP_LAPLACE, OP_GRADIENT, OP_UV_FROM_VORDIV = 0, 1, 2, 3, 4
+MAX_OPS = 16
+
+
 class ShtBatchItem(C.Structure):
     _fields_ = [("plan", C.c_void_p), ("direction", C.c_int), ("coeffs", C.c_void_p), ("ldc", C.c_int64),
                 ("grid", C.c_void_p), ("ldg", C.c_int64), ("nlayers", C.c_int), ("flags", C.c_uint)]
@@ -61,6 +71,7 @@ SIGNATURES = {
     "sht_uv_from_vordiv": (C.c_int, [_P, _P, _P, _P, _P, _I64, C.c_int, C.c_double, _P]),
     "sht_laplace": (C.c_int, [_P, _P, _P, _I64, C.c_int, C.c_uint, C.c_double, _P]),
     "sht_gradient": (C.c_int, [_P, _P, _P, _P, _I64, C.c_int, C.c_double, _P]),
+    "sht_operators": (C.c_int, [_P, C.POINTER(ShtOp), C.c_int, _P]),
     "sht_device_status": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "sht_diag_wait_expiry": (C.c_int, [_P, C.c_int32, _P]),
     "sht_analyze_static_scratch": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),

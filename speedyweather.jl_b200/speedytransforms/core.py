@@ -577,6 +577,57 @@ def _divcurl(fn, out, u, v, S, flipsign, add, radius):
     return out
 
 
+class Operators:
+    """Several spectral operators run in one kernel launch (sht_operators), each with the
+    arguments and the result of its single call (curl_, divergence_, laplace_,
+    inverse_laplace_, gradient_, UV_from_vordiv_), applied in the order added, so that
+    operators accumulating (add=True) into the same output match the separate calls bit
+    for bit. No counterpart in the reference, whose time step calls the operators one by
+    one (SpeedyWeather/src/dynamics/tendencies.jl:161-214, 585-594). Inputs must not
+    overlap any output of the set; overlapping outputs must be the same array. The set
+    keeps references to its arrays and can be run repeatedly (and captured in a graph)."""
+
+    def __init__(self, S):
+        self.S = S
+        self._ops = []
+        self._keep = []
+
+    def _add(self, kind, flags, out, out2, a, b, radius):
+        arrs = [x for x in (out, out2, a, b) if x is not None]
+        ld, K = _coeffs(self.S, *arrs)
+        if len(self._ops) >= _lib.MAX_OPS:
+            raise ValueError(f"at most {_lib.MAX_OPS} operators per set")
+        ptr = lambda x: x.data.data_ptr() if x is not None else None   # noqa: E731
+        self._ops.append(_lib.ShtOp(kind, flags, ptr(out), ptr(out2), ptr(a), ptr(b), ld, K, 0, float(radius)))
+        self._keep.extend(arrs)
+        return self
+
+    def curl(self, out, u, v, *, flipsign=False, add=False, radius=1.0):
+        flags = (_lib.FLIPSIGN if flipsign else 0) | (_lib.ADD if add else 0)
+        return self._add(_lib.OP_CURL, flags, out, None, u, v, radius)
+
+    def divergence(self, out, u, v, *, flipsign=False, add=False, radius=1.0):
+        flags = (_lib.FLIPSIGN if flipsign else 0) | (_lib.ADD if add else 0)
+        return self._add(_lib.OP_DIVERGENCE, flags, out, None, u, v, radius)
+
+    def laplace(self, out, alms, *, add=False, flipsign=False, inverse=False, radius=1.0):
+        flags = (_lib.FLIPSIGN if flipsign else 0) | (_lib.ADD if add else 0) | (_lib.INVERSE if inverse else 0)
+        return self._add(_lib.OP_LAPLACE, flags, out, None, alms, None, radius)
+
+    def gradient(self, dpdx, dpdy, p, *, radius=1.0):
+        return self._add(_lib.OP_GRADIENT, 0, dpdx, dpdy, p, None, radius)
+
+    def UV_from_vordiv(self, U, V, vor, div=None, *, radius=1.0):
+        return self._add(_lib.OP_UV_FROM_VORDIV, 0, U, V, vor, div, radius)
+
+    def __len__(self):
+        return len(self._ops)
+
+    def __call__(self):
+        arr = (_lib.ShtOp * max(1, len(self._ops)))(*self._ops)
+        check(lib.sht_operators(self.S.handle, arr, len(self._ops), _stream_ptr(self.S.device)))
+
+
 def curl_(out, u, v, S, *, flipsign=False, add=False, radius=1.0):
     """curl!(curl, u, v, S; flipsign, add, radius) (spectral_gradients.jl:30-41)."""
     return _divcurl(lib.sht_curl, out, u, v, S, flipsign, add, radius)
