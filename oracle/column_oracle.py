@@ -223,13 +223,16 @@ def bf16_round(a):
 
 
 def gelu(x):
-    from scipy.special import erf
-    return 0.5 * x * (1 + erf(x / np.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks & Gimpel 2016), as the emulator's kernels."""
+    u = np.sqrt(2.0 / np.pi) * (x + 0.044715 * x ** 3)
+    return 0.5 * x * (1 + np.tanh(u))
 
 
 def gelu_grad(x):
-    from scipy.special import erf
-    return 0.5 * (1 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2 * np.pi)
+    u = np.sqrt(2.0 / np.pi) * (x + 0.044715 * x ** 3)
+    t = np.tanh(u)
+    du = np.sqrt(2.0 / np.pi) * (1 + 3 * 0.044715 * x ** 2)
+    return 0.5 * (1 + t) + 0.5 * x * (1 - t * t) * du
 
 
 def mlp_forward(params, xn, bf16=True):

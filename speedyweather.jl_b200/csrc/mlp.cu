@@ -77,9 +77,21 @@ struct GemmArgs {
 constexpr int G_EPI_LD = 33;        // epilogue transpose tile [32 rows][33]
 constexpr int G_EPI_BYTES = 8 * 32 * G_EPI_LD * 4;
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel 2016): gelu(x) = x (1 + tanh(u)) / 2,
+// u = sqrt(2 / pi) (x + 0.044715 x^3), with tanh(u) = 1 - 2 / (exp(2 u) + 1) on the exp
+// intrinsic (relative error ~1e-7, a handful of instructions; exp overflows to +inf
+// for large u, which gives tanh = 1, and underflows to 0 for very negative u: -1).
+constexpr float GELU_C = 0.7978845608028654f;    // sqrt(2 / pi)
+constexpr float GELU_A = 0.044715f;
+__device__ __forceinline__ float gelu_tanh(float x) {
+    const float u = GELU_C * x * fmaf(GELU_A * x, x, 1.f);
+    return 1.f - __fdividef(2.f, __expf(2.f * u) + 1.f);
+}
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + gelu_tanh(x)); }
 __device__ __forceinline__ float gelu_grad(float x) {
-    return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.3989422804014327f * expf(-0.5f * x * x);
+    const float t = gelu_tanh(x);
+    const float du = GELU_C * fmaf(3.f * GELU_A * x, x, 1.f);
+    return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * du;
 }
 
 // One 128 x nt output tile per CTA (nt a multiple of 16, <= 256; tile y covers columns
@@ -450,12 +462,19 @@ constexpr int F_STAGES = 3;
 constexpr int F_W_STAGE = 4 * G_BOX_BYTES;           // 256 rows x 64 features
 constexpr int F_ACT_BYTES = 4 * 2 * G_BOX_BYTES;     // 128 rows x 256 features (4 blocks of 16 KB)
 constexpr int F_TAIL = 128 + 512;                    // barriers, inside flags [4][128]
-constexpr int F_SMEM = 1024 + F_ACT_BYTES + F_STAGES * F_W_STAGE + F_TAIL;
+// the network's constants, staged once per CTA: input mean / std [33] [33], output mean /
+// std [16] [16], biases [256] [256] [256] [16]
+constexpr int F_C_XM = 0, F_C_XS = 33, F_C_YM = 66, F_C_YS = 82, F_C_B0 = 98, F_C_B1 = 354, F_C_B2 = 610,
+              F_C_B3 = 866, F_C_N = 882;
+constexpr int F_CONST = 4096;
+static_assert(F_C_N * 4 <= F_CONST, "constants exceed their shared-memory area");
+constexpr int F_SMEM = 1024 + F_ACT_BYTES + F_STAGES * F_W_STAGE + F_TAIL + F_CONST;
 
 struct FusedArgs {
     const float *T, *q, *u, *v, *ps;
     int64_t ld;
     int ncol;
+    int cpb;                 // columns per CTA (<= 128: the MMA tile's rows)
     const float *xm, *xs, *ym, *ys;
     const float* bias[4];
     float zmax, dt;
@@ -470,9 +489,11 @@ struct FusedArgs {
 __device__ __forceinline__ uint32_t act_off(int r, int k) {
     return (uint32_t)((k >> 6) * (2 * G_BOX_BYTES) + r * 128 + ((((k & 63) >> 3) ^ (r & 7)) << 4) + ((k & 7) << 1));
 }
+// two reals rounded to bf16 (each to nearest, as two separate roundings) by one paired
+// conversion instruction
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
-    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(lo)) |
-           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(hi)) << 16);
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&h);
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
@@ -492,10 +513,14 @@ __global__ void __launch_bounds__(F_THREADS, 1)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     uint8_t* inside = reinterpret_cast<uint8_t*>(full_bar) + 128;
+    float* cst = reinterpret_cast<float*>(inside + 512);
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int col0 = blockIdx.x * 128;
-    const int nrow = min(128, a.ncol - col0);
-    const int nkb[4] = {1, 4, 4, 4}, nbox[4] = {4, 4, 4, 1}, nout[4] = {256, 256, 256, 16};
+    const int col0 = blockIdx.x * a.cpb;
+    const int nrow = min(a.cpb, a.ncol - col0);
+    // per layer: K blocks of 64 inputs, 64-row boxes of weights, outputs (no arrays: no stack)
+    auto nkb = [](int l) { return l == 0 ? 1 : 4; };
+    auto nbox = [](int l) { return l == 3 ? 1 : 4; };
+    auto nout = [](int l) { return l == 3 ? 16 : 256; };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < F_STAGES; ++s) {
@@ -514,6 +539,18 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    for (int i = threadIdx.x; i < F_C_N; i += blockDim.x) {   // the constants, read once
+        float c;
+        if (i < F_C_XS) c = a.xm[i];
+        else if (i < F_C_YM) c = a.xs[i - F_C_XS];
+        else if (i < F_C_YS) c = a.ym[i - F_C_YM];
+        else if (i < F_C_B0) c = a.ys[i - F_C_YS];
+        else if (i < F_C_B1) c = a.bias[0][i - F_C_B0];
+        else if (i < F_C_B2) c = a.bias[1][i - F_C_B1];
+        else if (i < F_C_B3) c = a.bias[2][i - F_C_B2];
+        else c = a.bias[3][i - F_C_B3];
+        cst[i] = c;
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -521,10 +558,10 @@ __global__ void __launch_bounds__(F_THREADS, 1)
 
     if (warp == 0 && lane == 0) {
         // ---- producer: the weight blocks of the four layers in order
-        const CUtensorMap* maps[4] = {&w0, &w1, &w2, &w3};
         int g = 0;
-        for (int l = 0; l < 4 && !*abort_flag; ++l)
-            for (int kb = 0; kb < nkb[l] && !*abort_flag; ++kb, ++g) {
+        for (int l = 0; l < 4 && !*abort_flag; ++l) {
+            const CUtensorMap* map = l == 0 ? &w0 : l == 1 ? &w1 : l == 2 ? &w2 : &w3;
+            for (int kb = 0; kb < nkb(l) && !*abort_flag; ++kb, ++g) {
                 const int s = g % F_STAGES;
                 if (g >= F_STAGES && !mbar_wait(&empty_bar[s], ((g / F_STAGES) - 1) & 1)) {
                     *abort_flag = 1;
@@ -532,9 +569,10 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                     break;
                 }
                 uint8_t* st = wst + s * F_W_STAGE;
-                mbar_expect_tx(&full_bar[s], (uint32_t)(nbox[l] * G_BOX_BYTES));
-                for (int h = 0; h < nbox[l]; ++h) tma_load_2d(st + h * G_BOX_BYTES, maps[l], kb * G_BOX, h * G_BOX, &full_bar[s]);
+                mbar_expect_tx(&full_bar[s], (uint32_t)(nbox(l) * G_BOX_BYTES));
+                for (int h = 0; h < nbox(l); ++h) tma_load_2d(st + h * G_BOX_BYTES, map, kb * G_BOX, h * G_BOX, &full_bar[s]);
             }
+        }
         for (int u = g - 1; u >= 0 && u >= g - F_STAGES; --u)   // no copy lands after the exit
             if (!mbar_wait(&full_bar[u % F_STAGES], (u / F_STAGES) & 1)) atomicExch(a.err, 22);
     } else if (warp == 1 && lane == 0) {
@@ -548,8 +586,8 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                 break;
             }
             tc_fence_after();
-            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)nout[l] >> 3) << 17) | ((128u >> 4) << 24);
-            for (int kb = 0; kb < nkb[l]; ++kb, ++g) {
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)nout(l) >> 3) << 17) | ((128u >> 4) << 24);
+            for (int kb = 0; kb < nkb(l); ++kb, ++g) {
                 const int s = g % F_STAGES;
                 if (!mbar_wait(&full_bar[s], (g / F_STAGES) & 1)) {
                     *abort_flag = 1;
@@ -590,7 +628,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                         } else {
                             x = logf(a.ps[ij]);
                         }
-                        z = (x - a.xm[c]) / a.xs[c];
+                        z = (x - cst[F_C_XM + c]) / cst[F_C_XS + c];
                         in = in && fabsf(z) <= a.zmax;
                     }
                     z2[e] = z;
@@ -613,6 +651,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
         const int r = quarter * 32 + lane;
         const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
         bool ok = true;
+        const bool rows_used = quarter * 32 < nrow;   // lane quarters past the CTA's columns skip the work
         for (int l = 0; l < 3 && ok; ++l) {   // ---- hidden layers: bias, GELU, BF16 in place
             ok = __all_sync(0xffffffffu, mbar_wait(acc_bar, l & 1));
             if (!ok) {
@@ -621,8 +660,8 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                 break;
             }
             tc_fence_after();
-            const float* bias = a.bias[l];
-            for (int c0 = 32 * half; c0 < 256; c0 += 128) {
+            const float* bias = cst + (l == 0 ? F_C_B0 : l == 1 ? F_C_B1 : F_C_B2);
+            for (int c0 = 32 * half; c0 < (rows_used ? 256 : 0); c0 += 128) {
                 float v[32];
                 tmem_ld32(taddr + c0, v);
                 uint32_t pk[16];
@@ -655,9 +694,9 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                 if (inside[r] && inside[128 + r] && inside[256 + r] && inside[384 + r]) {
 #pragma unroll
                     for (int k = 0; k < NLC; ++k) {
-                        const float y0 = v[k] + a.bias[3][k], y1 = v[NLC + k] + a.bias[3][NLC + k];
-                        dT[k] = y0 * a.ys[k] + a.ym[k];
-                        dq[k] = y1 * a.ys[NLC + k] + a.ym[NLC + k];
+                        const float y0 = v[k] + cst[F_C_B3 + k], y1 = v[NLC + k] + cst[F_C_B3 + NLC + k];
+                        dT[k] = y0 * cst[F_C_YS + k] + cst[F_C_YM + k];
+                        dq[k] = y1 * cst[F_C_YS + NLC + k] + cst[F_C_YM + NLC + k];
                     }
                 } else {
                     float T[NLC], q[NLC];
@@ -667,7 +706,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                         q[k] = a.q[(int64_t)k * a.ld + ij];
                     }
                     colphys::column_tendencies(T, q, a.ps[ij], a.dt, a.L, dT, dq);
-                    atomicAdd(a.nfallback, 1);
+                    if (a.nfallback) atomicAdd(a.nfallback, 1);
                 }
 #pragma unroll
                 for (int k = 0; k < NLC; ++k) {
@@ -1039,7 +1078,8 @@ int sht_column_emulate(sht_mlp* m, const float* temp, const float* humid, const 
     DevGuard dg(m->device);
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = fused_attributes();
-    if (e == cudaSuccess) e = cudaMemsetAsync(m->nfallback, 0, 4, s);
+    // the fallback count only when asked for (it synchronises the stream)
+    if (e == cudaSuccess && nfallback) e = cudaMemsetAsync(m->nfallback, 0, 4, s);
     if (e == cudaSuccess) {
         FusedArgs fa{};
         fa.T = temp;
@@ -1060,10 +1100,14 @@ int sht_column_emulate(sht_mlp* m, const float* temp, const float* humid, const 
         fa.dT = dtemp;
         fa.dq = dhumid;
         fa.add = (flags & SHT_ADD) ? 1 : 0;
-        fa.nfallback = m->nfallback;
+        fa.nfallback = nfallback ? m->nfallback : nullptr;
         fa.err = m->err;
-        mlp_fused_kernel<<<(ncol + 127) / 128, F_THREADS, F_SMEM, s>>>(m->wmap[0], m->wmap[1], m->wmap[2], m->wmap[3],
-                                                                       fa);
+        // one CTA per SM when the columns allow it (at most 128 per CTA: the MMA tile's rows)
+        int nsm = 148;
+        if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess || nsm < 1) nsm = 148;
+        fa.cpb = std::min(128, std::max(1, (ncol + nsm - 1) / nsm));
+        mlp_fused_kernel<<<(ncol + fa.cpb - 1) / fa.cpb, F_THREADS, F_SMEM, s>>>(m->wmap[0], m->wmap[1], m->wmap[2],
+                                                                               m->wmap[3], fa);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess && nfallback) {

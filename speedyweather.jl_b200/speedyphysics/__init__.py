@@ -7,6 +7,8 @@
 * ``ColumnEmulator`` -- the MLP that stands in for both, with hand-written BF16 training and
   inference kernels on the tensor cores, used as a parameterization with the plain
   schemes as fallback for columns outside its training range (``parameterization_``).
+* ``ModelStates`` -- columns of the wet model's own states at T63 (the reference's initial
+  state with seeded variations, through this library's transforms) to train it on.
 
 Fields are layer-major like a Field{npoints, nlayers}: torch tensors [8, ncol] float32 on
 the GPU, surface pressure [ncol]. Every compute call runs libsht's kernels.
@@ -14,6 +16,7 @@ the GPU, surface pressure [ncol]. Every compute call runs libsht's kernels.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 import torch
@@ -143,17 +146,26 @@ class ColumnEmulator:
         check(lib.sht_mlp_loss(self._m, C.byref(v)))
         return float(v.value)
 
-    def train(self, x, y, *, epochs=4, batch=4096, lr=1e-3, seed=0):
-        """Minibatch Adam over (x, y) [N, 33], [N, 16] on the GPU; returns the mean loss per epoch."""
+    def train(self, x, y, *, epochs=4, batch=4096, lr=1e-3, seed=0, schedule="halve"):
+        """Minibatch Adam over (x, y) [N, 33], [N, 16] on the GPU; returns the mean loss per
+        epoch. schedule: "halve" (lr / 2 per epoch) or "cosine" (cosine decay over all steps
+        to lr / 100)."""
         g = torch.Generator(device=x.device).manual_seed(seed)
         losses = []
         n = x.shape[0]
+        steps = max(1, epochs * (n // batch))
+        k = 0
         for ep in range(epochs):
             perm = torch.randperm(n, device=x.device, generator=g)
             tot, cnt = 0.0, 0
             for i in range(0, n - batch + 1, batch):
                 idx = perm[i:i + batch]
-                self.train_step(x[idx].contiguous(), y[idx].contiguous(), lr * (0.5 ** ep))
+                if schedule == "cosine":
+                    rate = lr * (0.01 + 0.99 * 0.5 * (1 + math.cos(math.pi * k / steps)))
+                else:
+                    rate = lr * (0.5 ** ep)
+                self.train_step(x[idx].contiguous(), y[idx].contiguous(), rate)
+                k += 1
                 if (i // batch) % 16 == 0:
                     tot += self.loss()
                     cnt += 1
@@ -207,3 +219,6 @@ def bf16_gemm(A, a_mn, B, b_mn, M, N, K):
     check(lib.sht_bf16_gemm(A.data_ptr(), A.shape[1], int(a_mn), B.data_ptr(), B.shape[1], int(b_mn), Cm.data_ptr(),
                             N, M, N, K, err.data_ptr(), _stream(A)))
     return Cm, err
+
+
+from .model_states import ModelStates  # noqa: E402,F401
