@@ -305,8 +305,11 @@ SHT_API int sht_batch_destroy(sht_batch* b);
  * replaces SpeedyTransforms/src/matrix_transform.jl:56-260: the transforms as products
  * with precomputed dense matrices (the transforms of unit vectors, :134-173), built here
  * by this library's FP32 transforms. desc as for sht_plan_create; precision
- * SHT_PREC_FP32 runs cuBLAS SGEMM (the reference's Float32 mul!), SHT_PREC_BF16X3 /
- * SHT_PREC_FP16X3 / SHT_PREC_BF16X5 the tcgen05 kernel with the matrix in 16-bit pieces.
+ * SHT_PREC_FP32 runs three TF32 products on the tensor cores (tcgen05 kind::tf32, the
+ * matrix read once as FP32 and split in shared memory; the reference's Float32 mul! to
+ * FP32 rounding), SHT_PREC_BF16X3 / SHT_PREC_FP16X3 / SHT_PREC_BF16X5 the tcgen05 kernel
+ * with the matrix in 16-bit pieces. Calls on one matrix transform share its scratch:
+ * issue them in order on one stream.
  * Matrices: npoints x 2 nlm floats each (T63 octahedral: 188 MB in FP32), so this suits
  * the small truncations the reference uses it for.
  * sht_matrix_synthesize: coeffs [K][ldc] complex -> grid [K][ldg]; flags SHT_UNSCALE_COSLAT.

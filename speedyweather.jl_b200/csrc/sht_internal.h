@@ -177,6 +177,12 @@ cudaError_t tc_matrix_create(TcMatrix** out, int precision, const float* const a
 void tc_matrix_destroy(TcMatrix* x);
 cudaError_t tc_matrix_apply(const TcMatrix* x, int which, const float* in, int64_t ld, float* out, int64_t ldo, int K,
                             const float* row_scale, int32_t* d_err, cudaStream_t st);
+// FP32 dense matrix transforms as three TF32 products on the tensor cores (sht_matrix_tf32.cu)
+struct MxTf32;
+cudaError_t mx_tf32_create(MxTf32** out, const float* const a[2], const int depth[2], const int M[2], int nlayers);
+void mx_tf32_destroy(MxTf32* x);
+cudaError_t mx_tf32_apply(const MxTf32* x, int which, const float* in, int64_t ld, float* out, int64_t ldo, int K,
+                          const float* row_scale, int32_t* d_err, cudaStream_t st);
 // failure-detection check of the bounded mbarrier waits (sht_legendre_tc.cu)
 cudaError_t launch_wait_probe(int32_t* err, uint64_t limit_ns, cudaStream_t s);
 cudaError_t launch_column_physics(const float* temp, const float* humid, const float* ps, int64_t ld, int ncol,

@@ -9,11 +9,13 @@
 //   B_r [2 nlm][npoints]  row 2lm = synthesis of coeffs e_lm (= Re B[:, lm]), row 2lm+1 =
 //                         synthesis of i e_lm (= -Im B[:, lm]), so field = B_r-product of
 //                         the coefficients viewed as floats (Re B Re c - Im B Im c)
-// Products: with an SHT_PREC_FP32 description one cuBLAS SGEMM per call (the reference's
-// Float32 mul!, :206-258); with a tensor-core precision the persistent tcgen05 kernel of
-// sht_legendre_tc.cu in its matrix mode (the matrix in 16-bit pieces by TMA, the layers
-// as the N columns). unscale_coslat scales the synthesised rings by 1/cos(lat) (:255-257).
-#include <cublas_v2.h>
+// Products: with an SHT_PREC_FP32 description three TF32 products on the tensor cores
+// (sht_matrix_tf32.cu: the matrix streamed once as FP32 and split in shared memory; the
+// reference's Float32 mul!, :206-258); with a split 16-bit precision the persistent
+// tcgen05 kernel of sht_legendre_tc.cu in its matrix mode (the matrix in 16-bit pieces
+// by TMA, the layers as the N columns). unscale_coslat scales the synthesised rings by
+// 1/cos(lat) (:255-257), in the products' epilogue.
+
 
 #include <cmath>
 #include <vector>
@@ -31,12 +33,12 @@ struct sht_matrix {
     sht_plan* base = nullptr;         // FP32 transform the matrices are built with
     sht_desc d{};
     int64_t npoints = 0, nlm = 0;
-    float* d_F = nullptr;             // F^T [npoints][2 nlm]   (FP32 plans)
-    float* d_B = nullptr;             // B_r [2 nlm][npoints]   (FP32 plans)
+    float* d_F = nullptr;             // F^T [npoints][2 nlm] (freed once the products' operands exist)
+    float* d_B = nullptr;             // B_r [2 nlm][npoints]
     float* d_row_scale = nullptr;     // [npoints]: 1 / cos(lat) of the point's ring
     int32_t* d_err = nullptr;
-    TcMatrix* tc = nullptr;
-    cublasHandle_t blas = nullptr;
+    TcMatrix* tc = nullptr;           // split 16-bit precisions
+    MxTf32* mx = nullptr;             // SHT_PREC_FP32
 };
 
 namespace {
@@ -66,16 +68,9 @@ __global__ void unit_columns_kernel(float* x, int64_t ld, int K, int64_t first) 
     if (k < K) x[(int64_t)k * ld + first + k] = 1.f;
 }
 
-// field[k ldg + ij] *= s[ij]
-__global__ void scale_rows_kernel(float* f, int64_t ldg, int64_t npoints, int K, const float* __restrict__ s) {
-    const int k = blockIdx.y;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npoints; i += (int64_t)gridDim.x * blockDim.x)
-        f[(int64_t)k * ldg + i] *= s[i];
-}
-
 void release(sht_matrix* m) {
     if (m->tc) tc_matrix_destroy(m->tc);
-    if (m->blas) cublasDestroy(m->blas);
+    if (m->mx) mx_tf32_destroy(m->mx);
     void* ptrs[] = {m->d_F, m->d_B, m->d_row_scale, m->d_err};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -129,17 +124,16 @@ int build(sht_matrix* m) {
         return mcuda(e, "sht_matrix_create");
     if ((e = cudaMalloc(&m->d_err, sizeof(int32_t))) != cudaSuccess) return mcuda(e, "sht_matrix_create");
     cudaMemset(m->d_err, 0, sizeof(int32_t));
-    if (m->d.precision == SHT_PREC_FP32) {
-        if (cublasCreate(&m->blas) != CUBLAS_STATUS_SUCCESS) return mfail(SHT_ECUDA, "sht_matrix_create: cuBLAS");
-        cublasSetMathMode(m->blas, CUBLAS_PEDANTIC_MATH);     // FP32 products, no TF32
-        return SHT_OK;
-    }
     const float* a[2] = {m->d_F, m->d_B};
     const int depth[2] = {(int)np, (int)n2};
     const int M[2] = {(int)n2, (int)np};
-    if ((e = tc_matrix_create(&m->tc, m->d.precision, a, depth, M, m->d.nlayers)) != cudaSuccess)
+    if (m->d.precision == SHT_PREC_FP32) {
+        if ((e = mx_tf32_create(&m->mx, a, depth, M, m->d.nlayers)) != cudaSuccess)
+            return mcuda(e, "sht_matrix_create (TF32 matrices)");
+    } else if ((e = tc_matrix_create(&m->tc, m->d.precision, a, depth, M, m->d.nlayers)) != cudaSuccess) {
         return mcuda(e, "sht_matrix_create (tensor-core matrices)");
-    cudaFree(m->d_F);                 // the pieces replace the FP32 matrices
+    }
+    cudaFree(m->d_F);                 // the products' operands replace the unit-vector matrices
     cudaFree(m->d_B);
     m->d_F = m->d_B = nullptr;
     return SHT_OK;
@@ -188,20 +182,9 @@ int sht_matrix_synthesize(sht_matrix* m, const void* coeffs, int64_t ldc, float*
     DevGuard g(m->d.device);
     cudaStream_t s = (cudaStream_t)stream;
     const bool unscale = flags & SHT_UNSCALE_COSLAT;
-    if (m->tc) {
-        const cudaError_t e = tc_matrix_apply(m->tc, 1, (const float*)coeffs, 2 * ldc, grid, ldg, K,
-                                              unscale ? m->d_row_scale : nullptr, m->d_err, s);
-        return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_matrix_synthesize");
-    }
-    const float one = 1.f, zero = 0.f;
-    cublasSetStream(m->blas, s);
-    // field (col-major npoints x K, ld ldg) = B_r^T-view (npoints x 2 nlm, ld npoints) * coeffs (2 nlm x K)
-    if (cublasSgemm(m->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)m->npoints, K, (int)(2 * m->nlm), &one, m->d_B,
-                    (int)m->npoints, (const float*)coeffs, (int)(2 * ldc), &zero, grid, (int)ldg) !=
-        CUBLAS_STATUS_SUCCESS)
-        return mfail(SHT_ECUDA, "sht_matrix_synthesize: cuBLAS SGEMM");
-    if (unscale) scale_rows_kernel<<<dim3(64, K), 256, 0, s>>>(grid, ldg, m->npoints, K, m->d_row_scale);
-    const cudaError_t e = cudaGetLastError();
+    const float* rs = unscale ? m->d_row_scale : nullptr;
+    const cudaError_t e = m->mx ? mx_tf32_apply(m->mx, 1, (const float*)coeffs, 2 * ldc, grid, ldg, K, rs, m->d_err, s)
+                                : tc_matrix_apply(m->tc, 1, (const float*)coeffs, 2 * ldc, grid, ldg, K, rs, m->d_err, s);
     return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_matrix_synthesize");
 }
 
@@ -212,17 +195,9 @@ int sht_matrix_analyze(sht_matrix* m, const float* grid, int64_t ldg, void* coef
     if (flags) return mfail(SHT_EINVAL, "sht_matrix_analyze: takes no flags");
     DevGuard g(m->d.device);
     cudaStream_t s = (cudaStream_t)stream;
-    if (m->tc) {
-        const cudaError_t e = tc_matrix_apply(m->tc, 0, grid, ldg, (float*)coeffs, 2 * ldc, K, nullptr, m->d_err, s);
-        return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_matrix_analyze");
-    }
-    const float one = 1.f, zero = 0.f;
-    cublasSetStream(m->blas, s);
-    // coeffs (col-major 2 nlm x K, ld 2 ldc) = F^T-view (2 nlm x npoints, ld 2 nlm) * field (npoints x K)
-    if (cublasSgemm(m->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)(2 * m->nlm), K, (int)m->npoints, &one, m->d_F,
-                    (int)(2 * m->nlm), grid, (int)ldg, &zero, (float*)coeffs, (int)(2 * ldc)) != CUBLAS_STATUS_SUCCESS)
-        return mfail(SHT_ECUDA, "sht_matrix_analyze: cuBLAS SGEMM");
-    return SHT_OK;
+    const cudaError_t e = m->mx ? mx_tf32_apply(m->mx, 0, grid, ldg, (float*)coeffs, 2 * ldc, K, nullptr, m->d_err, s)
+                                : tc_matrix_apply(m->tc, 0, grid, ldg, (float*)coeffs, 2 * ldc, K, nullptr, m->d_err, s);
+    return e == cudaSuccess ? SHT_OK : mcuda(e, "sht_matrix_analyze");
 }
 
 int sht_matrix_device_status(sht_matrix* m, int32_t* status) {

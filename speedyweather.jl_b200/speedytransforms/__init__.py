@@ -11,7 +11,7 @@ SpeedyTransforms/src/spectral_gradients.jl) over the C ABI of libsht.so:
 * operators ``curl_``, ``divergence_``, ``UV_from_vor_``, ``UV_from_vordiv_``,
   ``laplace_`` (``∇²!``), ``inverse_laplace_`` (``∇⁻²!``), ``gradient_`` (``∇!``)
   and their allocating forms; ``Operators`` -- several of them in one kernel launch;
-* ``MatrixSpectralTransform`` -- the dense-matrix transforms (cuBLAS FP32 or tcgen05);
+* ``MatrixSpectralTransform`` -- the dense-matrix transforms (3xTF32 or split 16-bit, tcgen05);
 * ``Batch`` -- many transforms in one grouped launch per stage, CUDA-graph capture;
 * ``spec2grid_pullback_``, ``grid2spec_pullback_`` -- the adjoints of the transforms.
 

@@ -347,8 +347,9 @@ class SpectralTransform:
 class MatrixSpectralTransform:
     """Dense-matrix spectral transform (matrix_transform.jl:56-260):
     ``MatrixSpectralTransform(spectrum, grid, nlayers=K, precision="fp32")``; the
-    matrices are the transforms of unit vectors. "fp32" multiplies with cuBLAS SGEMM
-    (the reference's Float32 mul!), "bf16x3" / "fp16x3" / "bf16x5" on the tensor cores.
+    matrices are the transforms of unit vectors. "fp32" multiplies as three TF32 products
+    on the tensor cores (the reference's Float32 mul!, to FP32 rounding), "bf16x3" /
+    "fp16x3" / "bf16x5" as split 16-bit products.
     Used through ``transform_`` / ``transform`` like a SpectralTransform (no ``add``)."""
 
     def __init__(self, spectrum: Spectrum, grid: _GaussianGrid, *, nlayers: int = 1, LegendreShortcut: str = "linear",

@@ -1,12 +1,14 @@
 """MatrixSpectralTransform (sht_matrix_*): the transforms as dense products.
 
-The matrices are this library's FP32 transforms of unit vectors (matrix_transform.jl:134-173),
-so the FP32 products (cuBLAS SGEMM) agree with the SpectralTransform to FP32 rounding;
-the tensor-core products carry their split-precision error. Against the FP64 oracle:
-FP32 1e-5; every tensor-core form 3e-5 (relative L2). A dense product is one dot product
-of length npoints (analysis) or 2 nlm (synthesis) whose terms cancel heavily (the DFT and
-Legendre sums fused into one), accumulated in the tensor core's FP32: its error is ~1-2e-5
-at T31 whatever the operand split (the transform's FFT plus short Legendre sums stay lower)."""
+The matrices are this library's FP32 transforms of unit vectors (matrix_transform.jl:134-173).
+The FP32 form computes its products as three TF32 products on the tensor cores (the
+matrix split into TF32 pieces in shared memory, the leading product drained every 128
+deep into FP32 registers with rounding to nearest), so it agrees with the
+SpectralTransform to FP32 rounding; the split 16-bit forms carry their split error.
+Against the FP64 oracle: FP32 1e-5; every split 16-bit form 3e-5 (relative L2: one dot
+product of length npoints or 2 nlm whose terms cancel heavily, accumulated in 512-deep
+chunks in the tensor core's truncating FP32).
+"""
 import numpy as np
 import pytest
 
@@ -72,3 +74,26 @@ def test_matrix_unscale_and_single_layer(st, prec):
     assert O.rel_err(np_of(f), ref) < TOL[prec]
     with pytest.raises(TypeError):
         st.transform_(st.Field.zeros(S.grid, 1), to_lta(st, S, c), M, add=True)
+
+
+def test_matrix_fp32_layer_tiles_and_determinism(st):
+    """70 layers (two column tiles of 64) against the oracle; a second call gives the same
+    bits; a 5-layer call gives the bits of the first 5 layers of the 70-layer call (each
+    layer's sums run in the same fixed order whatever K)."""
+    import torch
+    M = matrix(st, 31, "full", 24, 70, "fp32")
+    S, So = setup(st, 31, "full", 70, nh=24)
+    c = O.random_coeffs(So.spectrum, 70, seed=21)
+    lt = to_lta(st, S, c)
+    f1, f2 = st.transform(lt, M), st.transform(lt, M)
+    assert M.device_status() == 0
+    assert torch.equal(f1.data, f2.data)
+    ref = So.synthesize(c)
+    assert O.rel_err(np_of(f1), ref) < TOL["fp32"]
+    f5 = st.transform(st.LowerTriangularArray(lt.data[:5].contiguous(), S.spectrum), M)
+    assert torch.equal(f5.data, f1.data[:5])
+    g = ref.astype(np.float32)
+    a1, a2 = st.transform(to_field(st, S, g), M), st.transform(to_field(st, S, g), M)
+    assert M.device_status() == 0
+    assert torch.equal(a1.data, a2.data)
+    assert O.rel_err(np_of(a1), So.analyze(g.astype(np.float64))) < TOL["fp32"]
