@@ -331,6 +331,12 @@ def run_mixed_batch(args):
     t_each = timed(b.run_each)
     t_grouped = timed(b.run)
     t_graph = timed(b.launch)
+    plans = [e[2] for e in entries[::2]]
+    for S in plans:                          # the per-call sequence with the fused kernels
+        S.fusion = S.fusion_available
+    t_each_fused = timed(b.run_each)
+    for S in plans:
+        S.fusion = False
     line = {"metric": "mixed-batch round trips/s (octahedral T31 K1 + T63 K8 + T127 K16 + T255 K64, FP32)",
             "value": 1.0 / t_graph, "unit": "batches/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_graph * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -338,8 +344,80 @@ def run_mixed_batch(args):
             "config": {"workload": "mixed batch of 4 round trips, one grouped launch per stage, CUDA graph",
                        "legendre_tile_columns": bn},
             "ms_per_batch": {"one_call_per_transform": t_each * 1e3, "grouped_launches": t_grouped * 1e3,
-                             "grouped_graph": t_graph * 1e3},
-            "gpu_launches_per_batch": {"one_call_per_transform": 16, "grouped_launches": 4, "grouped_graph": 4}}
+                             "grouped_graph": t_graph * 1e3,
+                             "one_fused_call_per_transform": t_each_fused * 1e3},
+            "gpu_launches_per_batch": {"one_call_per_transform": 16, "grouped_launches": 4, "grouped_graph": 4,
+                                       "one_fused_call_per_transform": 8}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_fused(args):
+    """Fused transforms (the FFT and Legendre stages in one launch per direction,
+    thread-block clusters passing the Fourier rows through shared memory) beside the
+    separate kernels, FP32, at T31 on the full Gaussian grid with nlat 48 x 8 layers,
+    T63 octahedral nlat 96 x 8, T127 octahedral nlat 192 x 48 (8 layers x 6 fields) and
+    x 8. Per case: one synthesis and one analysis call timed eagerly with CUDA events,
+    and the round trip replayed from a CUDA graph of 20 round trips. Prints one JSON line
+    (not the headline metric)."""
+    import torch
+    import speedytransforms as st
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sht_oracle as O
+    cases = [("T31 full nlat 48 x 8", 31, True, 24, 8), ("T63 octahedral nlat 96 x 8", 63, False, 48, 8),
+             ("T127 octahedral nlat 192 x 48", 127, False, 96, 48), ("T127 octahedral nlat 192 x 8", 127, False, 96, 8),
+             ("T63 full nlat 96 x 8", 63, True, 48, 8), ("T127 full nlat 192 x 8", 127, True, 96, 8),
+             ("T31 full nlat 48 x 48", 31, True, 24, 48)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, n):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(n):
+            fn()
+        ev[1].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / n * 1e3
+    res = {}
+    for name, T_, full, nh, K in cases:
+        grid = st.FullGaussianGrid(nh) if full else st.OctahedralGaussianGrid(nh)
+        S = st.SpectralTransform(st.Spectrum(T_ + 1, T_), grid, nlayers=K, precision="fp32")
+        c = O.random_coeffs(O.Spectrum(T_ + 1, T_), K, seed=1)
+        lt = st.LowerTriangularArray(torch.tensor(np.ascontiguousarray(c.T), dtype=torch.complex64, device="cuda"),
+                                     S.spectrum)
+        f, a = st.Field.zeros(grid, K), st.LowerTriangularArray.zeros(S.spectrum, K)
+        r = {"fused_available": S.fusion_available}
+        for fused in ([False, True] if S.fusion_available else [False]):
+            S.fusion = fused
+            syn = timed(lambda: st.transform_(f, lt, S), args.steps)
+            ana = timed(lambda: st.transform_(a, f, S), args.steps)
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                for _ in range(3):
+                    st.transform_(f, lt, S)
+                    st.transform_(a, f, S)
+            torch.cuda.current_stream().wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                for _ in range(20):
+                    st.transform_(f, lt, S)
+                    st.transform_(a, f, S)
+            rt = timed(g.replay, max(3, args.steps // 20)) / 20
+            del g
+            r["fused" if fused else "separate"] = {"synthesis_us": syn, "analysis_us": ana, "graph_round_trip_us": rt}
+        S.fusion = False
+        assert S.device_status() == 0
+        res[name] = r
+    line = {"metric": "fused vs separate FFT + Legendre stages, FP32 round trip (graph-replayed), microseconds",
+            "value": res["T31 full nlat 48 x 8"].get("fused", {}).get("graph_round_trip_us"), "unit": "us",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "fused transforms at the small truncations",
+                       "gpu_launches_per_round_trip": {"separate": 4, "fused": 2}},
+            "by_case": res}
     print(json.dumps(line))
     return 0
 
@@ -878,7 +956,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="t511",
-                    choices=["t511", "mixed-batch", "column-emulator", "dycore-step", "operators", "matrix"],
+                    choices=["t511", "mixed-batch", "column-emulator", "dycore-step", "operators", "matrix", "fused"],
                     help="t511: the headline benchmark; mixed-batch: the grouped-launch comparison; "
                          "column-emulator: the MLP parameterization at T63; dycore-step: one time step's "
                          "transforms at T63 L8, eager and as a CUDA graph; operators: the spectral "
@@ -901,6 +979,8 @@ def main():
         return run_column_emulator(args)
     if args.workload == "dycore-step":
         return run_dycore_step(args)
+    if args.workload == "fused":
+        return run_fused(args)
     if args.workload == "matrix":
         return run_matrix(args)
     if args.workload == "operators":

@@ -261,6 +261,23 @@ SHT_API int sht_analyze_adjoint(sht_plan* plan, const void* coeffs_bar, int64_t 
  * return SHT_OK with tile_columns = {0, 0}. No counterpart in the reference. */
 SHT_API int sht_plan_autotune(sht_plan* plan, int K, void* stream, int32_t* tile_columns);
 
+/* Fused transforms: the Fourier and Legendre stages of sht_synthesize / sht_analyze in
+ * one launch per direction, for SHT_PREC_FP32 plans whose per-cluster data fits in
+ * shared memory (the small truncations). A thread-block cluster of up to 16 CTAs takes
+ * a chunk of layers and passes the Fourier rows between the stages through its CTAs'
+ * shared memory instead of the plan's global scratch. Same bits as the separate kernels.
+ * Replaces the two-stage data flow of SpeedyTransforms/src/spectral_transform.jl:551-570
+ * (synthesis: _legendre! -> scratch -> _fourier!) and :612-631 (analysis).
+ * A new plan starts fused where that measured faster on B200 (full Gaussian grids up to
+ * nlat 64), else with the separate kernels.
+ * sht_plan_set_fusion: mode SHT_FUSION_OFF or SHT_FUSION_ON (SHT_EUNSUPPORTED for a plan
+ * that cannot be fused: tensor-core precisions, or too large). sht_plan_get_fusion:
+ * the plan's mode and whether SHT_FUSION_ON is possible (either pointer may be NULL). */
+#define SHT_FUSION_OFF 0
+#define SHT_FUSION_ON 1
+SHT_API int sht_plan_set_fusion(sht_plan* plan, int mode);
+SHT_API int sht_plan_get_fusion(const sht_plan* plan, int32_t* mode, int32_t* available);
+
 /* ---- batches: many transforms (different plans, truncations, layer counts) in one
  * grouped launch per stage, optionally captured as one CUDA graph ---------------------
  * replaces the per-transform launch sequences of a time step

@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 
@@ -897,6 +898,396 @@ __global__ void __launch_bounds__(kFftGroupThreads, kFftCtasPerSm) fft_grouped_k
     }
 }
 
+// ---------------------------------------------------------------- fused transforms
+// FFT and Legendre stage in one launch per direction, for FP32 plans whose per-cluster
+// data fits in shared memory (the small truncations). A thread-block cluster of P CTAs
+// handles one chunk of C layers; CTA `rank` owns the orders m = rank + P ml and the
+// rings j = rank + P jl. The E/O Fourier rows pass between the two stages through the
+// CTAs' shared memory (distributed shared memory within the cluster) instead of the
+// global scratch:
+//   synthesis  Legendre sums of my orders on every ring -> cluster barrier -> each of my
+//              rings gathers its rows from the owners of its orders -> pack, FFT, store
+//   analysis   FFT of my rings -> E/O rows of every order -> cluster barrier -> each of
+//              my orders gathers its rows from the owners of the rings -> sums over the
+//              rings in ring order
+// Every value is computed with the same operations in the same order as by the separate
+// Legendre and Fourier kernels (the Legendre sums are fma chains over l, resp. over the
+// rings from j0(m) on; the FFT code is shared), so the two paths give the same bits.
+
+__device__ __forceinline__ uint32_t cl_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cl_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// the float2 at the same shared-memory offset as p in the CTA of the cluster with rank r
+__device__ __forceinline__ float2 cl_load(const float2* p, int r) {
+    uint32_t a = (uint32_t)__cvta_generic_to_shared(p), b;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(b) : "r"(a), "r"(r));
+    float2 v;
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(b) : "memory");
+    return v;
+}
+
+constexpr int kFusedMaxC = 8;          // layers per cluster (register accumulators per thread)
+
+__global__ void __launch_bounds__(kFftThreads, 1) fused_synthesis_kernel(const FusedView v) {
+    extern __shared__ float2 sm[];
+    const int P = v.P, rank = (int)cl_rank(), nh = v.nh;
+    const int k0 = (blockIdx.x / P) * v.C;
+    const int C = min(v.C, v.K - k0);
+    float2* EOS = sm;                                             // [ml][j][p][c], stride v.C
+    float2* TW = sm + (int64_t)v.nm_cta * nh * 2 * v.C;           // [jl][tw_max]: my rings' tables
+    float2* X = TW + (int64_t)v.nr_cta * v.tw_max;
+    float2* Y = X + (v.uniform ? v.nr_cta : 1) * v.C * v.ldx;
+    // twiddles and prime tables of my rings, fetched while the Legendre sums run
+    for (int j = rank, jl = 0; j < nh; j += P, ++jl) {
+        const RingDesc& rd = v.rings[j];
+        copy_twiddles_async(TW + (int64_t)jl * v.tw_max, v.twiddle + rd.tw_off, smem_tw_len(rd.n) + rd.gen_len);
+    }
+    // Legendre sums of my orders on every ring that carries them: a thread takes four
+    // consecutive rings (one 16-byte load of Lambda per degree) and the C layers
+    const int nj4 = (nh + 3) / 4;
+    for (int w = threadIdx.x; w < v.nm_cta * 2 * nj4; w += blockDim.x) {
+        const int j4 = w % nj4, mp = w / nj4, p = mp & 1, ml = mp >> 1;
+        const int m = rank + P * ml;
+        if (m >= v.mmax || 4 * j4 + 3 < v.j0[m]) continue;
+        const int rows = v.rows[m];
+        const int ni = min(rows, (v.lmax - m - p + 1) / 2);          // degrees l = m + 2 i + p < lmax
+        const float4* L = reinterpret_cast<const float4*>(v.lam + v.lam_off[m] + (int64_t)p * rows * v.nh_pad) + j4;
+        const int64_t ls = v.nh_pad / 4;
+        const float2* cb = v.cin + (int64_t)k0 * v.ldc + v.lm_off[m] + p;
+        float ar[4][kFusedMaxC], ai[4][kFusedMaxC];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int c = 0; c < kFusedMaxC; ++c) ar[q][c] = ai[q][c] = 0.f;
+        int i = 0;
+        for (; i + 4 <= ni; i += 4) {
+            float4 lam[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) lam[u] = __ldg(L + (int64_t)(i + u) * ls);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float lq[4] = {lam[u].x, lam[u].y, lam[u].z, lam[u].w};
+#pragma unroll
+                for (int c = 0; c < kFusedMaxC; ++c) {
+                    if (c < C) {
+                        const float2 x = __ldg(cb + (int64_t)c * v.ldc + 2 * (i + u));
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            ar[q][c] = fmaf(lq[q], x.x, ar[q][c]);
+                            ai[q][c] = fmaf(lq[q], x.y, ai[q][c]);
+                        }
+                    }
+                }
+            }
+        }
+        for (; i < ni; ++i) {
+            const float4 l4 = __ldg(L + (int64_t)i * ls);
+            const float lq[4] = {l4.x, l4.y, l4.z, l4.w};
+#pragma unroll
+            for (int c = 0; c < kFusedMaxC; ++c) {
+                if (c < C) {
+                    const float2 x = __ldg(cb + (int64_t)c * v.ldc + 2 * i);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        ar[q][c] = fmaf(lq[q], x.x, ar[q][c]);
+                        ai[q][c] = fmaf(lq[q], x.y, ai[q][c]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = 4 * j4 + q;
+            if (j < v.j0[m] || j >= nh) continue;
+            float2* e = EOS + ((int64_t)(ml * nh + j) * 2 + p) * v.C;
+#pragma unroll
+            for (int c = 0; c < kFusedMaxC; ++c)
+                if (c < C) e[c] = make_float2(ar[q][c], ai[q][c]);
+        }
+    }
+    cp_async_wait_all();
+    cl_sync();
+    if (v.uniform) {
+        // rings of one length (full grids): all my rings in one FFT, columns jl C + c
+        const int R = rank < nh ? (nh - 1 - rank) / P + 1 : 0;
+        if (R > 0) {
+            const RingDesc& r0 = v.rings[rank];
+            const int n = r0.n, ldx = v.ldx, CC = R * C, nrow = 2 * (r0.mt + 1);
+            const float2* W = TW;
+            const float2* G = W + smem_tw_len(n);
+            for (int w = threadIdx.x; w < nrow * CC; w += blockDim.x) {
+                const int r = w / CC, cc = w - r * CC, jl = cc / C, c = cc - jl * C, m = r >> 1, p = r & 1;
+                const int j = rank + P * jl;
+                Y[r * CC + cc] = cl_load(EOS + ((int64_t)((m / P) * nh + j) * 2 + p) * v.C + c, m % P);
+            }
+            __syncthreads();
+            const int nhalf = n / 2;
+            for (int w = threadIdx.x; w < CC * (nhalf + 1); w += blockDim.x) {
+                const int m = w / CC, cc = w - m * CC;
+                const RingDesc& rd = v.rings[rank + P * (cc / C)];
+                float2 e = make_float2(0.f, 0.f), o = e;
+                if (m <= rd.mt) {
+                    e = Y[2 * m * CC + cc];
+                    o = Y[(2 * m + 1) * CC + cc];
+                }
+                const float scale = syn_weight(rd, m, 0, v.unscale);
+                const float2 gn = make_float2(__fmul_rn(scale, e.x + o.x), __fmul_rn(scale, e.y + o.y));
+                const float2 gs = make_float2(__fmul_rn(scale, e.x - o.x), __fmul_rn(scale, e.y - o.y));
+                if (m == 0 || 2 * m == n) {
+                    X[cc * ldx + m] = make_float2(gn.x, gs.x);
+                } else {
+                    X[cc * ldx + m] = make_float2(gn.x - gs.y, gn.y + gs.x);
+                    X[cc * ldx + (n - m)] = make_float2(gn.x + gs.y, gs.x - gn.y);
+                }
+            }
+            __syncthreads();
+            const float2* z = run_fft<true>(X, Y, n, ldx, CC, r0, W, G);
+            const Div dn = mkdiv(n);
+            for (int jl = 0; jl < R; ++jl) {
+                const RingDesc& rd = v.rings[rank + P * jl];
+                store_rings(v.gout, v.ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn, z + jl * C * ldx, v.add);
+            }
+        }
+        cl_sync();
+        return;
+    }
+    // my rings one after another: gather the rows, pack, FFT, store
+    for (int j = rank; j < nh; j += P) {
+        const RingDesc& rd = v.rings[j];
+        const int n = rd.n, ldx = v.ldx;
+        const float2* W = TW + (int64_t)(j / P) * v.tw_max;
+        const float2* G = W + smem_tw_len(n);
+        __syncthreads();                                          // the previous ring is done
+        const int nrow = 2 * (rd.mt + 1);
+        for (int w = threadIdx.x; w < nrow * C; w += blockDim.x) {
+            const int r = w / C, c = w - r * C, m = r >> 1, p = r & 1;
+            Y[r * C + c] = cl_load(EOS + ((int64_t)((m / P) * nh + j) * 2 + p) * v.C + c, m % P);
+        }
+        __syncthreads();
+        const int nhalf = n / 2;
+        for (int w = threadIdx.x; w < C * (nhalf + 1); w += blockDim.x) {
+            const int m = w / C, c = w - m * C;
+            float2 e = make_float2(0.f, 0.f), o = e;
+            if (m <= rd.mt) {
+                e = Y[2 * m * C + c];
+                o = Y[(2 * m + 1) * C + c];
+            }
+            const float scale = syn_weight(rd, m, 0, v.unscale);
+            const float2 gn = make_float2(__fmul_rn(scale, e.x + o.x), __fmul_rn(scale, e.y + o.y));
+            const float2 gs = make_float2(__fmul_rn(scale, e.x - o.x), __fmul_rn(scale, e.y - o.y));
+            if (m == 0 || 2 * m == n) {
+                X[c * ldx + m] = make_float2(gn.x, gs.x);
+            } else {
+                X[c * ldx + m] = make_float2(gn.x - gs.y, gn.y + gs.x);
+                X[c * ldx + (n - m)] = make_float2(gn.x + gs.y, gs.x - gn.y);
+            }
+        }
+        __syncthreads();
+        const float2* z = run_fft<true>(X, Y, n, ldx, C, rd, W, G);
+        store_rings(v.gout, v.ldg, rd.off_north, rd.off_south, k0, C, n, ldx, mkdiv(n), z, v.add);
+    }
+    cl_sync();                                                    // my rows stay until all gathered
+}
+
+__global__ void __launch_bounds__(kFftThreads, 1) fused_analysis_kernel(const FusedView v) {
+    extern __shared__ float2 sm[];
+    const int P = v.P, rank = (int)cl_rank(), nh = v.nh;
+    const int k0 = (blockIdx.x / P) * v.C;
+    const int C = min(v.C, v.K - k0);
+    const int nmr = v.mt_max + 1;
+    float2* EOA = sm;                                             // [jl][m][p][c], stride v.C
+    float2* TW = sm + (int64_t)v.nr_cta * nmr * 2 * v.C;          // [jl][tw_max]: my rings' tables
+    float2* X = TW + (int64_t)v.nr_cta * v.tw_max;
+    float2* Y = X + (v.uniform ? v.nr_cta : 1) * v.C * v.ldx;
+    float2* EOM = TW;                                             // [ml][j][p][c] after the FFTs
+    for (int j = rank, jl = 0; j < nh; j += P, ++jl) {
+        const RingDesc& rd = v.rings[j];
+        copy_twiddles_async(TW + (int64_t)jl * v.tw_max, v.twiddle + rd.tw_off, smem_tw_len(rd.n) + rd.gen_len);
+    }
+    // FFT of my rings and their E/O rows (the arithmetic of fft_analysis_body)
+    if (v.uniform && rank < nh) {
+        // rings of one length (full grids): all my rings in one FFT, columns jl C + c
+        const int R = (nh - 1 - rank) / P + 1;
+        const RingDesc& r0 = v.rings[rank];
+        const int n = r0.n, ldx = v.ldx, CC = R * C, n4 = n >> 2;
+        const float2* W = TW;
+        const float2* G = W + smem_tw_len(n);
+        bool avec = ((v.ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(v.gin) & 15) == 0) && ((n & 3) == 0);
+        for (int jl = 0; jl < R; ++jl) {
+            const RingDesc& rd = v.rings[rank + P * jl];
+            avec = avec && ((rd.off_north & 3) == 0) && ((rd.off_south & 3) == 0);
+        }
+        const bool raw_first = avec && r0.nfac > 0;
+        float2* const land = raw_first ? X : Y;
+        if (avec) {
+            const Div d2n4 = mkdiv(2 * n4);
+            for (int w = threadIdx.x; w < CC * 2 * n4; w += blockDim.x) {
+                const int cc = quo(w, d2n4);
+                const int r = w - cc * 2 * n4;
+                const int hs = r >= n4 ? 1 : 0;
+                const int i4 = r - hs * n4;
+                const int jl = cc / C, c = cc - jl * C;
+                const RingDesc& rd = v.rings[rank + P * jl];
+                const float* src = v.gin + (int64_t)(k0 + c) * v.ldg + (hs ? rd.off_south : rd.off_north) + 4 * i4;
+                cp_async16(reinterpret_cast<float*>(land + cc * ldx) + hs * n + 4 * i4, src);
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        if (raw_first) {
+        } else if (avec) {
+            const Div dn4 = mkdiv(n4);
+            for (int w = threadIdx.x; w < CC * n4; w += blockDim.x) {
+                const int cc = quo(w, dn4);
+                const int i4 = w - cc * n4;
+                const float* raw = reinterpret_cast<const float*>(Y + cc * ldx);
+                const float4 a = reinterpret_cast<const float4*>(raw)[i4];
+                const float4 b = reinterpret_cast<const float4*>(raw + n)[i4];
+                float4* x = reinterpret_cast<float4*>(X + cc * ldx + 4 * i4);
+                x[0] = make_float4(a.x, b.x, a.y, b.y);
+                x[1] = make_float4(a.z, b.z, a.w, b.w);
+            }
+        } else {
+            for (int jl = 0; jl < R; ++jl) {
+                const RingDesc& rd = v.rings[rank + P * jl];
+                load_rings(X + jl * C * ldx, v.gin, v.ldg, rd.off_north, rd.off_south, k0, C, n, ldx, mkdiv(n));
+            }
+        }
+        if (!raw_first) __syncthreads();
+        const float2* Z = run_fft<false>(X, Y, n, ldx, CC, r0, W, G, raw_first);
+        const int nm = r0.mt + 1;
+        for (int w = threadIdx.x; w < CC * nm; w += blockDim.x) {
+            const int m = w / CC, cc = w - m * CC, jl = cc / C, c = cc - jl * C;
+            const RingDesc& rd = v.rings[rank + P * jl];
+            const float2 a = Z[cc * ldx + m];
+            const float2 b = Z[cc * ldx + (m == 0 ? 0 : n - m)];
+            const float2 fn = make_float2(a.x + b.x, a.y - b.y);
+            const float2 fs = make_float2(a.y + b.y, b.x - a.x);
+            const float hw = ana_weight(rd, m, 0, 0);
+            float2* eo = EOA + ((int64_t)(jl * nmr + m) * 2) * v.C + c;
+            eo[0] = make_float2(__fmul_rn(hw, fn.x + fs.x), __fmul_rn(hw, fn.y + fs.y));
+            eo[v.C] = make_float2(__fmul_rn(hw, fn.x - fs.x), __fmul_rn(hw, fn.y - fs.y));
+        }
+    }
+    for (int j = rank, jl = 0; j < nh && !v.uniform; j += P, ++jl) {
+        const RingDesc& rd = v.rings[j];
+        const int n = rd.n, ldx = v.ldx;
+        const float2* W = TW + (int64_t)jl * v.tw_max;
+        const float2* G = W + smem_tw_len(n);
+        __syncthreads();
+        const bool avec = ((v.ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(v.gin) & 15) == 0) &&
+                          ((rd.off_north & 3) == 0) && ((rd.off_south & 3) == 0) && ((n & 3) == 0);
+        const bool raw_first = avec && rd.nfac > 0;
+        float2* const land = raw_first ? X : Y;
+        const int n4 = n >> 2;
+        if (avec) {
+            const Div d2n4 = mkdiv(2 * n4);
+            for (int w = threadIdx.x; w < C * 2 * n4; w += blockDim.x) {
+                const int c = quo(w, d2n4);
+                const int r = w - c * 2 * n4;
+                const int hs = r >= n4 ? 1 : 0;
+                const int i4 = r - hs * n4;
+                const float* src = v.gin + (int64_t)(k0 + c) * v.ldg + (hs ? rd.off_south : rd.off_north) + 4 * i4;
+                cp_async16(reinterpret_cast<float*>(land + c * ldx) + hs * n + 4 * i4, src);
+            }
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        if (raw_first) {
+        } else if (avec) {
+            const Div dn4 = mkdiv(n4);
+            for (int w = threadIdx.x; w < C * n4; w += blockDim.x) {
+                const int c = quo(w, dn4);
+                const int i4 = w - c * n4;
+                const float* raw = reinterpret_cast<const float*>(Y + c * ldx);
+                const float4 a = reinterpret_cast<const float4*>(raw)[i4];
+                const float4 b = reinterpret_cast<const float4*>(raw + n)[i4];
+                float4* x = reinterpret_cast<float4*>(X + c * ldx + 4 * i4);
+                x[0] = make_float4(a.x, b.x, a.y, b.y);
+                x[1] = make_float4(a.z, b.z, a.w, b.w);
+            }
+        } else {
+            load_rings(X, v.gin, v.ldg, rd.off_north, rd.off_south, k0, C, n, ldx, mkdiv(n));
+        }
+        if (!raw_first) __syncthreads();
+        const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G, raw_first);
+        const int nm = rd.mt + 1;
+        for (int w = threadIdx.x; w < C * nm; w += blockDim.x) {
+            const int m = w / C, c = w - m * C;
+            const float2 a = Z[c * ldx + m];
+            const float2 b = Z[c * ldx + (m == 0 ? 0 : n - m)];
+            const float2 fn = make_float2(a.x + b.x, a.y - b.y);
+            const float2 fs = make_float2(a.y + b.y, b.x - a.x);
+            const float hw = ana_weight(rd, m, 0, 0);
+            float2* eo = EOA + ((int64_t)(jl * nmr + m) * 2) * v.C + c;
+            eo[0] = make_float2(__fmul_rn(hw, fn.x + fs.x), __fmul_rn(hw, fn.y + fs.y));
+            eo[v.C] = make_float2(__fmul_rn(hw, fn.x - fs.x), __fmul_rn(hw, fn.y - fs.y));
+        }
+    }
+    cl_sync();
+    // my orders' rows from every ring that carries them
+    __syncthreads();
+    for (int w = threadIdx.x; w < v.nm_cta * nh * 2 * C; w += blockDim.x) {
+        const int c = w % C, r = w / C, p = r & 1, mj = r >> 1, j = mj % nh, ml = mj / nh;
+        const int m = rank + P * ml;
+        if (m >= v.mmax || j < v.j0[m]) continue;
+        EOM[((int64_t)(ml * nh + j) * 2 + p) * v.C + c] =
+            cl_load(EOA + ((int64_t)((j / P) * nmr + m) * 2 + p) * v.C + c, j % P);
+    }
+    cl_sync();                                                    // every gather done: no remote reads follow
+    // Legendre sums over the rings j0(m) .. nh - 1, in ring order, for my orders
+    const int rmax = (v.lmax + 1) / 2;
+    for (int w = threadIdx.x; w < v.nm_cta * 2 * rmax; w += blockDim.x) {
+        const int i = w % rmax, mp = w / rmax, p = mp & 1, ml = mp >> 1;
+        const int m = rank + P * ml;
+        if (m >= v.mmax) continue;
+        const int rows = v.rows[m];
+        if (i >= rows || m + 2 * i + p >= v.lmax) continue;
+        const float* L = v.lam + v.lam_off[m] + ((int64_t)p * rows + i) * v.nh_pad;
+        const float2* eo = EOM + ((int64_t)ml * nh * 2 + p) * v.C;
+        float ar[kFusedMaxC], ai[kFusedMaxC];
+#pragma unroll
+        for (int c = 0; c < kFusedMaxC; ++c) ar[c] = ai[c] = 0.f;
+        // rings j0(m) .. nh - 1 in order; Lambda four rings per 16-byte load
+        const int jb = v.j0[m] & ~3;
+        for (int j4 = jb; j4 < nh; j4 += 4) {
+            const float4 l4 = __ldg(reinterpret_cast<const float4*>(L + j4));
+            const float lq[4] = {l4.x, l4.y, l4.z, l4.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = j4 + q;
+                if (j < v.j0[m] || j >= nh) continue;
+#pragma unroll
+                for (int c = 0; c < kFusedMaxC; ++c) {
+                    if (c < C) {
+                        const float2 x = eo[(int64_t)j * 2 * v.C + c];
+                        ar[c] = fmaf(lq[q], x.x, ar[c]);
+                        ai[c] = fmaf(lq[q], x.y, ai[c]);
+                    }
+                }
+            }
+        }
+        float2* dst = v.cout + (int64_t)k0 * v.ldc + v.lm_off[m] + 2 * i + p;
+#pragma unroll
+        for (int c = 0; c < kFusedMaxC; ++c) {
+            if (c < C) {
+                float2 x = make_float2(ar[c], ai[c]);
+                if (v.add) {
+                    const float2 o = dst[(int64_t)c * v.ldc];
+                    x.x += o.x;
+                    x.y += o.y;
+                }
+                dst[(int64_t)c * v.ldc] = x;
+            }
+        }
+    }
+}
+
 }  // namespace
 
 static int fft_threads(const Plan&) { return kFftThreads; }
@@ -974,6 +1365,167 @@ cudaError_t fft_set_smem(int bytes) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(fft_synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) current[dev] = bytes;
     return e;
+}
+
+namespace {
+// Layers per cluster of one call: enough that every cluster runs at once (no second
+// wave), and at least one CTA per SM's share of the layers.
+int fused_layers(const Plan& p, int K) {
+    const int once = (K + p.fused_ncl - 1) / p.fused_ncl;
+    const int fill = (K * p.fused_P + p.nsm - 1) / p.nsm;
+    return std::max(1, std::min(p.fused_cmax, std::min(std::max(once, fill), K)));
+}
+int fused_smem(const Plan& p, bool syn, int C) {
+    const int nm_cta = (p.mmax + p.fused_P - 1) / p.fused_P, nr_cta = (p.nh + p.fused_P - 1) / p.fused_P;
+    const int64_t work = (int64_t)nr_cta * p.fused_tw_max + 2LL * C * p.fused_ldx * (p.fused_uniform ? nr_cta : 1);
+    const int64_t eos = (int64_t)nm_cta * p.nh * 2 * C;
+    const int64_t f2 = syn ? eos + work : (int64_t)nr_cta * (p.fused_mt_max + 1) * 2 * C + std::max(work, eos);
+    return (int)(f2 * (int64_t)sizeof(float2));
+}
+FusedView fused_view(const Plan& p, int K, int C) {
+    FusedView v{};
+    v.rings = p.d_rings;
+    v.twiddle = p.d_twiddle;
+    v.lam = p.d_lam;
+    v.lam_off = p.d_lam_off;
+    v.rows = p.d_rows;
+    v.j0 = p.d_j0;
+    v.lm_off = p.d_lm_off;
+    v.nh = p.nh;
+    v.nh_pad = p.nh_pad;
+    v.lmax = p.lmax;
+    v.mmax = p.mmax;
+    v.mt_max = p.fused_mt_max;
+    v.K = K;
+    v.C = C;
+    v.P = p.fused_P;
+    v.nm_cta = (p.mmax + p.fused_P - 1) / p.fused_P;
+    v.nr_cta = (p.nh + p.fused_P - 1) / p.fused_P;
+    v.ldx = p.fused_ldx;
+    v.tw_max = p.fused_tw_max;
+    v.uniform = p.fused_uniform;
+    return v;
+}
+cudaError_t fused_launch(const Plan& p, bool syn, const FusedView& v, cudaStream_t s) {
+    const int ncl = (v.K + v.C - 1) / v.C;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(v.P * ncl);
+    cfg.blockDim = dim3(kFftThreads);
+    cfg.dynamicSmemBytes = fused_smem(p, syn, v.C);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = v.P;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return syn ? cudaLaunchKernelEx(&cfg, fused_synthesis_kernel, v) : cudaLaunchKernelEx(&cfg, fused_analysis_kernel, v);
+}
+}  // namespace
+
+// Launch shape of the fused kernels: the cluster size (16 or 8 CTAs) with more CTAs
+// resident at once (cudaOccupancyMaxActiveClusters), and the most layers per cluster
+// (<= 8) whose shared memory fits one CTA per SM. Tensor-core plans, and plans too large
+// for one layer per cluster, keep the separate kernels (fusion_ok = 0). A CTA transforms
+// its rings one after another, unless all rings have one length (full grids): then in
+// one FFT call with rings x layers as its columns.
+cudaError_t fused_prepare(Plan& p) {
+    p.fusion_ok = 0;
+    p.fusion = 0;
+    if (p.tc) return cudaSuccess;
+    int dev = 0, nsm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    p.nsm = std::max(1, nsm);
+    int ldx = 2, tw = 0, mtm = 0;
+    for (const RingDesc& r : p.h_rings) {
+        const int base = std::max(r.n, 2 * (r.mt + 1));
+        ldx = std::max(ldx, base + (((2 - base) % 16) + 16) % 16);
+        tw = std::max(tw, ((r.n + 1) & ~1) + r.gen_len);
+        mtm = std::max(mtm, r.mt);
+    }
+    p.fused_ldx = ldx;
+    p.fused_tw_max = tw;
+    p.fused_mt_max = mtm;
+    p.fused_uniform = 1;                              // every ring of one length and truncation
+    for (const RingDesc& r : p.h_rings)
+        if (r.n != p.h_rings[0].n || r.mt != p.h_rings[0].mt) p.fused_uniform = 0;
+    const int budget = 227 * 1024;
+    const void* ks[2] = {(const void*)fused_synthesis_kernel, (const void*)fused_analysis_kernel};
+    for (const void* k : ks) {
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, budget)) != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess) return e;
+    }
+    int best_P = 0, best_c = 0, best_ncl = 0;
+    for (int P : {16, 8}) {
+        p.fused_P = std::max(1, std::min(P, p.nh));
+        int cmax = 0;
+        for (int C = kFusedMaxC; C >= 1; --C)
+            if (fused_smem(p, true, C) <= budget && fused_smem(p, false, C) <= budget) {
+                cmax = C;
+                break;
+            }
+        if (cmax == 0) continue;
+        int ncl = 1 << 30;
+        for (int d = 0; d < 2; ++d) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(p.fused_P);
+            cfg.blockDim = dim3(kFftThreads);
+            cfg.dynamicSmemBytes = fused_smem(p, d == 0, cmax);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = p.fused_P;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, ks[d], &cfg) != cudaSuccess) {
+                cudaGetLastError();
+                n = 0;
+            }
+            ncl = std::min(ncl, n);
+        }
+        if (ncl >= 1 && ncl * p.fused_P > best_ncl * best_P) {
+            best_P = p.fused_P;
+            best_c = cmax;
+            best_ncl = ncl;
+        }
+    }
+    if (best_P == 0) return cudaSuccess;              // does not fit: separate kernels
+    p.fused_P = best_P;
+    p.fused_cmax = best_c;
+    p.fused_ncl = best_ncl;
+    p.fusion_ok = 1;
+    // on by default where it measured faster than the separate kernels on B200: full
+    // grids (one FFT per CTA for all its rings) up to nlat 64
+    p.fusion = p.fused_uniform && p.nlat <= 64 ? 1 : 0;
+    return cudaSuccess;
+}
+
+cudaError_t launch_fused_synthesis(const Plan& p, const float2* coeffs, int64_t ldc, float* grid, int64_t ldg, int K,
+                                   unsigned flags, cudaStream_t s) {
+    FusedView v = fused_view(p, K, fused_layers(p, K));
+    v.cin = coeffs;
+    v.ldc = ldc;
+    v.gout = grid;
+    v.ldg = ldg;
+    v.unscale = (flags & SHT_UNSCALE_COSLAT) ? 1 : 0;
+    v.add = (flags & SHT_ADD) ? 1 : 0;
+    return fused_launch(p, true, v, s);
+}
+
+cudaError_t launch_fused_analysis(const Plan& p, const float* grid, int64_t ldg, float2* coeffs, int64_t ldc, int K,
+                                  bool add, cudaStream_t s) {
+    FusedView v = fused_view(p, K, fused_layers(p, K));
+    v.gin = grid;
+    v.ldg = ldg;
+    v.cout = coeffs;
+    v.ldc = ldc;
+    v.add = add ? 1 : 0;
+    return fused_launch(p, false, v, s);
 }
 
 }  // namespace sht

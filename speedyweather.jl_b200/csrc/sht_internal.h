@@ -103,6 +103,30 @@ struct FftView {
     TcImage img;          // analysis operand image of tensor-core plans (base == nullptr: FP32 scratch)
 };
 
+// The operands of a fused (FFT + Legendre in one launch) transform of an FP32 plan:
+// a cluster of P CTAs per chunk of C layers (sht_fft.cu).
+struct FusedView {
+    const RingDesc* rings;
+    const float2* twiddle;
+    const float* lam;
+    const int64_t* lam_off;
+    const int32_t* rows;
+    const int32_t* j0;
+    const int64_t* lm_off;
+    int nh, nh_pad, lmax, mmax, mt_max;
+    const float2* cin;    // synthesis input coefficients
+    float2* cout;         // analysis output coefficients
+    int64_t ldc;
+    const float* gin;     // analysis input grid
+    float* gout;          // synthesis output grid
+    int64_t ldg;
+    int K, C, P;          // layers, layers per cluster, CTAs per cluster
+    int nm_cta, nr_cta;   // orders and rings per CTA: ceil(mmax / P), ceil(nh / P)
+    int ldx, tw_max;      // layer stride of the FFT buffers, float2 of the largest ring's tables
+    int unscale, add;
+    int uniform;          // all rings of one length: a CTA transforms its rings in one FFT
+};
+
 struct Plan {
     sht_desc d{};
     int nh = 0, nlat = 0, lmax = 0, mmax = 0, nlon_max = 0, nfreq_max = 0;
@@ -154,6 +178,12 @@ struct Plan {
     int2* d_fft_items = nullptr;        // FFT work list: (ring, layer chunk), costliest first
     int n_fft_items = 0;
     int leg_bn_syn = 128, leg_bn_ana = 128;   // FP32 Legendre tile widths (autotuned)
+    // fused transforms (FP32 plans whose cluster data fits in shared memory)
+    int fusion = 0;                     // 1: sht_synthesize / sht_analyze launch the fused kernels
+    int fusion_ok = 0;                  // the fused kernels can run this plan
+    int fused_P = 0, fused_cmax = 0, fused_ldx = 0, fused_tw_max = 0, fused_mt_max = 0, nsm = 148;
+    int fused_ncl = 1;                  // clusters of fused_P CTAs the device runs at once
+    int fused_uniform = 0;              // all rings of one length (full grids)
     // host copies for batches (grouped launches over several plans)
     std::vector<RingDesc> h_rings;
     std::vector<double> h_ring_cost;     // per ring: estimated FFT cost per layer
@@ -209,6 +239,12 @@ cudaError_t launch_uv_from_vordiv(const Plan& p, float2* U, float2* V, const flo
 cudaError_t launch_laplace(const Plan& p, float2* out, const float2* in, int64_t ldc, int K,
                            bool inverse, bool flipsign, bool add, float scale, cudaStream_t s);
 cudaError_t launch_operators(const Plan& p, const sht_op* ops, int nops, cudaStream_t s);
+// fused transforms (sht_fft.cu): fused_prepare sets fusion_ok and the launch shape
+cudaError_t fused_prepare(Plan& p);
+cudaError_t launch_fused_synthesis(const Plan& p, const float2* coeffs, int64_t ldc, float* grid, int64_t ldg, int K,
+                                   unsigned flags, cudaStream_t s);
+cudaError_t launch_fused_analysis(const Plan& p, const float* grid, int64_t ldg, float2* coeffs, int64_t ldc, int K,
+                                  bool add, cudaStream_t s);
 cudaError_t launch_gradient(const Plan& p, float2* dpdx, float2* dpdy, const float2* in, int64_t ldc,
                             int K, float inv_radius, cudaStream_t s);
 

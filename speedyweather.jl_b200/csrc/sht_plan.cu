@@ -498,6 +498,7 @@ int build_plan(Plan& p) {
         if (!tc_supported()) return fail(SHT_EUNSUPPORTED, "tensor-core Legendre precision %d not available", d.precision);
         if ((e = tc_prepare(p)) != cudaSuccess) return cuda_fail(e, "sht_plan_create tensor-core tables");
     }
+    if ((e = fused_prepare(p)) != cudaSuccess) return cuda_fail(e, "sht_plan_create fused kernels");
     return SHT_OK;
 }
 
@@ -678,6 +679,25 @@ int sht_plan_autotune(sht_plan* plan, int K, void* stream, int32_t* tile_columns
     return SHT_OK;
 }
 
+int sht_plan_set_fusion(sht_plan* plan, int mode) {
+    if (!plan) return fail(SHT_EINVAL, "sht_plan_set_fusion: NULL plan");
+    if (mode != SHT_FUSION_OFF && mode != SHT_FUSION_ON)
+        return fail(SHT_EINVAL, "sht_plan_set_fusion: mode %d is neither SHT_FUSION_OFF nor SHT_FUSION_ON", mode);
+    Plan& p = plan->p;
+    if (mode == SHT_FUSION_ON && !p.fusion_ok)
+        return fail(SHT_EUNSUPPORTED, "sht_plan_set_fusion: %s", p.tc ? "tensor-core plans keep the separate kernels"
+                                                                    : "the plan's cluster data exceeds shared memory");
+    p.fusion = mode;
+    return SHT_OK;
+}
+
+int sht_plan_get_fusion(const sht_plan* plan, int32_t* mode, int32_t* available) {
+    if (!plan) return fail(SHT_EINVAL, "sht_plan_get_fusion: NULL plan");
+    if (mode) *mode = plan->p.fusion;
+    if (available) *available = plan->p.fusion_ok;
+    return SHT_OK;
+}
+
 int sht_device_status(sht_plan* plan, int32_t* status) {
     if (!plan || !status) return fail(SHT_EINVAL, "sht_device_status: NULL argument");
     DeviceGuard g(plan->p.device);
@@ -750,6 +770,9 @@ int sht_synthesize(sht_plan* plan, const void* coeffs, int64_t ldc, float* grid,
     if (!ok_ptr(coeffs) || !ok_ptr(grid)) return fail(SHT_EINVAL, "sht_synthesize: NULL array");
     DeviceGuard g(plan->p.device);
     cudaStream_t s = (cudaStream_t)stream;
+    if (plan->p.fusion)
+        return finish(launch_fused_synthesis(plan->p, (const float2*)coeffs, ldc, grid, ldg, K, flags, s),
+                      "sht_synthesize (fused)");
     cudaError_t e = legendre_synthesis(plan->p, (const float2*)coeffs, ldc, K, s);
     if (e != cudaSuccess) return cuda_fail(e, "sht_synthesize (Legendre)");
     return finish(launch_fft_synthesis(plan->p, grid, ldg, K, flags, s), "sht_synthesize (Fourier)");
@@ -765,6 +788,9 @@ int sht_analyze(sht_plan* plan, const float* grid, int64_t ldg, void* coeffs, in
     if (!ok_ptr(coeffs) || !ok_ptr(grid)) return fail(SHT_EINVAL, "sht_analyze: NULL array");
     DeviceGuard g(plan->p.device);
     cudaStream_t s = (cudaStream_t)stream;
+    if (plan->p.fusion)
+        return finish(launch_fused_analysis(plan->p, grid, ldg, (float2*)coeffs, ldc, K, (flags & SHT_ADD) != 0, s),
+                      "sht_analyze (fused)");
     cudaError_t e = launch_fft_analysis(plan->p, grid, ldg, K, s);
     if (e != cudaSuccess) return cuda_fail(e, "sht_analyze (Fourier)");
     return finish(legendre_analysis(plan->p, (float2*)coeffs, ldc, K, (flags & SHT_ADD) != 0, s),

@@ -339,6 +339,26 @@ class SpectralTransform:
         check(lib.sht_plan_autotune(self._plan, int(nlayers or self.nlayers), _stream_ptr(self.device), cols))
         return int(cols[0]), int(cols[1])
 
+    @property
+    def fusion(self) -> bool:
+        """True when transforms run fused (FFT and Legendre stage in one launch per
+        direction, thread-block clusters passing the Fourier rows through shared memory);
+        same bits as the separate kernels. Settable; FP32 plans of small truncations only.
+        On by default for full Gaussian grids up to nlat 64, where it measured faster."""
+        mode = C.c_int32(0)
+        check(lib.sht_plan_get_fusion(self._plan, C.byref(mode), None))
+        return bool(mode.value)
+
+    @fusion.setter
+    def fusion(self, on: bool):
+        check(lib.sht_plan_set_fusion(self._plan, 1 if on else 0))
+
+    @property
+    def fusion_available(self) -> bool:
+        ok = C.c_int32(0)
+        check(lib.sht_plan_get_fusion(self._plan, None, C.byref(ok)))
+        return bool(ok.value)
+
     def __repr__(self):
         return (f"SpectralTransform({self.spectrum}, {self.grid}, nlayers={self.nlayers}, "
                 f"precision={self.precision!r})")
