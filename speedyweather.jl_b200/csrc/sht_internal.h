@@ -62,6 +62,7 @@ struct LegView {
     const int32_t* j0;
     const int64_t* lm_off;
     const RingDesc* rings;
+    const int64_t* gofs;  // per ring: first Fourier-scratch row (m = 0)
     int nh, nh_pad, lmax;
     const float2* cin;    // synthesis input coefficients
     float2* cout;         // analysis output coefficients

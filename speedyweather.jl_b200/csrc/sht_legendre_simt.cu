@@ -172,7 +172,8 @@ __device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, flo
     const int rows = v.rows[m];
     const float* L = v.lam + v.lam_off[m] + (int64_t)par * rows * v.nh_pad;
     const int64_t lmo = v.lm_off[m];
-    const int jstart = (v.j0[m] / BK) * BK;
+    const int j0m = v.j0[m];
+    const int jstart = (j0m / BK) * BK;
     const int t = threadIdx.x;
     const int tx = t % 16, ty = t / 16;
     const int a_i = t / 2, a_j = (t % 2) * 4;     // 64 rows x 8 rings: one float4 per thread
@@ -194,10 +195,8 @@ __device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, flo
         for (int q = 0; q < NB; ++q) {
             const int j = jc + b_j0 + BSTEP * q;
             float2 x = make_float2(0.f, 0.f);
-            if (j < v.nh && k < v.K) {
-                const RingDesc& rd = v.rings[j];
-                if (m <= rd.mt) x = v.four[((rd.gofs + m) * 2 + par) * v.K + k];
-            }
+            // rings j >= j0(m) carry order m (m <= mt(j)); one load of the ring's scratch base
+            if (j < v.nh && k < v.K && j >= j0m) x = v.four[((__ldg(v.gofs + j) + m) * 2 + par) * v.K + k];
             rb[q] = x;
         }
     };
@@ -307,6 +306,7 @@ LegView leg_view(const Plan& p, const float2* cin, float2* cout, int64_t ldc, co
     v.j0 = p.d_j0;
     v.lm_off = p.d_lm_off;
     v.rings = p.d_rings;
+    v.gofs = p.d_gofs;
     v.nh = p.nh;
     v.nh_pad = p.nh_pad;
     v.lmax = p.lmax;
