@@ -445,6 +445,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------ MMA issuer
         const uint32_t idesc = idesc_f16(t.fp16 ? 0u : 1u, SYN ? 1u : 0u, SYN ? 0u : 1u, (uint32_t)nt_cols);
+        // Three products L0 B0 + (L0 B1 + L1 B0) with split accumulators: B0 and B1 lie next
+        // to each other in the stage, so L0 x [B0; B1] is one MMA of N = 2 nt_cols whose two
+        // halves are exactly the leading and the cross accumulator; L1 x B0 then adds to the
+        // cross half. Two MMAs per step instead of three, and A piece 0 is read once.
+        const bool stacked = split && t.nprod == 3 && t.npa == 2 && t.npb == 2 && 2 * nt_cols <= 256 &&
+                             xoff == (uint32_t)nt_cols &&
+                             t.prod == ((0u | (0u << 2)) | ((0u | (1u << 2)) << 4) | ((1u | (0u << 2)) << 8));
+        const uint32_t idesc2 = idesc_f16(t.fp16 ? 0u : 1u, SYN ? 1u : 0u, SYN ? 0u : 1u, (uint32_t)(2 * nt_cols));
         int g = 0, ti = 0;
         bool ok = true;
         for (int i = 0, ix = blockIdx.x; ix < nitems && ok && !*abort_flag; ++i, ix += gridDim.x) {
@@ -472,6 +480,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 tc_fence_after();
                 const uint32_t st = smem_u32(smem + (size_t)s * stage_bytes);
+                if (stacked) {
+                    for (int kk = 0; kk < BLK / 16; ++kk) {
+                        const uint32_t a0 = st, a1 = st + A_PIECE_BYTES, b0 = st + a_bytes;
+                        uint64_t da0, da1, db;
+                        if (SYN) {
+                            da0 = sdesc(a0 + kk * 2048, BOX_BYTES, 1024);
+                            da1 = sdesc(a1 + kk * 2048, BOX_BYTES, 1024);
+                            db = sdesc(b0 + kk * 32, 16, 1024);
+                        } else {
+                            da0 = sdesc(a0 + kk * 32, 16, 1024);
+                            da1 = sdesc(a1 + kk * 32, 16, 1024);
+                            db = sdesc(b0 + kk * 2048, BOX_BYTES, 1024);
+                        }
+                        umma_f16(dacc, da0, db, idesc2, (ks == ks0 && kk == 0) ? 0u : 1u);   // L0 [B0; B1]
+                        umma_f16(dacc + xoff, da1, db, idesc, 1u);                           // L1 B0
+                    }
+                    umma_commit(&empty_bar[s]);
+                    continue;
+                }
                 for (int kk = 0; kk < BLK / 16; ++kk) {
                     for (int q = 0; q < t.nprod; ++q) {
                         const int pa = (t.prod >> (4 * q)) & 3, pb = (t.prod >> (4 * q + 2)) & 3;
