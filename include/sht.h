@@ -253,13 +253,15 @@ SHT_API int sht_synthesize_adjoint(sht_plan* plan, const float* grid_bar, int64_
 SHT_API int sht_analyze_adjoint(sht_plan* plan, const void* coeffs_bar, int64_t ldc, float* grid_bar, int64_t ldg,
                                 int K, unsigned flags, void* stream);
 
-/* Autotuner of a plan's own launches: times the FP32 Legendre kernels of an
- * SHT_PREC_FP32 plan at K layers for each tile width (32, 64, 128 real columns) on
- * scratch buffers it allocates, keeps the fastest per direction for later calls, and
- * reports them in tile_columns[2] (synthesis, analysis; may be NULL). Results are
- * bitwise the same for every tile width. Tensor-core plans have nothing to tune and
- * return SHT_OK with tile_columns = {0, 0}. No counterpart in the reference. */
+/* Autotuner of a plan's own launches: times the Legendre kernels at K layers on scratch
+ * buffers it allocates, keeps the fastest choice for later calls, and reports it in
+ * tile_columns[2] (synthesis, analysis; may be NULL). SHT_PREC_FP32 plans: the SIMT tile
+ * width (32, 64, 128 real columns) per direction. Tensor-core plans: the tcgen05 GEMMs'
+ * column tile width (64 or 128 columns, N of the MMAs), one for both directions. Results
+ * are bitwise the same for every width. sht_plan_set_tile_columns sets the widths
+ * directly (same rules; SHT_EINVAL otherwise). No counterpart in the reference. */
 SHT_API int sht_plan_autotune(sht_plan* plan, int K, void* stream, int32_t* tile_columns);
+SHT_API int sht_plan_set_tile_columns(sht_plan* plan, int synthesis, int analysis);
 
 /* Fused transforms: the Fourier and Legendre stages of sht_synthesize / sht_analyze in
  * one launch per direction, for SHT_PREC_FP32 plans whose per-cluster data fits in
@@ -285,9 +287,12 @@ SHT_API int sht_plan_get_fusion(const sht_plan* plan, int32_t* mode, int32_t* av
  * graphs the reference caches by field pointer (SpeedyTransforms/ext/gpu_graphs_common.jl:296-343).
  * A batch runs all SHT_SYNTHESIS items, then all SHT_ANALYSIS items, as four persistent
  * launches (Legendre synthesis, FFT synthesis, FFT analysis, Legendre analysis) over the
- * union of the items' work lists; each item has its own Fourier scratch, allocated by
- * sht_batch_create, so items may share a plan. Arrays are bound at creation: later runs
- * read and write the same device buffers. Plans: SHT_PREC_FP32, one device. */
+ * union of the items' FP32 work lists; each such item has its own Fourier scratch,
+ * allocated by sht_batch_create, so items may share a plan. Items of tensor-core plans
+ * (split precisions) run as their own sht_synthesize / sht_analyze calls on the same
+ * stream, after the grouped syntheses and after the grouped analyses respectively, and
+ * use their plan's buffers (items of one tensor-core plan run in order). Arrays are
+ * bound at creation: later runs read and write the same device buffers. One device. */
 #define SHT_SYNTHESIS 0          /* coeffs -> grid */
 #define SHT_ANALYSIS 1           /* grid -> coeffs */
 

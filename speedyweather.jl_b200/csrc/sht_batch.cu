@@ -70,6 +70,7 @@ void build_lists(const sht_batch& b, int bn, std::vector<GroupItem> (&lists)[4])
     for (int t = 0; t < (int)b.items.size(); ++t) {
         const sht_batch_item& it = b.items[t];
         const Plan& p = *plan_impl(it.plan);
+        if (p.d.precision != SHT_PREC_FP32) continue;      // tensor-core plans run as their own calls
         const int K = it.nlayers;
         const bool syn = it.direction == SHT_SYNTHESIS;
         const int nct = (2 * K + bn - 1) / bn;
@@ -119,6 +120,23 @@ cudaError_t upload_lists(sht_batch& b, int bn) {
 
 int bn_index(int bn) { return bn == 32 ? 0 : bn == 64 ? 1 : 2; }
 
+// The items of tensor-core plans in one direction, each as its own sht_synthesize /
+// sht_analyze call on the stream (their Legendre stage is the persistent tcgen05 kernel).
+cudaError_t run_tc_items(const sht_batch& b, bool synthesis, cudaStream_t s) {
+    for (const sht_batch_item& it : b.items) {
+        if (plan_impl(it.plan)->d.precision == SHT_PREC_FP32 || (it.direction == SHT_SYNTHESIS) != synthesis)
+            continue;
+        const int rc = synthesis
+                           ? sht_synthesize(it.plan, it.coeffs, it.ldc, it.grid, it.ldg, it.nlayers, it.flags, s)
+                           : sht_analyze(it.plan, it.grid, it.ldg, it.coeffs, it.ldc, it.nlayers, it.flags, s);
+        if (rc != SHT_OK) return cudaErrorLaunchFailure;
+    }
+    return cudaSuccess;
+}
+
+// Every synthesis of the batch completes before any analysis starts (an analysis may read
+// a grid a synthesis of the same batch writes): grouped Legendre and Fourier synthesis,
+// tensor-core syntheses, grouped Fourier and Legendre analysis, tensor-core analyses.
 cudaError_t run(const sht_batch& b, cudaStream_t s) {
     cudaError_t e;
     const int lg = b.leg_grid[bn_index(b.bn)];
@@ -128,10 +146,14 @@ cudaError_t run(const sht_batch& b, cudaStream_t s) {
     if ((e = launch_fft_grouped(b.d_fft, b.d_lists + b.off_list[1], b.n_list[1], true, b.fft_smem,
                                 kFftCtasPerSm * b.nsm, s)) != cudaSuccess)
         return e;
+    if ((e = run_tc_items(b, true, s)) != cudaSuccess) return e;
     if ((e = launch_fft_grouped(b.d_fft, b.d_lists + b.off_list[2], b.n_list[2], false, b.fft_smem,
                                 kFftCtasPerSm * b.nsm, s)) != cudaSuccess)
         return e;
-    return launch_legendre_grouped(b.d_leg, b.d_lists + b.off_list[3], b.n_list[3], b.bn, false, lg, s);
+    if ((e = launch_legendre_grouped(b.d_leg, b.d_lists + b.off_list[3], b.n_list[3], b.bn, false, lg, s)) !=
+        cudaSuccess)
+        return e;
+    return run_tc_items(b, false, s);
 }
 
 void release(sht_batch* b) {
@@ -155,8 +177,6 @@ int sht_batch_create(const sht_batch_item* items, int nitems, sht_batch** out) {
         const sht_batch_item& it = items[t];
         if (!it.plan) return bfail(SHT_EINVAL, "sht_batch_create: NULL plan");
         const Plan& p = *plan_impl(it.plan);
-        if (p.d.precision != SHT_PREC_FP32)
-            return bfail(SHT_EUNSUPPORTED, "sht_batch_create: grouped launches take SHT_PREC_FP32 plans");
         if (device >= 0 && p.device != device)
             return bfail(SHT_EINVAL, "sht_batch_create: plans on different devices");
         device = p.device;
@@ -181,6 +201,7 @@ int sht_batch_create(const sht_batch_item* items, int nitems, sht_batch** out) {
     for (int t = 0; t < nitems && e == cudaSuccess; ++t) {
         const sht_batch_item& it = items[t];
         const Plan& p = *plan_impl(it.plan);
+        if (p.d.precision != SHT_PREC_FP32) continue;      // runs as its own call on the plan's buffers
         e = cudaMalloc(&b->scratch[t], std::max<int64_t>(1, p.scratch_rows * 2 * it.nlayers) * sizeof(float2));
         if (e != cudaSuccess) break;
         const bool syn = it.direction == SHT_SYNTHESIS;

@@ -219,6 +219,8 @@ cudaError_t launch_wait_probe(int32_t* err, uint64_t limit_ns, cudaStream_t s);
 cudaError_t launch_column_physics(const float* temp, const float* humid, const float* ps, int64_t ld, int ncol,
                                   float dt, float* dtemp, float* dhumid, int64_t ldo, bool add, cudaStream_t s);
 cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s, float mul);
+int tc_tile_cols(const Plan& p);                 // tensor-core plans: GEMM column tile width
+bool tc_set_tile_cols(Plan& p, int cols);        // 64 or 128; false for other widths or FP32 plans
 cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t s,
                                 bool to_image = false, unsigned flags = 0, bool adjoint = false);
 cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags,

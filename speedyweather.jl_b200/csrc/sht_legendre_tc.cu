@@ -115,6 +115,7 @@ struct TcDev {
 };
 
 struct TcState {
+    int ctw = kTcTileCols;         // column tile width of the transforms' GEMMs (64 or 128; autotuned)
     int npa = 2, npb = 2, nprod = 3;
     uint32_t prod = 0;
     int nmax = 0;
@@ -1056,12 +1057,12 @@ cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, in
     e = cudaGetLastError();
     if (e != cudaSuccess || s.n_syn_items == 0) return e;
     const int ncols = 2 * K;
-    const int nct = (ncols + kTcTileCols - 1) / kTcTileCols;
-    const int nt_cols = std::min(kTcTileCols, (ncols + 63) / 64 * 64);
+    const int nct = (ncols + s.ctw - 1) / s.ctw;
+    const int nt_cols = std::min(s.ctw, (ncols + 63) / 64 * 64);
     int stages;
     const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
     legendre_tc_kernel<true><<<dim3(std::min(s.n_syn_items, s.nsm), nct), TC_THREADS, smem, st>>>(
-        t, s.d_syn_items, s.n_syn_items, K, kTcTileCols, nt_cols, stages, tmem_cols_for(nt_cols), 1, p.d_four, nullptr,
+        t, s.d_syn_items, s.n_syn_items, K, s.ctw, nt_cols, stages, tmem_cols_for(nt_cols), 1, p.d_four, nullptr,
         0, 0);
     return cudaGetLastError();
 }
@@ -1291,6 +1292,15 @@ cudaError_t tc_matrix_apply(const TcMatrix* x, int which, const float* in, int64
     return cudaGetLastError();
 }
 
+// Column tile width of a tensor-core plan's Legendre GEMMs: 128 (one tile for 64 layers)
+// or 64. Each output column is computed alike in either; the speed differs.
+int tc_tile_cols(const Plan& p) { return p.tc ? static_cast<const TcState*>(p.tc)->ctw : 0; }
+bool tc_set_tile_cols(Plan& p, int cols) {
+    if (!p.tc || (cols != 64 && cols != kTcTileCols)) return false;
+    static_cast<TcState*>(p.tc)->ctw = cols;
+    return true;
+}
+
 cudaError_t tc_analysis_scale(const Plan& p, const float* grid, int64_t ldg, int K, cudaStream_t st, float mul) {
     const TcState* s = static_cast<const TcState*>(p.tc);
     if (!s || !s->fp16 || K <= 0) return cudaSuccess;
@@ -1307,12 +1317,12 @@ cudaError_t launch_legendre_analysis_tc(const Plan& p, float2* coeffs, int64_t l
     if (s.n_ana_items == 0) return cudaSuccess;
     const TcDev t = make_dev(p);
     const int ncols = 2 * K;
-    const int nct = (ncols + kTcTileCols - 1) / kTcTileCols;
-    const int nt_cols = std::min(kTcTileCols, (ncols + 63) / 64 * 64);
+    const int nct = (ncols + s.ctw - 1) / s.ctw;
+    const int nt_cols = std::min(s.ctw, (ncols + 63) / 64 * 64);
     int stages;
     const int smem = smem_for(s.npa, s.npb, nt_cols, stages);
     legendre_tc_kernel<false><<<dim3(std::min(s.n_ana_items, s.nsm), nct), TC_THREADS, smem, st>>>(
-        t, s.d_ana_items, s.n_ana_items, K, kTcTileCols, nt_cols, stages, tmem_cols_for(nt_cols), 1, nullptr, coeffs,
+        t, s.d_ana_items, s.n_ana_items, K, s.ctw, nt_cols, stages, tmem_cols_for(nt_cols), 1, nullptr, coeffs,
         ldc, add ? 1 : 0);
     return cudaGetLastError();
 }

@@ -635,39 +635,62 @@ int sht_plan_autotune(sht_plan* plan, int K, void* stream, int32_t* tile_columns
     if ((rc = check_call(plan, K, "sht_plan_autotune")) != SHT_OK) return rc;
     if (tile_columns) tile_columns[0] = tile_columns[1] = 0;
     Plan& p = plan->p;
-    if (p.d.precision != SHT_PREC_FP32 || K == 0) return SHT_OK;
+    if (K == 0) return SHT_OK;
     DeviceGuard g(p.device);
     cudaStream_t s = (cudaStream_t)stream;
+    const bool tc = p.d.precision != SHT_PREC_FP32;
     float2* c = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t e = cudaMalloc(&c, p.nlm * K * sizeof(float2));
     if (e == cudaSuccess) e = cudaMemsetAsync(c, 0, p.nlm * K * sizeof(float2), s);
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    auto time = [&](auto&& launch, float& ms) {
+        for (int w = 0; w < 2 && e == cudaSuccess; ++w) e = launch();
+        if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+        for (int r = 0; r < 5 && e == cudaSuccess; ++r) e = launch();
+        if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    };
     int best[2] = {p.leg_bn_syn, p.leg_bn_ana};
-    for (int dir = 0; dir < 2 && e == cudaSuccess; ++dir) {
+    if (tc) {
+        // tcgen05 column tile width: one width serves both directions (the images are laid out for it)
+        best[0] = best[1] = tc_tile_cols(p);
         float best_ms = 1e30f;
-        for (int bn : {32, 64, 128}) {
-            (dir == 0 ? p.leg_bn_syn : p.leg_bn_ana) = bn;
-            auto launch = [&]() {
-                return dir == 0 ? launch_legendre_synthesis_fp32(p, c, p.nlm, K, s)
-                                : launch_legendre_analysis_fp32(p, c, p.nlm, K, false, s);
-            };
-            for (int w = 0; w < 2 && e == cudaSuccess; ++w) e = launch();
-            if (e == cudaSuccess) e = cudaEventRecord(e0, s);
-            for (int r = 0; r < 5 && e == cudaSuccess; ++r) e = launch();
-            if (e == cudaSuccess) e = cudaEventRecord(e1, s);
-            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        for (int cols : {128, 64}) {
+            if (cols == 64 && 2 * K <= 64) break;       // a single tile of <= 64 columns either way
+            tc_set_tile_cols(p, cols);
             float ms = 0.f;
-            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            time([&]() {
+                cudaError_t x = legendre_synthesis(p, c, p.nlm, K, s);
+                return x == cudaSuccess ? legendre_analysis(p, c, p.nlm, K, false, s) : x;
+            }, ms);
             if (e == cudaSuccess && ms < best_ms) {
                 best_ms = ms;
-                best[dir] = bn;
+                best[0] = best[1] = cols;
             }
         }
+        tc_set_tile_cols(p, best[0]);
+    } else {
+        for (int dir = 0; dir < 2 && e == cudaSuccess; ++dir) {
+            float best_ms = 1e30f;
+            for (int bn : {32, 64, 128}) {
+                (dir == 0 ? p.leg_bn_syn : p.leg_bn_ana) = bn;
+                float ms = 0.f;
+                time([&]() {
+                    return dir == 0 ? launch_legendre_synthesis_fp32(p, c, p.nlm, K, s)
+                                    : launch_legendre_analysis_fp32(p, c, p.nlm, K, false, s);
+                }, ms);
+                if (e == cudaSuccess && ms < best_ms) {
+                    best_ms = ms;
+                    best[dir] = bn;
+                }
+            }
+        }
+        p.leg_bn_syn = best[0];
+        p.leg_bn_ana = best[1];
     }
-    p.leg_bn_syn = best[0];
-    p.leg_bn_ana = best[1];
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (c) cudaFree(c);
@@ -676,6 +699,23 @@ int sht_plan_autotune(sht_plan* plan, int K, void* stream, int32_t* tile_columns
         tile_columns[0] = best[0];
         tile_columns[1] = best[1];
     }
+    return SHT_OK;
+}
+
+int sht_plan_set_tile_columns(sht_plan* plan, int synthesis, int analysis) {
+    if (!plan) return fail(SHT_EINVAL, "sht_plan_set_tile_columns: NULL plan");
+    Plan& p = plan->p;
+    if (p.d.precision == SHT_PREC_FP32) {
+        auto ok = [](int v) { return v == 32 || v == 64 || v == 128; };
+        if (!ok(synthesis) || !ok(analysis))
+            return fail(SHT_EINVAL, "sht_plan_set_tile_columns: FP32 plans take 32, 64 or 128 columns");
+        p.leg_bn_syn = synthesis;
+        p.leg_bn_ana = analysis;
+        return SHT_OK;
+    }
+    if (synthesis != analysis || !tc_set_tile_cols(p, synthesis))
+        return fail(SHT_EINVAL, "sht_plan_set_tile_columns: tensor-core plans take 64 or 128 columns, the same for "
+                                "both directions");
     return SHT_OK;
 }
 

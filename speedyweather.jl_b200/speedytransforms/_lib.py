@@ -76,6 +76,7 @@ SIGNATURES = {
     "sht_diag_wait_expiry": (C.c_int, [_P, C.c_int32, _P]),
     "sht_analyze_static_scratch": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
     "sht_plan_autotune": (C.c_int, [_P, C.c_int, _P, C.POINTER(C.c_int32)]),
+    "sht_plan_set_tile_columns": (C.c_int, [_P, C.c_int, C.c_int]),
     "sht_plan_set_fusion": (C.c_int, [_P, C.c_int]),
     "sht_plan_get_fusion": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "sht_synthesize_adjoint": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),

@@ -332,12 +332,17 @@ class SpectralTransform:
         check(lib.sht_plan_set_host_chunk(self._plan, int(layers)))
 
     def autotune(self, nlayers: int | None = None):
-        """Time the FP32 Legendre kernels at ``nlayers`` layers for each tile width and
-        keep the fastest per direction (results are bitwise independent of the choice).
-        Returns (synthesis, analysis) tile widths; (0, 0) for tensor-core plans."""
+        """Time the Legendre kernels at ``nlayers`` layers for each tile width and keep the
+        fastest (results are bitwise independent of the choice): the SIMT tile width per
+        direction for "fp32" plans, the tcgen05 column tile width (64 or 128) for the
+        tensor-core precisions. Returns the (synthesis, analysis) widths."""
         cols = (C.c_int32 * 2)()
         check(lib.sht_plan_autotune(self._plan, int(nlayers or self.nlayers), _stream_ptr(self.device), cols))
         return int(cols[0]), int(cols[1])
+
+    def set_tile_columns(self, synthesis: int, analysis: int | None = None):
+        """Set the Legendre tile widths directly (as autotune's choices)."""
+        check(lib.sht_plan_set_tile_columns(self._plan, int(synthesis), int(analysis or synthesis)))
 
     @property
     def fusion(self) -> bool:

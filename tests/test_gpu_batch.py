@@ -129,14 +129,7 @@ def test_batch_flags(st, mixed):
 
 
 def test_batch_errors(st, mixed):
-    from speedytransforms._lib import SHT_EUNSUPPORTED, ShtError
     cs = mixed[1]
-    St = st.SpectralTransform(st.Spectrum(64, 64), st.OctahedralGaussianGrid(48), nlayers=8, precision="bf16x3")
-    f = st.Field.zeros(St.grid, 8, device=cs["lt"].data.device)
-    lt = st.LowerTriangularArray.zeros(St.spectrum, 8, device=cs["lt"].data.device)
-    with pytest.raises(ShtError) as e:
-        st.Batch([(f, lt, St)])
-    assert e.value.code == SHT_EUNSUPPORTED
     big = st.LowerTriangularArray.zeros(cs["S"].spectrum, cs["K"] + 1, device=cs["lt"].data.device)
     fb = st.Field.zeros(cs["S"].grid, cs["K"] + 1, device=cs["lt"].data.device)
     with pytest.raises(st.DimensionMismatch):
@@ -155,4 +148,71 @@ def test_plan_autotune_keeps_results(st, mixed):
     np.testing.assert_array_equal(np_of(f), cs["f_ref"])
     np.testing.assert_array_equal(np_of(a), cs["a_ref"])
     St = st.SpectralTransform(st.Spectrum(32, 32), st.OctahedralGaussianGrid(24), nlayers=2, precision="bf16x3")
-    assert St.autotune() == (0, 0)
+    assert St.autotune() in ((64, 64), (128, 128))
+
+
+def test_batch_with_tensor_core_plans(st, mixed):
+    """FP32 items in the grouped launches and split-FP16 / split-BF16 items as their own
+    calls in one batch: run and graph replay give the bits of one transform_ per item;
+    the split items stay within their tolerance of the oracle."""
+    import torch
+    dev = mixed[0]["lt"].data.device
+    entries, refs = [], []
+    for cs in mixed[:2]:                                  # FP32 T31 x 1 and T63 x 8
+        f = st.Field.zeros(cs["S"].grid, cs["K"], device=dev)
+        a = st.LowerTriangularArray.zeros(cs["S"].spectrum, cs["K"], device=dev)
+        entries += [(f, cs["lt"], cs["S"]), (a, f, cs["S"])]
+        refs += [cs["f_ref"], cs["a_ref"]]
+    tc = []
+    for prec, T, nh, K in [("fp16x3", 64, 48, 8), ("bf16x3", 128, 96, 16)]:
+        S = st.SpectralTransform(st.Spectrum(T, T), st.OctahedralGaussianGrid(nh), nlayers=K, precision=prec)
+        So = O.SpectralTransform(O.Spectrum(T, T), O.Grid(O.OCTAHEDRAL_GAUSSIAN, nh))
+        c = O.random_coeffs(So.spectrum, K, seed=T + 1)
+        lt = to_lta(st, S, c)
+        f_ref = st.transform(lt, S)
+        a_ref = st.transform(f_ref, S)
+        torch.cuda.synchronize()
+        f = st.Field.zeros(S.grid, K, device=dev)
+        a = st.LowerTriangularArray.zeros(S.spectrum, K, device=dev)
+        entries += [(f, lt, S), (a, f, S)]
+        refs += [np_of(f_ref), np_of(a_ref)]
+        tc.append((So, c, f, prec))
+    b = st.Batch(entries)
+    for how in (b.run, b.run_each):
+        for out, _, _ in entries:
+            out.data.zero_()
+        how()
+        torch.cuda.synchronize()
+        for (out, _, _), ref in zip(entries, refs):
+            np.testing.assert_array_equal(np_of(out), ref)
+    b.capture()
+    for out, _, _ in entries:
+        out.data.zero_()
+    b.launch()
+    torch.cuda.synchronize()
+    for (out, _, _), ref in zip(entries, refs):
+        np.testing.assert_array_equal(np_of(out), ref)
+    for So, c, f, prec in tc:
+        assert O.rel_err(np_of(f), So.synthesize(c)) < (1e-6 if prec == "fp16x3" else 1e-5)
+
+
+@pytest.mark.parametrize("prec", ["fp16x3", "bf16x3"])
+def test_tensor_core_tile_widths_give_the_same_bits(st, prec):
+    """64-column and 128-column tcgen05 tiles (48 layers: 96 columns, so 2 tiles of 64 or one
+    of 128) compute every output column alike."""
+    import torch
+    S = st.SpectralTransform(st.Spectrum(64, 64), st.OctahedralGaussianGrid(48), nlayers=48, precision=prec)
+    So = O.SpectralTransform(O.Spectrum(64, 64), O.Grid(O.OCTAHEDRAL_GAUSSIAN, 48))
+    lt = to_lta(st, S, O.random_coeffs(So.spectrum, 48, seed=9))
+    out = {}
+    for cols in (128, 64):
+        S.set_tile_columns(cols)
+        f = st.transform(lt, S)
+        a = st.transform(f, S)
+        torch.cuda.synchronize()
+        out[cols] = (f.data.clone(), a.data.clone())
+    assert S.device_status() == 0
+    assert torch.equal(out[64][0], out[128][0]) and torch.equal(out[64][1], out[128][1])
+    from speedytransforms._lib import ShtError
+    with pytest.raises(ShtError):
+        S.set_tile_columns(32)
