@@ -78,15 +78,17 @@ constexpr int G_EPI_LD = 33;        // epilogue transpose tile [32 rows][33]
 constexpr int G_EPI_BYTES = 8 * 32 * G_EPI_LD * 4;
 
 // GELU in its tanh form (Hendrycks & Gimpel 2016): gelu(x) = x (1 + tanh(u)) / 2,
-// u = sqrt(2 / pi) (x + 0.044715 x^3), with tanh(u) = 1 - 2 / (exp(2 u) + 1) on the exp
-// intrinsic (relative error ~1e-7, a handful of instructions; exp overflows to +inf
-// for large u, which gives tanh = 1, and underflows to 0 for very negative u: -1).
+// u = sqrt(2 / pi) (x + 0.044715 x^3), with tanh on the special-function unit
+// (tanh.approx.f32: one instruction, relative error about 2^-11, saturating to +-1; the
+// activations are rounded to BF16, 2^-9, right after).
 constexpr float GELU_C = 0.7978845608028654f;    // sqrt(2 / pi)
 constexpr float GELU_A = 0.044715f;
-__device__ __forceinline__ float gelu_tanh(float x) {
-    const float u = GELU_C * x * fmaf(GELU_A * x, x, 1.f);
-    return 1.f - __fdividef(2.f, __expf(2.f * u) + 1.f);
+__device__ __forceinline__ float tanh_sfu(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
+__device__ __forceinline__ float gelu_tanh(float x) { return tanh_sfu(GELU_C * x * fmaf(GELU_A * x, x, 1.f)); }
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + gelu_tanh(x)); }
 __device__ __forceinline__ float gelu_grad(float x) {
     const float t = gelu_tanh(x);
@@ -539,6 +541,27 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    // the epilogue warps' raw inputs, loaded before the barrier that publishes the
+    // constants (both loads in flight at once): row r, features [16 kh, 16 kh + 16)
+    float raw[16];
+    if (warp >= 2) {
+        const int et = threadIdx.x - 64, r = et & 127, kh = et >> 7;
+        const int64_t ij = col0 + r;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int c = 16 * kh + i;
+            float x = 0.f;
+            if (c < 4 * NLC + 1 && r < nrow) {
+                if (c < 4 * NLC) {
+                    const float* f = c < NLC ? a.T : c < 2 * NLC ? a.q : c < 3 * NLC ? a.u : a.v;
+                    x = __ldg(f + (int64_t)(c % NLC) * a.ld + ij);
+                } else {
+                    x = __ldg(a.ps + ij);
+                }
+            }
+            raw[i] = x;
+        }
+    }
     for (int i = threadIdx.x; i < F_C_N; i += blockDim.x) {   // the constants, read once
         float c;
         if (i < F_C_XS) c = a.xm[i];
@@ -610,7 +633,6 @@ __global__ void __launch_bounds__(F_THREADS, 1)
         const int et = threadIdx.x - 64;
         {   // ---- gather: row r, features [16 kh, 16 kh + 16), normalised, BF16 into the tile
             const int r = et & 127, kh = et >> 7;
-            const int64_t ij = col0 + r;
             bool in = true;
             uint32_t pk[8];
 #pragma unroll
@@ -621,13 +643,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                     const int c = 16 * kh + i + e;
                     float z = 0.f;
                     if (c < 4 * NLC + 1 && r < nrow) {
-                        float x;
-                        if (c < 4 * NLC) {
-                            const float* f = c < NLC ? a.T : c < 2 * NLC ? a.q : c < 3 * NLC ? a.u : a.v;
-                            x = f[(int64_t)(c % NLC) * a.ld + ij];
-                        } else {
-                            x = logf(a.ps[ij]);
-                        }
+                        const float x = c < 4 * NLC ? raw[i + e] : logf(raw[i + e]);
                         z = (x - cst[F_C_XM + c]) / cst[F_C_XS + c];
                         in = in && fabsf(z) <= a.zmax;
                     }

@@ -258,10 +258,12 @@ def model_trained(sp):
 def test_what_the_emulator_gains_on_model_states(sp, model_trained):
     """The emulator against the method it stands in for (the plain condensation +
     convection) on 8 fresh model states at T63 (10 944 columns each): time per grid and
-    tendency error. Measured on a B200: emulator 0.033 ms per grid (0.027 ms when no
-    column falls back; 2.6 % do at the 4-sigma range) against 0.012 ms for the plain kernel:
-    no speed gain (the plain scheme is a few hundred flops per column, the network 150 k
-    multiply-adds plus 768 activations); relative L2 tendency error 0.24 (T) and 0.17 (q). The bounds are the measured values plus 20 % (error) and a 3x ceiling on
+    tendency error. Measured on a B200: emulator 0.028 ms per grid (2.6 % of the columns
+    fall back at the 4-sigma range) against 0.012 ms for the plain kernel: no speed gain
+    (the plain scheme is a few hundred flops per column; the network is 150 k
+    multiply-adds plus 768 activations per column, four dependent layers of about 2 us of
+    MMAs and 2 us of activations each per 128-column tile); relative L2 tendency error 0.24
+    (T) and 0.17 (q). The bounds are the measured values plus 20 % (error) and a 3x ceiling on
     the time ratio (a regression guard, not a claimed gain)."""
     import torch
     em, ms = model_trained
