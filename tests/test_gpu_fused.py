@@ -16,7 +16,8 @@ from test_gpu_parity import np_of, setup, to_field, to_lta
 pytestmark = pytest.mark.gpu
 
 CASES = [(31, "full", 24, 8), (31, "octa", 24, 5), (63, "octa", 48, 8), (63, "octa", 48, 1), (127, "octa", 96, 48),
-         (63, "full", 48, 13), (127, "full", 96, 8)]
+         (63, "full", 48, 13), (127, "full", 96, 8),
+         (7, "full", 4, 3), (5, "octa", 3, 11)]       # fewer rings than a cluster has CTAs
 
 
 @pytest.fixture(scope="module")

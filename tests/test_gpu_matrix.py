@@ -97,3 +97,18 @@ def test_matrix_fp32_layer_tiles_and_determinism(st):
     assert M.device_status() == 0
     assert torch.equal(a1.data, a2.data)
     assert O.rel_err(np_of(a1), So.analyze(g.astype(np.float64))) < TOL["fp32"]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16x3"])
+def test_matrix_smaller_than_one_tile(st, prec):
+    """T5 on the full grid with nlat 8: matrices of 2 nlm = 42 x npoints = 128, less than one
+    128 x 32 tile in one direction and one k-block deep in the other."""
+    M = matrix(st, 5, "full", 4, 3, prec)
+    S, So = setup(st, 5, "full", 3, nh=4)
+    c = O.random_coeffs(So.spectrum, 3, seed=12)
+    f = st.transform(to_lta(st, S, c), M)
+    assert M.device_status() == 0
+    ref = So.synthesize(c)
+    assert O.rel_err(np_of(f), ref) < TOL[prec]
+    a = st.transform(to_field(st, S, ref.astype(np.float32)), M)
+    assert O.rel_err(np_of(a), So.analyze(ref.astype(np.float32).astype(np.float64))) < TOL[prec]
