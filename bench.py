@@ -839,6 +839,41 @@ def run_ours(args):
     clocks = clk.summary()
     value = world * args.steps / secs
 
+    # outside the timed region: the distribution of single round trips (an event after each,
+    # no host synchronisation between them) and the round trip replayed from a CUDA graph
+    nsamp = max(3, min(200, args.steps))
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(nsamp + 1)]
+    evs[0].record()
+    for i in range(nsamp):
+        round_trip(S)
+        evs[i + 1].record()
+    torch.cuda.synchronize()
+    per = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(nsamp))
+    per_step = {"median": per[nsamp // 2], "min": per[0], "max": per[-1], "samples": nsamp}
+    side = torch.cuda.Stream(device=device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            round_trip(S)
+    torch.cuda.current_stream(device).wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    GRAPH_RT = 10
+    with torch.cuda.graph(graph):
+        for _ in range(GRAPH_RT):
+            round_trip(S)
+    for _ in range(2):
+        graph.replay()
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nrep = max(3, args.steps // GRAPH_RT)
+    g0.record()
+    for _ in range(nrep):
+        graph.replay()
+    g1.record()
+    torch.cuda.synchronize()
+    graph_ms = g0.elapsed_time(g1) / (nrep * GRAPH_RT)
+    del graph
+
     # end to end through the public API with host buffers: every step copies its 64 layers
     # of coefficients in from page-locked host memory and its results back into it, inside
     # the transforms (sht_synthesize_host / sht_analyze_host), one round trip per chunk of
@@ -936,6 +971,9 @@ def run_ours(args):
             "e2e": {"value": world * args.steps / e2e_secs, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes, "plain_copy_ms": link},
             "roofline": roofline, "clocks": clocks, "gpu_launches": launches_per_rt * args.steps,
+            "per_round_trip_ms": per_step,
+            "graph": {"ms_per_round_trip": graph_ms, "round_trips_per_s": world * 1e3 / graph_ms,
+                      "round_trips_per_replay": GRAPH_RT},
             "variants": variants}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
