@@ -24,6 +24,18 @@ namespace {
 constexpr int BM = 64;    // rings (synthesis) or parity rows (analysis) per CTA
 constexpr int BK = 8;     // contraction depth per shared-memory stage
 constexpr int NT = 128;   // threads
+constexpr int SS = 3;     // shared-memory stages of the synthesis tiles (asynchronous copies)
+
+__device__ __forceinline__ void cp_async_zfill(void* dst, const void* src, int bytes, int src_bytes) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <int N>
 struct Vec;
@@ -89,8 +101,8 @@ __device__ __forceinline__ int col_of(int tx, int c) {
 }
 
 template <int BN>
-__device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[2][BK][BM],
-                         float (&Bs)[2][BK][BN]) {
+__device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[SS][BK][BM],
+                         float (&Bs)[SS][BK][BN]) {
     constexpr int TN = BN / 16;
     constexpr int NB = BN / 32;                   // complex coefficients per thread and stage
     const int j0 = tile * BM;
@@ -110,41 +122,39 @@ __device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, flo
 #pragma unroll
         for (int c = 0; c < TN; ++c) acc[r][c] = 0.f;
 
-    auto load_tiles = [&](int i0, float4& ra, float2 (&rb)[NB]) {
+    // SS-stage pipeline of asynchronous copies into shared memory (zero-filled outside the
+    // order's rows and degrees): the copies of step st + SS - 1 are in flight while step st
+    // computes; the contraction order is the same as with any other staging
+    const float* La = L + j0 + a_j;
+    const int kb = kt0 + b_k;
+    auto issue = [&](int step) {
+        const int stg = step % SS, i0 = step * BK;
         const int i = i0 + a_i;
-        ra = (i < rows) ? *reinterpret_cast<const float4*>(L + (int64_t)i * v.nh_pad + j0 + a_j)
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
-        const int k = kt0 + b_k;
+        const bool aok = i < rows;
+        cp_async_zfill(&As[stg][a_i][a_j], aok ? La + (int64_t)i * v.nh_pad : L, 16, aok ? 16 : 0);
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
             const int ii = i0 + b_i0 + BSTEP * q;
-            const int l = m + 2 * ii + par;
-            rb[q] = (ii < rows && l < v.lmax && k < v.K) ? v.cin[(int64_t)k * v.ldc + lmo + 2 * ii + par]
-                                                          : make_float2(0.f, 0.f);
+            const bool bok = ii < rows && m + 2 * ii + par < v.lmax && kb < v.K;
+            cp_async_zfill(&Bs[stg][b_i0 + BSTEP * q][2 * b_k],
+                           bok ? (const void*)(v.cin + (int64_t)kb * v.ldc + lmo + 2 * ii + par) : (const void*)v.cin, 8,
+                           bok ? 8 : 0);
         }
+        cp_async_commit();
     };
-    auto store_tiles = [&](int buf, const float4& ra, const float2 (&rb)[NB]) {
-        *reinterpret_cast<float4*>(&As[buf][a_i][a_j]) = ra;
-#pragma unroll
-        for (int q = 0; q < NB; ++q) *reinterpret_cast<float2*>(&Bs[buf][b_i0 + BSTEP * q][2 * b_k]) = rb[q];
-    };
-
-    float4 ra;
-    float2 rb[NB];
+    const int nsteps = (rows + BK - 1) / BK;
     __syncthreads();                               // the previous tile's reads of As/Bs are done
-    load_tiles(0, ra, rb);
-    store_tiles(0, ra, rb);
-    __syncthreads();
-    int buf = 0;
-    for (int i0 = 0; i0 < rows; i0 += BK) {
-        const bool more = i0 + BK < rows;
-        if (more) load_tiles(i0 + BK, ra, rb);
-        mma_step<BN>(As[buf], Bs[buf], tx, ty, acc);
-        if (more) {
-            store_tiles(buf ^ 1, ra, rb);
-            __syncthreads();
-            buf ^= 1;
-        }
+#pragma unroll
+    for (int st = 0; st < SS - 1; ++st) {
+        if (st < nsteps) issue(st);
+        else cp_async_commit();
+    }
+    for (int st = 0; st < nsteps; ++st) {
+        cp_async_wait<SS - 2>();                   // this thread's copies of step st have landed
+        __syncthreads();                           // everyone's; step st - 1's stage is free
+        if (st + SS - 1 < nsteps) issue(st + SS - 1);
+        else cp_async_commit();
+        mma_step<BN>(As[st % SS], Bs[st % SS], tx, ty, acc);
     }
     // epilogue: rows -> rings, column pairs -> complex layers
 #pragma unroll
@@ -163,8 +173,8 @@ __device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, flo
 }
 
 template <int BN>
-__device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[2][BK][BM],
-                         float (&Bs)[2][BK][BN]) {
+__device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[SS][BK][BM],
+                         float (&Bs)[SS][BK][BN]) {
     constexpr int TN = BN / 16;
     constexpr int NB = BN / 32;
     const int i_base = tile * BM;
@@ -250,8 +260,8 @@ __device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, flo
 template <int BN>
 __global__ void __launch_bounds__(NT) legendre_synthesis_fp32_kernel(const LegItem* __restrict__ items,
                                                                      const LegView v) {
-    __shared__ __align__(16) float As[2][BK][BM];
-    __shared__ __align__(16) float Bs[2][BK][BN];
+    __shared__ __align__(16) float As[SS][BK][BM];
+    __shared__ __align__(16) float Bs[SS][BK][BN];
     const LegItem it = items[blockIdx.x];
     syn_tile<BN>(v, it.m, it.tile, blockIdx.y, blockIdx.z, As, Bs);
 }
@@ -259,8 +269,8 @@ __global__ void __launch_bounds__(NT) legendre_synthesis_fp32_kernel(const LegIt
 template <int BN>
 __global__ void __launch_bounds__(NT) legendre_analysis_fp32_kernel(const LegItem* __restrict__ items,
                                                                     const LegView v) {
-    __shared__ __align__(16) float As[2][BK][BM];
-    __shared__ __align__(16) float Bs[2][BK][BN];
+    __shared__ __align__(16) float As[SS][BK][BM];
+    __shared__ __align__(16) float Bs[SS][BK][BN];
     const LegItem it = items[blockIdx.x];
     ana_tile<BN>(v, it.m, it.tile, blockIdx.y, blockIdx.z, As, Bs);
 }
@@ -271,8 +281,8 @@ template <int BN>
 __global__ void __launch_bounds__(NT) legendre_grouped_kernel(const LegView* __restrict__ views,
                                                               const GroupItem* __restrict__ items, int nitems,
                                                               int synthesis) {
-    __shared__ __align__(16) float As[2][BK][BM];
-    __shared__ __align__(16) float Bs[2][BK][BN];
+    __shared__ __align__(16) float As[SS][BK][BM];
+    __shared__ __align__(16) float Bs[SS][BK][BN];
     for (int ix = blockIdx.x; ix < nitems; ix += gridDim.x) {
         const GroupItem it = items[ix];
         const LegView& v = views[it.task];
