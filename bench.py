@@ -450,7 +450,7 @@ def run_column_emulator(args):
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     torch.cuda.synchronize()
     ev[0].record()
-    em.train(x, y, epochs=epochs, batch=batch, lr=2e-3, schedule="cosine")
+    em.train(x, y, epochs=epochs, batch=batch, lr=3e-3, schedule="cosine")
     ev[1].record()
     torch.cuda.synchronize()
     t_train = ev[0].elapsed_time(ev[1]) / 1e3
@@ -492,7 +492,7 @@ def run_column_emulator(args):
             "config": {"workload": "MLP 33-256-256-256-16 GELU (tanh form) emulator of condensation + "
                                    "convection, plain-physics fallback beyond 4 standard deviations",
                        "columns_per_grid": ncol, "train_columns": ntrain, "train_states": 96, "batch": batch,
-                       "epochs": epochs, "lr_schedule": "cosine 2e-3 -> 2e-5"},
+                       "epochs": epochs, "lr_schedule": "cosine 3e-3 -> 3e-5"},
             "train_columns_per_s": epochs * (ntrain // batch) * batch / t_train,
             "train_ms_per_step": t_train / max(nsteps, 1) * 1e3, "final_train_loss": final_loss,
             "plain_physics_grids_per_s": 1.0 / t_plain, "plain_physics_ms": t_plain * 1e3,
@@ -1004,7 +1004,7 @@ def main():
                          "operators at T511 x 64, GB/s per kernel")
     ap.add_argument("--profile-run", action="store_true",
                     help="only W + K round trips of one precision (default bf16x3), for profilers")
-    ap.add_argument("--train-epochs", type=int, default=20, help="column-emulator: training epochs")
+    ap.add_argument("--train-epochs", type=int, default=120, help="column-emulator: training epochs")
     ap.add_argument("--ref-seconds", type=float, default=240.0,
                     help="reference arm: CPU seconds for all steps; steps of all 64 layers unless they "
                          "would take longer")
