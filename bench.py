@@ -628,6 +628,22 @@ def run_operators(args):
                      "frac_of_measured_hbm": (gbs / peak) if peak else None}
     assert S.device_status() == 0
     total = sum(r["ms"] for r in res.values())
+    # CPU beside it: the six operators once each through the FP64 numpy restatement of
+    # spectral_gradients.jl on the same [nlm][64] shapes (host threads as numpy uses them)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sht_oracle as O
+    osp = O.Spectrum(T + 1, T)
+    rng = np.random.default_rng(1)
+    cu = rng.standard_normal((osp.nlm, K)) + 1j * rng.standard_normal((osp.nlm, K))
+    cv = rng.standard_normal((osp.nlm, K)) + 1j * rng.standard_normal((osp.nlm, K))
+    t0 = time.perf_counter()
+    O.curl(osp, cu, cv, radius=6.371e6)
+    O.divergence(osp, cu, cv, radius=6.371e6)
+    O.UV_from_vordiv(osp, cu, cv, radius=6.371e6)
+    O.laplace(osp, cu, radius=6.371e6)
+    O.laplace(osp, cu, inverse=True, radius=6.371e6)
+    O.gradient(osp, cu, radius=6.371e6)
+    cpu_s = time.perf_counter() - t0
     line = {"metric": "spectral operators at T511 x 64 layers (lmax = mmax + 1 = 513), achieved HBM GB/s",
             "value": sum(r["algorithmic_bytes"] for r in res.values()) / (total * 1e-3) / 1e9, "unit": "GB/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total,
@@ -637,7 +653,11 @@ def run_operators(args):
                                    "on [64][nlm] complex FP32 fields, each call timed alone",
                        "nlm": spec.nlm, "layers": K, "field_mb": nbytes / 1e6,
                        "l2": "three sets of fields in turn, so consecutive calls share no data (810 MB)"},
-            "by_operator": res}
+            "by_operator": res,
+            "cpu_baseline": {"value": sum(r["algorithmic_bytes"] for r in res.values()) / cpu_s / 1e9,
+                             "unit": "GB/s", "cores": os.cpu_count(),
+                             "kind": "port", "ms_all_six": cpu_s * 1e3,
+                             "sample": "the six operators once each, FP64 numpy restatement (oracle), same shapes"}}
     print(json.dumps(line))
     return 0
 
@@ -701,6 +721,22 @@ def run_matrix(args):
         st.transform_(field, lt, S)
         st.transform_(out, field, S)
     res["spectral_transform_fp32"] = {"ms": timed(sstep)}
+    # CPU beside it: the reference's Float32 mul! is a BLAS SGEMM; numpy's FP32 matmul (BLAS,
+    # all host threads) on the same shapes, a synthesis and an analysis product per round trip
+    rng = np.random.default_rng(0)
+    A_ana = rng.standard_normal((2 * spec.nlm, grid.npoints), dtype=np.float32)
+    A_syn = rng.standard_normal((grid.npoints, 2 * spec.nlm), dtype=np.float32)
+    xs = rng.standard_normal((2 * spec.nlm, K), dtype=np.float32)
+    xg = rng.standard_normal((grid.npoints, K), dtype=np.float32)
+    A_syn @ xs
+    A_ana @ xg
+    t0 = time.perf_counter()
+    ncpu = 0
+    while time.perf_counter() - t0 < 3.0 or ncpu < 3:
+        A_syn @ xs
+        A_ana @ xg
+        ncpu += 1
+    cpu_rt = ncpu / (time.perf_counter() - t0)
     r = res["fp32"]
     line = {"metric": "MatrixSpectralTransform round trips per second, T63 octahedral nlat 96 x 8 layers, FP32",
             "value": r["round_trips_per_s"], "unit": "round trips/s", "n_gpus": 1, "steps": args.steps,
@@ -713,7 +749,9 @@ def run_matrix(args):
             "config": {"workload": "dense-matrix synthesis + analysis, T63 OctahedralGaussianGrid nlat 96 x 8 layers",
                        "npoints": grid.npoints, "nlm": spec.nlm,
                        "l2": "each 188 MB matrix exceeds the L2; the directions alternate"},
-            "by_precision": res}
+            "by_precision": res,
+            "cpu_baseline": {"value": cpu_rt, "unit": "round trips/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{ncpu} round trips: numpy FP32 matmul (BLAS) of the two dense products"}}
     print(json.dumps(line))
     return 0
 
