@@ -280,6 +280,23 @@ SHT_API int sht_plan_set_tile_columns(sht_plan* plan, int synthesis, int analysi
 SHT_API int sht_plan_set_fusion(sht_plan* plan, int mode);
 SHT_API int sht_plan_get_fusion(const sht_plan* plan, int32_t* mode, int32_t* available);
 
+/* Prime stages of the ring FFTs. A ring of n = p nb points whose largest prime factor p
+ * is at least 64 (octahedral rings n = 16 + 4j from n = 256 on; none on full grids of
+ * smooth lengths) starts its FFT with nb direct DFTs of length p. SHT_PRIME_TENSOR runs
+ * that stage for all such rings and all layers as one tcgen05 launch (three TF32
+ * products, FP32 accumulation, about 22 significant bits per term) ahead of the FFT
+ * kernel, through a buffer of sum(n) x nlayers complex values over those rings (allocated
+ * when the mode is first set); SHT_PRIME_DIRECT, the default, runs it inside the FFT
+ * kernel on the FP32 pipes (faster on B200 at T511 x 64: 0.30 / 0.24 ms against 0.38 /
+ * 0.36 ms per analysis / synthesis Fourier stage). The two agree to FP32 rounding, not
+ * bit for bit. Fused transforms and batches always run the stage inside their FFT
+ * kernels. sht_plan_get_prime_stage: the mode and whether the plan has such rings (either
+ * pointer may be NULL). */
+#define SHT_PRIME_DIRECT 0
+#define SHT_PRIME_TENSOR 1
+SHT_API int sht_plan_set_prime_stage(sht_plan* plan, int mode);
+SHT_API int sht_plan_get_prime_stage(const sht_plan* plan, int32_t* mode, int32_t* available);
+
 /* ---- batches: many transforms (different plans, truncations, layer counts) in one
  * grouped launch per stage, optionally captured as one CUDA graph ---------------------
  * replaces the per-transform launch sequences of a time step

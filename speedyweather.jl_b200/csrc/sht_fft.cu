@@ -352,12 +352,18 @@ __device__ void stage_prime(float2* __restrict__ X, float2* __restrict__ Y, int 
     }
 }
 
-// Runs all stages; returns the buffer holding the result. G: the ring's prime tables.
+// Runs the stages from `first` on (1: the first, a prime radix, was done by the
+// tensor-core kernel and its output is in X); returns the buffer holding the result.
+// G: the ring's prime tables.
 template <bool INV>
 __device__ float2* run_fft(float2* X, float2* Y, int n, int ldx, int C, const RingDesc& rd, const float2* W,
-                           const float2* G, bool raw_first = false) {
+                           const float2* G, bool raw_first = false, int first = 0) {
     int Ns = 1;
-    for (int s = 0; s < rd.nfac; ++s) {
+    if (first) {
+        Ns = rd.fac[0];
+        G += 3 * prime_hpad(rd.fac[0]);
+    }
+    for (int s = first; s < rd.nfac; ++s) {
         const int p = rd.fac[s];
         if (p > 8) {
             if (Ns > 1) {
@@ -576,13 +582,6 @@ __device__ __forceinline__ float ana_weight(const RingDesc& rd, int m, int adjoi
     const float sm = (m == 0 || 2 * m == rd.n) ? 1.f : 2.f;
     return 0.5f * sm * (unscale ? rd.coslat_inv : 1.f);
 }
-// Factor of the Fourier coefficients of order m in the synthesis prologue: 1 / cos(lat)
-// or 1 for the transform; for the adjoint of the analysis the solid angle / the rfft
-// adjoint scale (SpeedyTransformsEnzymeExt.jl:294-323).
-__device__ __forceinline__ float syn_weight(const RingDesc& rd, int m, int adjoint, int unscale) {
-    if (!adjoint) return unscale ? rd.coslat_inv : 1.f;
-    return (m == 0 || 2 * m == rd.n) ? rd.domega : 0.5f * rd.domega;
-}
 
 // grid -> Fourier scratch (E/O combinations weighted by the solid angle), one work
 // item (ring, layer chunk) of one transform. IMG: the tensor-core operand-image epilogue
@@ -615,11 +614,22 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
     // register path.
     const bool avec = ((ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(grid) & 15) == 0) &&
                       ((rd.off_north & 3) == 0) && ((rd.off_south & 3) == 0) && ((n & 3) == 0);
-    const bool raw_first = avec && rd.nfac > 0;
+    const bool pre = v.ymid != nullptr && rd.pre;
+    const bool raw_first = !pre && avec && rd.nfac > 0;
     float2* const land = raw_first ? X : Y;
     copy_twiddles_async(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
     const int n4 = n >> 2;
-    if (avec) {
+    if (pre) {
+        // the first stage's output, [k][n] per ring, straight into X (n even: 16-byte runs)
+        const int n2 = n >> 1;
+        const Div dn2 = mkdiv(n2);
+        const float2* src0 = v.ymid + rd.yofs + (int64_t)k0 * n;
+        for (int w = threadIdx.x; w < C * n2; w += blockDim.x) {
+            const int c = quo(w, dn2);
+            const int i2 = w - c * n2;
+            cp_async16(X + c * ldx + 2 * i2, src0 + (int64_t)c * n + 2 * i2);
+        }
+    } else if (avec) {
         const Div d2n4 = mkdiv(2 * n4);
         for (int w = threadIdx.x; w < C * 2 * n4; w += blockDim.x) {
             const int c = quo(w, d2n4);
@@ -632,8 +642,9 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
     }
     cp_async_wait_all();
     __syncthreads();
-    if (raw_first) {
-        // the prime stage reads the raw layout (visible after the barrier above)
+    if (raw_first || pre) {
+        // the prime stage reads the raw layout, or the prime stage's output is in place
+        // (visible after the barrier above)
     } else if (avec) {
         const Div dn4 = mkdiv(n4);
         for (int w = threadIdx.x; w < C * n4; w += blockDim.x) {
@@ -649,8 +660,8 @@ __device__ void fft_analysis_body(const FftView& v, int ring, int chunk, float2*
     } else {
         load_rings(X, grid, ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn);
     }
-    if (!raw_first) __syncthreads();
-    const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G, raw_first);
+    if (!raw_first && !pre) __syncthreads();
+    const float2* Z = run_fft<false>(X, Y, n, ldx, C, rd, W, G, raw_first, pre ? 1 : 0);
     const int adj = v.adjoint, unsc = v.unscale;
     const int nm = rd.mt + 1;
     if (IMG && img.base != nullptr) {
@@ -762,9 +773,25 @@ __device__ void fft_synthesis_body(const FftView& v, int ring, int chunk, float2
     // The scratch rows r = 2 m + eo (m <= mt) of the C layers land in Y as [r][c] by
     // asynchronous copies issued together with the twiddles (2 (mt + 1) <= ldx). Odd
     // layer counts or offsets read the scratch directly.
+    copy_twiddles_async(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
+    if (v.ymid != nullptr && rd.pre) {
+        // the first stage ran on the tensor cores: its output, [k][n] per ring, into X
+        const int n2 = n >> 1;
+        const Div dn2 = mkdiv(n2);
+        const float2* src0 = v.ymid + rd.yofs + (int64_t)k0 * n;
+        for (int w = threadIdx.x; w < C * n2; w += blockDim.x) {
+            const int c = quo(w, dn2);
+            const int i2 = w - c * n2;
+            cp_async16(X + c * ldx + 2 * i2, src0 + (int64_t)c * n + 2 * i2);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        const float2* z = run_fft<true>(X, Y, n, ldx, C, rd, W, G, false, 1);
+        store_rings(grid, ldg, rd.off_north, rd.off_south, k0, C, n, ldx, dn, z, add);
+        return;
+    }
     const bool svec = ((K & 1) == 0) && ((k0 & 1) == 0) && ((C & 1) == 0) &&
                       ((reinterpret_cast<uintptr_t>(four) & 15) == 0);
-    copy_twiddles_async(W, twiddle + rd.tw_off, smem_tw_len(n) + rd.gen_len);
     if (svec) {
         const int half = C / 2, nrow = 2 * (rd.mt + 1);
         const Div dh = mkdiv(half);
@@ -1306,6 +1333,7 @@ FftView fft_view(const Plan& p, const float* gin, float* gout, int64_t ldg, floa
     v.add = (flags & SHT_ADD) ? 1 : 0;
     v.adjoint = adjoint ? 1 : 0;
     if (image) v.img = p.ana_img;
+    v.ymid = nullptr;   // set by the launches that run the tensor-core first stages
     return v;
 }
 
@@ -1332,17 +1360,24 @@ cudaError_t launch_fft_analysis(const Plan& p, const float* grid, int64_t ldg, i
         const cudaError_t e = tc_analysis_scale(p, grid, ldg, K, s, mul);
         if (e != cudaSuccess) return e;
     }
-    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(
-        p.d_fft_items, fft_view(p, grid, nullptr, ldg, p.d_four, K, flags & SHT_UNSCALE_COSLAT, to_image || p.tc,
-                                adjoint));
+    FftView v = fft_view(p, grid, nullptr, ldg, p.d_four, K, flags & SHT_UNSCALE_COSLAT, to_image || p.tc, adjoint);
+    if ((v.ymid = prime_buffer(p)) != nullptr) {
+        const cudaError_t e = launch_prime_stage(p, false, grid, ldg, K, flags, adjoint, s);
+        if (e != cudaSuccess) return e;
+    }
+    fft_analysis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, v);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fft_synthesis(const Plan& p, float* grid, int64_t ldg, int K, unsigned flags, cudaStream_t s,
                                  bool adjoint) {
     const dim3 g(p.n_fft_items);
-    fft_synthesis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(
-        p.d_fft_items, fft_view(p, nullptr, grid, ldg, p.d_four, K, flags, false, adjoint));
+    FftView v = fft_view(p, nullptr, grid, ldg, p.d_four, K, flags, false, adjoint);
+    if ((v.ymid = prime_buffer(p)) != nullptr) {
+        const cudaError_t e = launch_prime_stage(p, true, nullptr, 0, K, flags, adjoint, s);
+        if (e != cudaSuccess) return e;
+    }
+    fft_synthesis_kernel<<<g, fft_threads(p), p.smem_fft, s>>>(p.d_fft_items, v);
     return cudaGetLastError();
 }
 

@@ -45,6 +45,9 @@ struct RingDesc {
     int64_t tw_off;       // offset of this ring's twiddles ((n + 1) & ~1 entries) and prime tables
     float domega;         // solid angle w_j 2pi / n_j
     float coslat_inv;     // 1 / cos(latitude)
+    int32_t pre;          // 1: the first stage (a large prime radix) may run on the tensor cores
+    int32_t spare;
+    int64_t yofs;         // float2 offset of this ring's first-stage output [k][n] in the prime buffer
     int32_t fac[kMaxFactors];
 };
 
@@ -102,6 +105,7 @@ struct FftView {
     int K, unscale, add;
     int adjoint;          // 1: the adjoint weights (of the synthesis for the analysis direction and v.v.)
     TcImage img;          // analysis operand image of tensor-core plans (base == nullptr: FP32 scratch)
+    float2* ymid;         // first-stage output of the rings with pre = 1 (nullptr: every stage in the FFT kernel)
 };
 
 // The operands of a fused (FFT + Legendre in one launch) transform of an FP32 plan:
@@ -173,6 +177,8 @@ struct Plan {
     int64_t table_bytes = 0;
     int32_t* d_err = nullptr;           // device status word of the bounded waits (0 = ok)
     void* tc = nullptr;                 // tensor-core Legendre state (sht_legendre_tc.cu)
+    void* prime = nullptr;              // tensor-core prime stages of the ring FFTs (sht_prime_tc.cu)
+    int prime_mode = 0;                 // 1: the FFT launches run those stages on the tensor cores
     TcImage ana_img;                    // analysis data image written by the FFT (tensor-core plans)
     int smem_fft = 0;                   // dynamic shared memory of the FFT kernels
     int min_chunk = 1;
@@ -250,5 +256,26 @@ cudaError_t launch_fused_analysis(const Plan& p, const float* grid, int64_t ldg,
                                   bool add, cudaStream_t s);
 cudaError_t launch_gradient(const Plan& p, float2* dpdx, float2* dpdy, const float2* in, int64_t ldc,
                             int K, float inv_radius, cudaStream_t s);
+// tensor-core first stages of the ring FFTs (sht_prime_tc.cu). prime_prepare marks the
+// rings whose first radix is a prime of at least kPrimeTcMin (RingDesc.pre, yofs) before
+// the rings are uploaded and returns the prime buffer's length in float2;
+// prime_create builds the stage matrices and the work list once the plan is on the device.
+constexpr int kPrimeTcMin = 64;
+int64_t prime_mark_rings(std::vector<RingDesc>& rings, int nlayers);
+cudaError_t prime_create(Plan& p, int64_t ymid_elems);
+void prime_release(Plan& p);
+bool prime_available(const Plan& p);
+cudaError_t prime_set_mode(Plan& p, int mode);    // 0: FFT kernels only, 1: tensor-core first stages
+float2* prime_buffer(const Plan& p);               // the first-stage output when the mode is 1, else nullptr
+cudaError_t launch_prime_stage(const Plan& p, bool synthesis, const float* grid, int64_t ldg, int K,
+                               unsigned flags, bool adjoint, cudaStream_t s);
+
+// Factor of the Fourier coefficients of order m in the synthesis prologue: 1 / cos(lat)
+// or 1 for the transform; for the adjoint of the analysis the solid angle / the rfft
+// adjoint scale (SpeedyTransformsEnzymeExt.jl:294-323).
+__device__ __forceinline__ float syn_weight(const RingDesc& rd, int m, int adjoint, int unscale) {
+    if (!adjoint) return unscale ? rd.coslat_inv : 1.f;
+    return (m == 0 || 2 * m == rd.n) ? rd.domega : 0.5f * rd.domega;
+}
 
 }  // namespace sht

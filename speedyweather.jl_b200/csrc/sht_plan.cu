@@ -130,6 +130,44 @@ int factorize(int n, int32_t* fac) {
     return (int)out.size();
 }
 
+// FFT cost of one layer of a ring: FMAs of the prime stages (2 n hpad each) plus ~3 n per
+// small-radix stage and ~4 n of copies; with pre, the first (prime) stage runs elsewhere.
+double fft_ring_cost(const RingDesc& r, bool pre) {
+    double per_layer = 4.0 * r.n;
+    for (int s2 = (pre && r.pre) ? 1 : 0; s2 < r.nfac; ++s2)
+        per_layer += r.fac[s2] > 8 ? 2.0 * r.n * ((r.fac[s2] - 1) / 2 + kPrimeGroup - 1) / kPrimeGroup * kPrimeGroup
+                                   : 3.0 * r.n;
+    return per_layer;
+}
+
+// FFT work list: one CTA per (ring, chunk of layers), issued costliest first so that the
+// last wave holds the cheapest CTAs.
+std::vector<int2> fft_item_order(const Plan& p, bool pre) {
+    std::vector<std::pair<double, int2>> fitems;
+    const int kmax = std::max(1, p.d.nlayers);
+    for (int j = 0; j < (int)p.h_rings.size(); ++j) {
+        const RingDesc& r = p.h_rings[j];
+        const double per_layer = fft_ring_cost(r, pre);
+        for (int ci = 0; ci * r.chunk < kmax; ++ci) {
+            const int c = std::min(r.chunk, kmax - ci * r.chunk);
+            fitems.push_back({c * per_layer, make_int2(j, ci)});
+        }
+    }
+    std::stable_sort(fitems.begin(), fitems.end(),
+                     [](const std::pair<double, int2>& a, const std::pair<double, int2>& b) { return a.first > b.first; });
+    std::vector<int2> out;
+    for (auto& f : fitems) out.push_back(f.second);
+    return out;
+}
+
+// Turns the tensor-core first stages on or off and reorders the FFT work list for it.
+cudaError_t apply_prime_mode(Plan& p, int mode) {
+    cudaError_t e = prime_set_mode(p, mode);
+    if (e != cudaSuccess) return e;
+    const std::vector<int2> items = fft_item_order(p, p.prime_mode != 0);
+    return cudaMemcpy(p.d_fft_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice);
+}
+
 // Table block of a prime stage p > 8 (layout and use in sht_fft.cu, stage_prime):
 // T[e] = (cos, sin)(2 pi g^(e - hpad + 1) / p) for e < 2 hpad, q_b = g^-b, r_a = g^a.
 static int primitive_root(int p) {
@@ -207,6 +245,7 @@ cudaError_t upload(T** dst, const std::vector<T>& src, int64_t& bytes) {
 
 void release(Plan& p) {
     tc_release(p);
+    prime_release(p);
     void* ptrs[] = {p.d_rings, p.d_twiddle, p.d_lam, p.d_lam_off, p.d_j0, p.d_rows, p.d_lm_off, p.d_syn_items,
                     p.d_ana_items, p.d_mt, p.d_gofs, p.d_grad, p.d_l_of, p.d_m_of, p.d_eig, p.d_eig_inv, p.d_four,
                     p.d_err, p.d_fft_items};
@@ -385,36 +424,12 @@ int build_plan(Plan& p) {
     p.scratch_rows = gofs;
     p.smem_fft = max_smem;
 
-    // --- FFT work list: one CTA per (ring, chunk of layers), issued costliest first so
-    // that the last wave holds the cheapest CTAs. Cost per layer: FMAs of the prime
-    // stages (2 n hpad each) plus ~3 n per small-radix stage and ~4 n of copies.
-    std::vector<std::pair<double, int2>> fitems;
-    const int kmax = std::max(1, d.nlayers);
-    for (int j = 0; j < nh; ++j) {
-        const RingDesc& r = rings[j];
-        double per_layer = 4.0 * r.n;
-        for (int s2 = 0; s2 < r.nfac; ++s2)
-            per_layer += r.fac[s2] > 8 ? 2.0 * r.n * ((r.fac[s2] - 1) / 2 + kPrimeGroup - 1) / kPrimeGroup * kPrimeGroup
-                                       : 3.0 * r.n;
-        for (int ci = 0; ci * r.chunk < kmax; ++ci) {
-            const int c = std::min(r.chunk, kmax - ci * r.chunk);
-            fitems.push_back({c * per_layer, make_int2(j, ci)});
-        }
-    }
-    std::stable_sort(fitems.begin(), fitems.end(),
-                     [](const std::pair<double, int2>& a, const std::pair<double, int2>& b) { return a.first > b.first; });
-    std::vector<int2> fft_items;
-    for (auto& f : fitems) fft_items.push_back(f.second);
+    // rings whose first stage may run on the tensor cores (sht_prime_tc.cu)
+    const int64_t ymid_elems = prime_mark_rings(rings, d.nlayers);
     p.h_rings = rings;
     p.h_ring_cost.assign(nh, 0.0);
-    for (int j = 0; j < nh; ++j) {
-        const RingDesc& r = rings[j];
-        double per_layer = 4.0 * r.n;
-        for (int s2 = 0; s2 < r.nfac; ++s2)
-            per_layer += r.fac[s2] > 8 ? 2.0 * r.n * ((r.fac[s2] - 1) / 2 + kPrimeGroup - 1) / kPrimeGroup * kPrimeGroup
-                                       : 3.0 * r.n;
-        p.h_ring_cost[j] = per_layer;
-    }
+    for (int j = 0; j < nh; ++j) p.h_ring_cost[j] = fft_ring_cost(rings[j], false);
+    const std::vector<int2> fft_items = fft_item_order(p, false);
 
     // --- work lists of the Legendre kernels (64-row tiles, heavy orders first) ---
     std::vector<LegItem> syn, ana;
@@ -499,6 +514,8 @@ int build_plan(Plan& p) {
         if ((e = tc_prepare(p)) != cudaSuccess) return cuda_fail(e, "sht_plan_create tensor-core tables");
     }
     if ((e = fused_prepare(p)) != cudaSuccess) return cuda_fail(e, "sht_plan_create fused kernels");
+    // the tensor-core prime stages (off until sht_plan_set_prime_stage turns them on)
+    if ((e = prime_create(p, ymid_elems)) != cudaSuccess) return cuda_fail(e, "sht_plan_create prime stages");
     return SHT_OK;
 }
 
@@ -716,6 +733,25 @@ int sht_plan_set_tile_columns(sht_plan* plan, int synthesis, int analysis) {
     if (synthesis != analysis || !tc_set_tile_cols(p, synthesis))
         return fail(SHT_EINVAL, "sht_plan_set_tile_columns: tensor-core plans take 64 or 128 columns, the same for "
                                 "both directions");
+    return SHT_OK;
+}
+
+int sht_plan_set_prime_stage(sht_plan* plan, int mode) {
+    if (!plan) return fail(SHT_EINVAL, "sht_plan_set_prime_stage: NULL plan");
+    if (mode != SHT_PRIME_DIRECT && mode != SHT_PRIME_TENSOR)
+        return fail(SHT_EINVAL, "sht_plan_set_prime_stage: mode %d is neither SHT_PRIME_DIRECT nor SHT_PRIME_TENSOR",
+                    mode);
+    if (mode == SHT_PRIME_TENSOR && !tc_supported())
+        return fail(SHT_EUNSUPPORTED, "sht_plan_set_prime_stage: tensor cores (sm_100) not available");
+    DeviceGuard g(plan->p.device);
+    const cudaError_t e = apply_prime_mode(plan->p, mode);
+    return e == cudaSuccess ? SHT_OK : cuda_fail(e, "sht_plan_set_prime_stage");
+}
+
+int sht_plan_get_prime_stage(const sht_plan* plan, int32_t* mode, int32_t* available) {
+    if (!plan) return fail(SHT_EINVAL, "sht_plan_get_prime_stage: NULL plan");
+    if (mode) *mode = plan->p.prime_mode;
+    if (available) *available = prime_available(plan->p) ? 1 : 0;
     return SHT_OK;
 }
 

@@ -79,6 +79,8 @@ SIGNATURES = {
     "sht_plan_set_tile_columns": (C.c_int, [_P, C.c_int, C.c_int]),
     "sht_plan_set_fusion": (C.c_int, [_P, C.c_int]),
     "sht_plan_get_fusion": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "sht_plan_set_prime_stage": (C.c_int, [_P, C.c_int]),
+    "sht_plan_get_prime_stage": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "sht_synthesize_adjoint": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
     "sht_analyze_adjoint": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_uint, _P]),
     "sht_batch_create": (C.c_int, [C.POINTER(ShtBatchItem), C.c_int, C.POINTER(C.c_void_p)]),

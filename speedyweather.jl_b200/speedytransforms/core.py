@@ -364,6 +364,29 @@ class SpectralTransform:
         check(lib.sht_plan_get_fusion(self._plan, None, C.byref(ok)))
         return bool(ok.value)
 
+    @property
+    def prime_stage(self) -> str:
+        """Where the ring FFTs run their first stage when it is a prime radix p >= 64:
+        "tensor" (one tcgen05 launch for all such rings, three TF32 products) or "direct"
+        (inside the FFT kernel on the FP32 pipes, the default: faster at T511 x 64). Settable.
+        The two agree to FP32 rounding, not bit for bit."""
+        mode = C.c_int32(0)
+        check(lib.sht_plan_get_prime_stage(self._plan, C.byref(mode), None))
+        return "tensor" if mode.value else "direct"
+
+    @prime_stage.setter
+    def prime_stage(self, where: str):
+        if where not in ("tensor", "direct"):
+            raise ValueError(f"prime_stage must be 'tensor' or 'direct', not {where!r}")
+        check(lib.sht_plan_set_prime_stage(self._plan, 1 if where == "tensor" else 0))
+
+    @property
+    def prime_stage_available(self) -> bool:
+        """True when some ring's FFT starts with a prime radix p >= 64."""
+        ok = C.c_int32(0)
+        check(lib.sht_plan_get_prime_stage(self._plan, None, C.byref(ok)))
+        return bool(ok.value)
+
     def __repr__(self):
         return (f"SpectralTransform({self.spectrum}, {self.grid}, nlayers={self.nlayers}, "
                 f"precision={self.precision!r})")
