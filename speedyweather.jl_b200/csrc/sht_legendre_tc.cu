@@ -101,7 +101,8 @@ struct TcDev {
     int nmax;                      // columns of the data images (multiple of 64)
     int fp16;                      // 1: fp16 pieces with power-of-two scaling
     const int32_t* mexp;           // per m: e_m of the Legendre scaling
-    const float2* kscale_syn;      // per layer: (2^(e_k - 15), 2^(15 - e_k)) of the synthesis input
+    const float2* kscale_syn;      // per layer: (2^(e_k - 15), 2^(15 - e_k)) of the dense-matrix input
+    float2* mkscale_syn;           // per (m, layer), [m K + k]: the same for the synthesis input of order m
     const float2* kscale_ana;      // per layer: the same for the analysis data (E, O)
     // dense matrix transforms (MatrixSpectralTransform): one "order" m = 0 whose A operand
     // is the matrix; the epilogue writes out[n ldo + row] for the K layer columns n
@@ -136,6 +137,7 @@ struct TcState {
     int32_t* d_mexp = nullptr;
     float* d_absmax = nullptr;     // [2 nlayers]: synthesis, analysis max-abs of the call's input
     float2* d_kscale = nullptr;    // [2 nlayers]: (2^(e_k - 15), 2^(15 - e_k)) per layer
+    float2* d_mkscale = nullptr;   // [mmax][nlayers]: the same per order and layer (synthesis input)
     float ana_mul = 0.f;
 };
 
@@ -282,9 +284,10 @@ __device__ void epilogue_store(const TcDev& t, const TcItem& it, int ct, int ctw
             if (vm == 0) continue;
             const int k0 = (ct * ctw + c0) / 2;
             if (t.fp16) {
+                const float2* mk = t.mkscale_syn + (int64_t)m * K;
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
-                    const float f = t.kscale_syn[min(k0 + q, K - 1)].x;
+                    const float f = mk[min(k0 + q, K - 1)].x;
                     v[2 * q] = v[2 * q] * mscale * f;
                     v[2 * q + 1] = v[2 * q + 1] * mscale * f;
                 }
@@ -606,14 +609,12 @@ __device__ __forceinline__ void cp_async_8(uint32_t dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
 }
 
+// One 128-coefficient block kt of order m for the 32 layers from kbase: staged in shared
+// memory by asynchronous copies, scaled by sc (the fp16 data scale of this thread's layer;
+// 1 for bf16), split into NPB 16-bit pieces and written as swizzled image rows.
 template <int NPB, bool F16>
-__global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const float2* __restrict__ coeffs,
-                                                        int64_t ldc, int K) {
-    __shared__ __align__(16) uint8_t stage[32 * IMG_LAYER];
-    const int m = blockIdx.x;
-    const int kt = blockIdx.y;
-    if (kt >= t.nkt[m]) return;
-    const int kbase = blockIdx.z * 32;
+__device__ __forceinline__ void syn_image_block(const TcDev& t, const float2* __restrict__ coeffs, int64_t ldc,
+                                                int K, int m, int kt, int kbase, float sc, uint8_t* stage) {
     const int lmrem = t.lmax - m - 2 * BLK * kt;             // packed coefficients left from this block
     const float2* src0 = coeffs + t.lm_off[m] + 2 * BLK * kt;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(stage);
@@ -645,43 +646,94 @@ __global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const flo
     __syncthreads();
     const int ib8 = threadIdx.x & 7;
     const int k = kbase + (threadIdx.x >> 3);
-    if (k >= K) return;
-    float2 v[16];
-    const float4* run = reinterpret_cast<const float4*>(stage + (threadIdx.x >> 3) * IMG_LAYER + ib8 * IMG_RUN);
+    if (k < K) {
+        float2 v[16];
+        const float4* run = reinterpret_cast<const float4*>(stage + (threadIdx.x >> 3) * IMG_LAYER + ib8 * IMG_RUN);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const float4 f = run[q];
-        v[2 * q] = make_float2(f.x, f.y);
-        v[2 * q + 1] = make_float2(f.z, f.w);
-    }
-    if (F16) {
-        const float sc = t.kscale_syn[k].y;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = make_float2(v[q].x * sc, v[q].y * sc);
-    }
-    uint8_t* img = reinterpret_cast<uint8_t*>(const_cast<uint16_t*>(t.syn_img));
-#pragma unroll
-    for (int par = 0; par < 2; ++par) {
-        const int64_t tile = t.syn_tile_base[m] + (int64_t)par * t.nkt[m] + kt;
-#pragma unroll
-        for (int ri = 0; ri < 2; ++ri) {
-            const int c = 2 * k + ri;
-            uint32_t w[NPB][4];
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                float r0 = ri ? v[2 * (2 * h) + par].y : v[2 * (2 * h) + par].x;
-                float r1 = ri ? v[2 * (2 * h + 1) + par].y : v[2 * (2 * h + 1) + par].x;
-#pragma unroll
-                for (int q = 0; q < NPB; ++q) {
-                    w[q][h] = q + 1 < NPB ? piece_bits2<F16, true>(r0, r1) : piece_bits2<F16, false>(r0, r1);
-                }
-            }
-            const int64_t off = (int64_t)(c / 8) * 1024 + (c % 8) * 128 + ((ib8 ^ (c % 8)) * 16);
-#pragma unroll
-            for (int q = 0; q < NPB; ++q)
-                *reinterpret_cast<uint4*>(img + (tile * NPB + q) * t.syn_tile_bytes + off) =
-                    make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+        for (int q = 0; q < 8; ++q) {
+            const float4 f = run[q];
+            v[2 * q] = make_float2(f.x, f.y);
+            v[2 * q + 1] = make_float2(f.z, f.w);
         }
+        if (F16) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = make_float2(v[q].x * sc, v[q].y * sc);
+        }
+        uint8_t* img = reinterpret_cast<uint8_t*>(const_cast<uint16_t*>(t.syn_img));
+#pragma unroll
+        for (int par = 0; par < 2; ++par) {
+            const int64_t tile = t.syn_tile_base[m] + (int64_t)par * t.nkt[m] + kt;
+#pragma unroll
+            for (int ri = 0; ri < 2; ++ri) {
+                const int c = 2 * k + ri;
+                uint32_t w[NPB][4];
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    float r0 = ri ? v[2 * (2 * h) + par].y : v[2 * (2 * h) + par].x;
+                    float r1 = ri ? v[2 * (2 * h + 1) + par].y : v[2 * (2 * h + 1) + par].x;
+#pragma unroll
+                    for (int q = 0; q < NPB; ++q) {
+                        w[q][h] = q + 1 < NPB ? piece_bits2<F16, true>(r0, r1) : piece_bits2<F16, false>(r0, r1);
+                    }
+                }
+                const int64_t off = (int64_t)(c / 8) * 1024 + (c % 8) * 128 + ((ib8 ^ (c % 8)) * 16);
+#pragma unroll
+                for (int q = 0; q < NPB; ++q)
+                    *reinterpret_cast<uint4*>(img + (tile * NPB + q) * t.syn_tile_bytes + off) =
+                        make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+            }
+        }
+    }
+}
+
+// bf16 pieces: one block (m, kt, 32 layers).
+template <int NPB>
+__global__ void __launch_bounds__(256) syn_image_kernel(const TcDev t, const float2* __restrict__ coeffs,
+                                                        int64_t ldc, int K) {
+    __shared__ __align__(16) uint8_t stage[32 * IMG_LAYER];
+    const int m = blockIdx.x;
+    const int kt = blockIdx.y;
+    if (kt >= t.nkt[m]) return;
+    syn_image_block<NPB, false>(t, coeffs, ldc, K, m, kt, blockIdx.z * 32, 1.f, stage);
+}
+
+// fp16 pieces: one block per (m, 32 layers) takes all blocks kt of the order. It first
+// reduces each layer's max-abs over the order's coefficients (8 lanes per layer), which
+// sets the data scale 2^(15 - e_mk) of that order and layer (stored for the GEMM's
+// epilogue as (2^(e_mk - 15), 2^(15 - e_mk))), then writes the blocks; the second read
+// of the coefficients comes from L2.
+__global__ void __launch_bounds__(256) syn_image_f16_kernel(const TcDev t, const float2* __restrict__ coeffs,
+                                                            int64_t ldc, int K) {
+    __shared__ __align__(16) uint8_t stage[32 * IMG_LAYER];
+    const int m = blockIdx.x;
+    const int kbase = blockIdx.z * 32;
+    const int k = kbase + (threadIdx.x >> 3);
+    const int n = t.lmax - m;                                // coefficients of order m
+    float mx = 0.f;
+    if (k < K) {
+        const float2* src = coeffs + (int64_t)k * ldc + t.lm_off[m];
+        int e = threadIdx.x & 7;
+        for (; e + 24 < n; e += 32) {                        // four loads in flight
+            const float2 a = __ldg(src + e), b = __ldg(src + e + 8), c = __ldg(src + e + 16), d = __ldg(src + e + 24);
+            mx = fmaxf(mx, fmaxf(fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fmaxf(fabsf(b.x), fabsf(b.y))),
+                                 fmaxf(fmaxf(fabsf(c.x), fabsf(c.y)), fmaxf(fabsf(d.x), fabsf(d.y)))));
+        }
+        for (; e < n; e += 8) {
+            const float2 a = __ldg(src + e);
+            mx = fmaxf(mx, fmaxf(fabsf(a.x), fabsf(a.y)));
+        }
+    }
+    // the 8 lanes of a layer are consecutive lanes of one warp
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+    const int ex = scale_exp(mx);
+    if (k < K && (threadIdx.x & 7) == 0)
+        t.mkscale_syn[(int64_t)m * K + k] = make_float2(ldexpf(1.f, ex - F16_TOP), ldexpf(1.f, F16_TOP - ex));
+    const float sc = ldexpf(1.f, F16_TOP - ex);
+    for (int kt = 0; kt < t.nkt[m]; ++kt) {
+        if (kt > 0) __syncthreads();                         // the stage's previous block is consumed
+        syn_image_block<2, true>(t, coeffs, ldc, K, m, kt, kbase, sc, stage);
     }
 }
 
@@ -759,6 +811,7 @@ TcDev make_dev(const Plan& p) {
     t.fp16 = s.fp16;
     t.mexp = s.d_mexp;
     t.kscale_syn = s.d_kscale;
+    t.mkscale_syn = s.d_mkscale;
     t.kscale_ana = s.d_kscale ? s.d_kscale + p.d.nlayers : nullptr;
     return t;
 }
@@ -999,6 +1052,8 @@ cudaError_t tc_prepare(Plan& p) {
         if ((e = cudaMalloc(&s->d_absmax, 2 * sizeof(float) * std::max(1, p.d.nlayers))) != cudaSuccess) return e;
         if ((e = cudaMemset(s->d_absmax, 0, 2 * sizeof(float) * std::max(1, p.d.nlayers))) != cudaSuccess) return e;
         if ((e = cudaMalloc(&s->d_kscale, 2 * sizeof(float2) * std::max(1, p.d.nlayers))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&s->d_mkscale, sizeof(float2) * (size_t)p.mmax * std::max(1, p.d.nlayers))) != cudaSuccess)
+            return e;
         double wmax = 0.0;
         for (int j = 0; j < p.nlat; ++j) wmax = std::max(wmax, p.weights[j]);
         s->ana_mul = (float)(4.0 * M_PI * wmax * 1.0000001);
@@ -1023,7 +1078,7 @@ void tc_release(Plan& p) {
     if (!s) return;
     void* ptrs[] = {s->d_maps, s->d_lam, s->d_nr, s->d_nkt, s->d_njt, s->d_syn_base, s->d_ana_base,
                     s->d_syn_img, s->d_ana_img, s->d_syn_items, s->d_ana_items, s->d_mexp, s->d_absmax,
-                    s->d_kscale};
+                    s->d_kscale, s->d_mkscale};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete s;
@@ -1040,20 +1095,13 @@ cudaError_t launch_legendre_synthesis_tc(const Plan& p, const float2* coeffs, in
     const TcState& s = *static_cast<const TcState*>(p.tc);
     const TcDev t = make_dev(p);
     cudaError_t e;
-    if (s.fp16 && K > 0) {
-        if ((e = cudaMemsetAsync(s.d_absmax, 0, sizeof(float) * K, st)) != cudaSuccess) return e;
-        // a complex layer is 2 nlm floats
-        absmax_kernel<<<dim3(std::max(1, 2 * s.nsm / std::max(1, K)) * 4, K), 256, 0, st>>>(
-            reinterpret_cast<const float*>(coeffs), 2 * ldc, 2 * p.nlm, s.d_absmax);
-        kscale_kernel<<<1, 256, 0, st>>>(s.d_absmax, 1.f, K, s.d_kscale);
-    }
     const dim3 ig(p.mmax, (p.rows[0] + BLK - 1) / BLK, (K + 31) / 32);
     if (s.fp16)
-        syn_image_kernel<2, true><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
+        syn_image_f16_kernel<<<dim3(p.mmax, 1, (K + 31) / 32), 256, 0, st>>>(t, coeffs, ldc, K);
     else if (s.npb == 2)
-        syn_image_kernel<2, false><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
+        syn_image_kernel<2><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
     else
-        syn_image_kernel<3, false><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
+        syn_image_kernel<3><<<ig, 256, 0, st>>>(t, coeffs, ldc, K);
     e = cudaGetLastError();
     if (e != cudaSuccess || s.n_syn_items == 0) return e;
     const int ncols = 2 * K;
