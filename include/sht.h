@@ -54,8 +54,9 @@ extern "C" {
 #define SHT_PREC_FP32 0          /* FP32 CUDA-core FMA, matches the reference's Float32 */
 #define SHT_PREC_BF16X3 1        /* tcgen05, split-BF16 hi/lo operands, 3 products, FP32 accumulate */
 #define SHT_PREC_FP16X3 2        /* tcgen05, split-FP16 hi/lo, 3 products, FP32 accumulate; Legendre
-                                    polynomials scaled by 2^-e per order m, data by 2^-e per layer
-                                    from a max-abs pass over each call's input */
+                                    polynomials scaled by 2^-e per order m, data by 2^-e per order
+                                    and layer (synthesis) or per layer (analysis) from the max-abs
+                                    of each call's input */
 #define SHT_PREC_BF16X5 3        /* tcgen05, Legendre polynomials in 3 bf16 pieces (from FP64), data
                                     in 2, the 5 products above the split residual, FP32 accumulate */
 

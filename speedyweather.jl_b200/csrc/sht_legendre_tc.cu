@@ -13,12 +13,13 @@
 //   SHT_PREC_BF16X5: Lam in 3 bf16 pieces (from FP64), data in 2:
 //                    L0 B0 + L0 B1 + L1 B0 + L1 B1 + L2 B0
 //   SHT_PREC_FP16X3: as BF16X3 with fp16 pieces (11-bit significands), Lam scaled by
-//                    2^(15 - e_m) per order and the data by 2^(15 - e_k) per layer
-//                    (e from a max-abs reduction of the call's input), so that the
-//                    largest values sit in [2^14, 2^15): both pieces stay normal fp16
-//                    numbers down to 2^-18 of the maximum, and the products stay far
-//                    inside FP32's range. The epilogue multiplies by 2^(e_m + e_k - 30),
-//                    which is exact.
+//                    2^(15 - e_m) per order and the data by 2^(15 - e) with e from
+//                    the max-abs of the call's input: per order and layer for the
+//                    synthesis (reduced by the image kernel), per layer for the analysis
+//                    (a pass over the grid), so that the largest values sit in
+//                    [2^14, 2^15): both pieces stay normal fp16 numbers down to 2^-18 of
+//                    the maximum, and the products stay far inside FP32's range. The
+//                    epilogue multiplies by 2^(e_m + e - 30), which is exact.
 //
 // Operands in shared memory use the SWIZZLE_128B canonical layouts of tcgen05:
 // * Lam[m][p] is stored [piece][i][j - j0(m)] in global memory; one TMA tensor map

@@ -4,7 +4,7 @@ Tolerances (relative L2 vs FP64) at T31-T127, measured per direction (worst of 1
 layers, T31-T255): split BF16 with 3 products 5.7e-6 (round trip 7.8e-6), so 1e-5;
 the 5-product form (Legendre polynomials in three BF16 pieces) 4.3e-6, so 5e-6;
 split FP16 with 3 products (11-bit pieces, power-of-two scaling of the Legendre
-polynomials per order and of the data per layer) 5e-7, so 1e-6. The T511 x 64 tests
+polynomials per order and of the data per order and layer or per layer) 5e-7, so 1e-6. The T511 x 64 tests
 check each layer against the 1e-5 bar (FP16 and the 5-product BF16 meet it; the
 3-product BF16 does not on every layer, and its test pins its level).
 """
