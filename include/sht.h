@@ -291,8 +291,9 @@ SHT_API int sht_plan_get_fusion(const sht_plan* plan, int32_t* mode, int32_t* av
  * kernel on the FP32 pipes (faster on B200 at T511 x 64: 0.30 / 0.24 ms against 0.38 /
  * 0.36 ms per analysis / synthesis Fourier stage). The two agree to FP32 rounding, not
  * bit for bit. Fused transforms and batches always run the stage inside their FFT
- * kernels. sht_plan_get_prime_stage: the mode and whether the plan has such rings (either
- * pointer may be NULL). */
+ * kernels. On a plan without such rings SHT_PRIME_TENSOR leaves the mode at
+ * SHT_PRIME_DIRECT. sht_plan_get_prime_stage: the mode and whether the plan has such rings
+ * (either pointer may be NULL). */
 #define SHT_PRIME_DIRECT 0
 #define SHT_PRIME_TENSOR 1
 SHT_API int sht_plan_set_prime_stage(sht_plan* plan, int mode);
