@@ -793,6 +793,8 @@ def profile_run(args):
     field = st.Field.zeros(grid, LAYERS, device=device)
     out = st.LowerTriangularArray.zeros(spec, LAYERS, device=device)
     S = st.SpectralTransform(spec, grid, nlayers=LAYERS, precision=prec, device=device)
+    if args.prime_stage != "direct":
+        S.prime_stage = args.prime_stage
     for _ in range(args.warmup + args.steps):
         st.transform_(field, lt, S)
         st.transform_(out, field, S)
@@ -835,6 +837,8 @@ def run_ours(args):
         # the library's autotuner (tile widths; results do not depend on them), once per
         # plan before anything is timed, as a user sets a plan up
         variants.setdefault(prec, {})["tile_columns"] = list(S.autotune())
+        if args.prime_stage != "direct":
+            S.prime_stage = args.prime_stage
         transforms[prec] = S
 
     # accuracy vs the FP64 oracle on every layer (rank 0), outside any timed region: the
@@ -1025,6 +1029,8 @@ def run_ours(args):
     # synthesis data image (which, for fp16, also finds the data scales), plus for fp16 the
     # analysis input's max-abs pass and its scale kernel
     launches_per_rt = {"fp32": 4, "bf16x3": 5, "bf16x5": 5, "fp16x3": 7}[head]
+    if args.prime_stage == "tensor":
+        launches_per_rt += 2                       # the tensor-core prime stage ahead of each FFT
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": head, "data": "synthetic",
@@ -1036,6 +1042,8 @@ def run_ours(args):
             "graph": {"ms_per_round_trip": graph_ms, "round_trips_per_s": world * 1e3 / graph_ms,
                       "round_trips_per_replay": GRAPH_RT},
             "variants": variants}
+    if args.prime_stage != "direct":
+        line["prime_stage"] = args.prime_stage
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
     if rank == 0:
@@ -1056,6 +1064,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16x3", "fp16x3", "bf16x5"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--prime-stage", default="direct", choices=["direct", "tensor"],
+                    help="where the ring FFTs' prime-radix first stages run (sht_plan_set_prime_stage)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="t511",
                     choices=["t511", "mixed-batch", "column-emulator", "dycore-step", "operators", "matrix", "fused"],
