@@ -256,10 +256,11 @@ cudaError_t launch_fused_analysis(const Plan& p, const float* grid, int64_t ldg,
                                   bool add, cudaStream_t s);
 cudaError_t launch_gradient(const Plan& p, float2* dpdx, float2* dpdy, const float2* in, int64_t ldc,
                             int K, float inv_radius, cudaStream_t s);
-// tensor-core first stages of the ring FFTs (sht_prime_tc.cu). prime_prepare marks the
+// tensor-core first stages of the ring FFTs (sht_prime_tc.cu). prime_mark_rings marks the
 // rings whose first radix is a prime of at least kPrimeTcMin (RingDesc.pre, yofs) before
-// the rings are uploaded and returns the prime buffer's length in float2;
-// prime_create builds the stage matrices and the work list once the plan is on the device.
+// the rings are uploaded and returns the prime buffer's length in float2; prime_create
+// records it, and the first prime_set_mode(p, 1) builds the stage matrices, the work list
+// and the buffer.
 constexpr int kPrimeTcMin = 64;
 int64_t prime_mark_rings(std::vector<RingDesc>& rings, int nlayers);
 cudaError_t prime_create(Plan& p, int64_t ymid_elems);

@@ -430,6 +430,13 @@ cudaError_t prime_create(Plan& p, int64_t ymid_elems) {
     if (ymid_elems == 0) return cudaSuccess;
     PrimeState* st = new PrimeState();
     st->ymid_elems = ymid_elems;
+    p.prime = st;               // the tables are built when the mode is first turned on
+    return cudaSuccess;
+}
+
+namespace {
+// Stage matrices, ring descriptors and the work list, on the device.
+cudaError_t prime_build(Plan& p, PrimeState* st) {
     std::vector<PrimeRing> prs;
     std::vector<float> mat;
     std::map<int, int64_t> mofs;
@@ -505,10 +512,18 @@ cudaError_t prime_create(Plan& p, int64_t ymid_elems) {
         e = cudaFuncSetAttribute(prime_stage_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, PT_SMEM);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(prime_stage_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, PT_SMEM);
-    p.prime = st;
-    if (e == cudaSuccess) p.table_bytes += (int64_t)(mat.size() * sizeof(float) + prs.size() * sizeof(PrimeRing));
+    if (e == cudaSuccess) {
+        p.table_bytes += (int64_t)(mat.size() * sizeof(float) + prs.size() * sizeof(PrimeRing));
+    } else {           // leave nothing half-built: a later call starts over
+        for (void** q : {(void**)&st->d_prs, (void**)&st->d_items, (void**)&st->d_mat}) {
+            if (*q) cudaFree(*q);
+            *q = nullptr;
+        }
+        st->nitems = 0;
+    }
     return e;
 }
+}  // namespace
 
 void prime_release(Plan& p) {
     PrimeState* st = static_cast<PrimeState*>(p.prime);
@@ -528,6 +543,10 @@ cudaError_t prime_set_mode(Plan& p, int mode) {
     if (!st) {
         p.prime_mode = 0;
         return cudaSuccess;
+    }
+    if (mode && !st->d_mat) {
+        const cudaError_t e = prime_build(p, st);
+        if (e != cudaSuccess) return e;
     }
     if (mode && !st->d_ymid) {
         const cudaError_t e = cudaMalloc((void**)&st->d_ymid, st->ymid_elems * sizeof(float2));
