@@ -169,3 +169,42 @@ def test_t511_tensor_vs_direct(st, prec):
     at, ad = _both(S, ana)
     assert np.all(np.isfinite(at))
     assert _rel(at, ad) < MODE_TOL
+
+
+@pytest.mark.parametrize("K", [1, 3])
+def test_strided_views_tensor_vs_direct(st, K):
+    """Row views of larger parents (leading dimensions not multiples of 4: the FFT kernel's
+    unaligned paths) and one or three layers."""
+    import torch
+    S, So = setup(st, 127, "octa", 8)
+    c = O.random_coeffs(So.spectrum, K, seed=21 + K)
+    parent = torch.zeros(K + 2, S.spectrum.nlm + 17, dtype=torch.complex64, device="cuda")
+    parent[1:K + 1, :S.spectrum.nlm] = torch.tensor(c.T, dtype=torch.complex64, device="cuda")
+    lt = st.LowerTriangularArray(parent[1:K + 1, :S.spectrum.nlm], S.spectrum)
+    gparent = torch.full((K + 2, S.grid.npoints + 5), 7.0, device="cuda")
+
+    def syn():
+        gparent.fill_(7.0)
+        f = st.Field(gparent[1:K + 1, :S.grid.npoints], S.grid)
+        st.transform_(f, lt, S)
+        assert torch.all(gparent[0] == 7.0) and torch.all(gparent[K + 1] == 7.0)
+        assert torch.all(gparent[1:K + 1, S.grid.npoints:] == 7.0)
+        return np_of(f)
+
+    ft, fd = _both(S, syn)
+    assert _rel(ft, fd) < MODE_TOL
+    assert O.rel_err(ft, So.synthesize(c)) < TOL
+    gparent.fill_(7.0)
+    gparent[1:K + 1, :S.grid.npoints] = torch.tensor(ft.T, dtype=torch.float32, device="cuda")
+    field = st.Field(gparent[1:K + 1, :S.grid.npoints], S.grid)
+
+    def ana():
+        op = torch.full((K + 2, S.spectrum.nlm + 17), complex("nan+nanj"), dtype=torch.complex64, device="cuda")
+        out = st.LowerTriangularArray(op[1:K + 1, :S.spectrum.nlm], S.spectrum)
+        st.transform_(out, field, S)
+        assert torch.all(torch.isnan(op[0])) and torch.all(torch.isnan(op[1:K + 1, S.spectrum.nlm:]))
+        return np_of(out)
+
+    at, ad = _both(S, ana)
+    assert np.all(np.isfinite(at))
+    assert _rel(at, ad) < MODE_TOL
