@@ -172,6 +172,42 @@ __device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, flo
     }
 }
 
+// mma_step with A stored row-major, [BM][BK] (rows i, BK rings each), as the analysis
+// copies Lam rows straight into shared memory: four k at a time, a float4 per row.
+// The FMA order per accumulator (k ascending) is that of mma_step.
+template <int BN>
+__device__ __forceinline__ void mma_step_rows(const float (&Ar)[BM][BK], const float (&Bs)[BK][BN], int tx, int ty,
+                                              float (&acc)[8][BN / 16]) {
+    constexpr int TN = Cols<BN>::TN, H = Cols<BN>::H;
+#pragma unroll
+    for (int kq = 0; kq < BK; kq += 4) {
+        float4 a[8];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            a[r] = *reinterpret_cast<const float4*>(&Ar[ty * 4 + r][kq]);
+            a[4 + r] = *reinterpret_cast<const float4*>(&Ar[32 + ty * 4 + r][kq]);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int kk = kq + e;
+            float bv[TN];
+            if constexpr (Cols<BN>::SPLIT) {
+                Vec<H>::ld(&Bs[kk][tx * H], bv);
+                Vec<H>::ld(&Bs[kk][BN / 2 + tx * H], bv + H);
+            } else {
+                Vec<TN>::ld(&Bs[kk][tx * TN], bv);
+            }
+            float av[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) av[r] = e == 0 ? a[r].x : e == 1 ? a[r].y : e == 2 ? a[r].z : a[r].w;
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int c = 0; c < TN; ++c) acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
+        }
+    }
+}
+
 template <int BN>
 __device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[SS][BK][BM],
                          float (&Bs)[SS][BK][BN]) {
@@ -186,9 +222,11 @@ __device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, flo
     const int jstart = (j0m / BK) * BK;
     const int t = threadIdx.x;
     const int tx = t % 16, ty = t / 16;
-    const int a_i = t / 2, a_j = (t % 2) * 4;     // 64 rows x 8 rings: one float4 per thread
+    const int a_i = t / 2, a_j = (t % 2) * 4;     // 64 rows x 8 rings: one 16-byte copy per thread
     const int b_k = t % (BN / 2), b_j0 = t / (BN / 2);
     constexpr int BSTEP = NT / (BN / 2);
+    // Lam rows land as they are stored (rows i, rings j): [SS][BM][BK] over the same bytes
+    float (&Ar)[SS][BM][BK] = *reinterpret_cast<float (*)[SS][BM][BK]>(&As);
 
     float acc[8][TN];
 #pragma unroll
@@ -196,45 +234,39 @@ __device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, flo
 #pragma unroll
         for (int c = 0; c < TN; ++c) acc[r][c] = 0.f;
 
-    auto load_tiles = [&](int jc, float4& ra, float2 (&rb)[NB]) {
-        const int i = i_base + a_i;
-        ra = (i < rows && jc < v.nh) ? *reinterpret_cast<const float4*>(L + (int64_t)i * v.nh_pad + jc + a_j)
-                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-        const int k = kt0 + b_k;
+    // SS-stage pipeline of asynchronous copies (zero-filled outside the order's rows and
+    // the rings that carry it), as in syn_tile
+    const int k = kt0 + b_k;
+    const int i = i_base + a_i;
+    auto issue = [&](int step) {
+        const int stg = step % SS, jc = jstart + step * BK;
+        const bool aok = i < rows && jc < v.nh;
+        cp_async_zfill(&Ar[stg][a_i][a_j], aok ? L + (int64_t)i * v.nh_pad + jc + a_j : L, 16, aok ? 16 : 0);
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
             const int j = jc + b_j0 + BSTEP * q;
-            float2 x = make_float2(0.f, 0.f);
             // rings j >= j0(m) carry order m (m <= mt(j)); one load of the ring's scratch base
-            if (j < v.nh && k < v.K && j >= j0m) x = v.four[((__ldg(v.gofs + j) + m) * 2 + par) * v.K + k];
-            rb[q] = x;
+            const bool bok = j < v.nh && k < v.K && j >= j0m;
+            cp_async_zfill(&Bs[stg][b_j0 + BSTEP * q][2 * b_k],
+                           bok ? (const void*)(v.four + ((__ldg(v.gofs + j) + m) * 2 + par) * v.K + k)
+                               : (const void*)v.four,
+                           8, bok ? 8 : 0);
         }
+        cp_async_commit();
     };
-    auto store_tiles = [&](int buf, const float4& ra, const float2 (&rb)[NB]) {
-        As[buf][a_j + 0][a_i] = ra.x;
-        As[buf][a_j + 1][a_i] = ra.y;
-        As[buf][a_j + 2][a_i] = ra.z;
-        As[buf][a_j + 3][a_i] = ra.w;
+    const int nsteps = (v.nh - jstart + BK - 1) / BK;
+    __syncthreads();                               // the previous tile's reads of As/Bs are done
 #pragma unroll
-        for (int q = 0; q < NB; ++q) *reinterpret_cast<float2*>(&Bs[buf][b_j0 + BSTEP * q][2 * b_k]) = rb[q];
-    };
-
-    float4 ra;
-    float2 rb[NB];
-    __syncthreads();
-    load_tiles(jstart, ra, rb);
-    store_tiles(0, ra, rb);
-    __syncthreads();
-    int buf = 0;
-    for (int jc = jstart; jc < v.nh; jc += BK) {
-        const bool more = jc + BK < v.nh;
-        if (more) load_tiles(jc + BK, ra, rb);
-        mma_step<BN>(As[buf], Bs[buf], tx, ty, acc);
-        if (more) {
-            store_tiles(buf ^ 1, ra, rb);
-            __syncthreads();
-            buf ^= 1;
-        }
+    for (int st = 0; st < SS - 1; ++st) {
+        if (st < nsteps) issue(st);
+        else cp_async_commit();
+    }
+    for (int st = 0; st < nsteps; ++st) {
+        cp_async_wait<SS - 2>();                   // this thread's copies of step st have landed
+        __syncthreads();                           // everyone's; step st - 1's stage is free
+        if (st + SS - 1 < nsteps) issue(st + SS - 1);
+        else cp_async_commit();
+        mma_step_rows<BN>(Ar[st % SS], Bs[st % SS], tx, ty, acc);
     }
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
