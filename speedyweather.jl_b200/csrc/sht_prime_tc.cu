@@ -49,8 +49,10 @@ namespace {
 
 using namespace tcx;
 
-constexpr int PT_THREADS = 448;               // warp 0 copies, 1 MMAs, 2-9 builders, 10-13 drain
-constexpr int PT_BUILDERS = 8;
+constexpr int PT_THREADS = 576;               // warp 0 copies, 1 MMAs, 2-9 builders, 10-17 drain
+constexpr int PT_BUILDERS = 8;                // two groups of four warps, alternate units
+constexpr int PT_GROUP = 4;                   // warps per builder group
+constexpr int PT_DRAIN = 8;                   // drain warps, two per TMEM lane quarter
 constexpr int PT_TILE = 16384;                // 128 rows x 32 FP32 (128 bytes per row)
 constexpr int PT_A_SLOT = 4 * PT_TILE;        // matrix pieces (hi, lo) of up to two row tiles
 constexpr int PT_B_SLOT = 2 * PT_TILE;        // data pieces [hi rows; lo rows], up to 128 + 128 rows
@@ -133,6 +135,125 @@ __device__ __forceinline__ float2 stage_input(const PtArgs& a, const RingDesc& r
     return make_float2(gn.x + gs.y, gs.x - gn.y);
 }
 
+// hi and lo pieces of four q-values (chunk jc of the k-block) of one data row
+__device__ __forceinline__ void put_row(float* hi, float* lo, int row, int jc, float4 v) {
+    float4 h, l;
+    h.x = tf32_rn(v.x); l.x = tf32_rn(v.x - h.x);
+    h.y = tf32_rn(v.y); l.y = tf32_rn(v.y - h.y);
+    h.z = tf32_rn(v.z); l.z = tf32_rn(v.z - h.z);
+    h.w = tf32_rn(v.w); l.w = tf32_rn(v.w - h.w);
+    *reinterpret_cast<float4*>(hi + pt_swz(row, 4 * jc)) = h;
+    *reinterpret_cast<float4*>(lo + pt_swz(row, 4 * jc)) = l;
+}
+__device__ __forceinline__ float comp(const float4& v, int d) { return d == 0 ? v.x : d == 1 ? v.y : d == 2 ? v.z : v.w; }
+__device__ __forceinline__ void setc(float4& v, int d, float x) {
+    if (d == 0) v.x = x; else if (d == 1) v.y = x; else if (d == 2) v.z = x; else v.w = x;
+}
+
+// The ring fields a builder needs, read once per work item.
+struct RingIn {
+    int64_t off_n, off_s, gofs;
+    int n, mt;
+    float domega, coslat_inv;
+};
+
+// Analysis, four columns at once: layer k, i0 .. i0 + 3 (nb is a multiple of 4 on these
+// grids), q = q0 .. q0 + 3; 16-byte loads of the northern and southern rings.
+__device__ __forceinline__ void build_ana4(const PtArgs& a, const RingIn& ri, int p, int h, int nb, int k, int i0,
+                                           int q0, int mat, float* hi, float* lo, int row0, int jc) {
+    const float* gn = a.grid + (int64_t)k * a.ldg + ri.off_n + i0;
+    const float* gs = a.grid + (int64_t)k * a.ldg + ri.off_s + i0;
+    float4 nq[4], sq[4], nm[4], sm[4];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int q = q0 + e;
+        const bool in = q <= h, pair = in && q > 0;
+        nq[e] = in ? __ldg(reinterpret_cast<const float4*>(gn + q * nb)) : z4;
+        sq[e] = in ? __ldg(reinterpret_cast<const float4*>(gs + q * nb)) : z4;
+        nm[e] = pair ? __ldg(reinterpret_cast<const float4*>(gn + (p - q) * nb)) : z4;
+        sm[e] = pair ? __ldg(reinterpret_cast<const float4*>(gs + (p - q) * nb)) : z4;
+    }
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        float4 re, im;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const bool zero = mat == 1 && q0 + e == 0;             // v_0 = 0
+            setc(re, e, zero ? 0.f : mat == 0 ? comp(nq[e], d) + comp(nm[e], d) : comp(nq[e], d) - comp(nm[e], d));
+            setc(im, e, zero ? 0.f : mat == 0 ? comp(sq[e], d) + comp(sm[e], d) : comp(sq[e], d) - comp(sm[e], d));
+        }
+        put_row(hi, lo, row0 + 2 * d, jc, re);
+        put_row(hi, lo, row0 + 2 * d + 1, jc, im);
+    }
+}
+
+// Synthesis input z_t of layers k .. k + 3 (K a multiple of 4): the packed spectrum the FFT
+// kernel's prologue builds, from 16-byte loads of the scratch rows.
+__device__ __forceinline__ void syn_in4(const PtArgs& a, const RingIn& ri, int k, int t, float4& re, float4& im) {
+    const int m = 2 * t <= ri.n ? t : ri.n - t;
+    re = im = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (m > ri.mt) return;
+    const float2* er = a.four + (ri.gofs + m) * 2 * a.K + k;
+    const float2* orw = er + a.K;
+    const float4 e01 = __ldg(reinterpret_cast<const float4*>(er)), e23 = __ldg(reinterpret_cast<const float4*>(er + 2));
+    const float4 o01 = __ldg(reinterpret_cast<const float4*>(orw)), o23 = __ldg(reinterpret_cast<const float4*>(orw + 2));
+    const float scale = !a.adjoint ? (a.unscale ? ri.coslat_inv : 1.f)
+                                   : ((m == 0 || 2 * m == ri.n) ? ri.domega : 0.5f * ri.domega);
+    const float2 ev[4] = {make_float2(e01.x, e01.y), make_float2(e01.z, e01.w), make_float2(e23.x, e23.y),
+                          make_float2(e23.z, e23.w)};
+    const float2 ov[4] = {make_float2(o01.x, o01.y), make_float2(o01.z, o01.w), make_float2(o23.x, o23.y),
+                          make_float2(o23.z, o23.w)};
+    const bool selfconj = m == 0 || 2 * m == ri.n, pos = 2 * t < ri.n;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        const float2 gn = make_float2(__fmul_rn(scale, ev[l].x + ov[l].x), __fmul_rn(scale, ev[l].y + ov[l].y));
+        const float2 gs = make_float2(__fmul_rn(scale, ev[l].x - ov[l].x), __fmul_rn(scale, ev[l].y - ov[l].y));
+        setc(re, l, selfconj ? gn.x : pos ? gn.x - gs.y : gn.x + gs.y);
+        setc(im, l, selfconj ? gs.x : pos ? gn.y + gs.x : gs.x - gn.y);
+    }
+}
+
+// Synthesis, four columns at once: layers k .. k + 3 of column i0, q = q0 .. q0 + 3.
+__device__ __forceinline__ void build_syn4(const PtArgs& a, const RingIn& ri, int p, int h, int nb, int k, int i0,
+                                           int q0, int mat, float* hi, float* lo, int row0, int jc) {
+    float4 re[4], im[4];                           // [layer] over the four q
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int q = q0 + e;
+        float4 ar = make_float4(0.f, 0.f, 0.f, 0.f), ai = ar, br = ar, bi = ar;
+        if (q <= h) syn_in4(a, ri, k, i0 + q * nb, ar, ai);
+        if (q <= h && q > 0) syn_in4(a, ri, k, i0 + (p - q) * nb, br, bi);
+        const bool zero = mat == 1 && q == 0;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            setc(re[l], e, zero ? 0.f : mat == 0 ? comp(ar, l) + comp(br, l) : comp(ar, l) - comp(br, l));
+            setc(im[l], e, zero ? 0.f : mat == 0 ? comp(ai, l) + comp(bi, l) : comp(ai, l) - comp(bi, l));
+        }
+    }
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        put_row(hi, lo, row0 + 2 * l, jc, re[l]);
+        put_row(hi, lo, row0 + 2 * l + 1, jc, im[l]);
+    }
+}
+
+// tcgen05.ld of 16 columns without the wait; tmem_wait_ld waits for every load of the warp
+// and fences the registers so that no use moves above the wait.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+template <int N>
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[N]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < N; ++i) asm volatile("" : "+r"(r[i]));
+}
+
 template <bool SYN>
 __global__ void __launch_bounds__(PT_THREADS, 1) prime_stage_kernel(const PtArgs a) {
     extern __shared__ uint8_t smem_raw[];
@@ -156,11 +277,11 @@ __global__ void __launch_bounds__(PT_THREADS, 1) prime_stage_kernel(const PtArgs
             mbar_init(&a_empty[s], 1);
         }
         for (int s = 0; s < PT_B_SLOTS; ++s) {
-            mbar_init(&b_full[s], PT_BUILDERS);
+            mbar_init(&b_full[s], PT_GROUP);
             mbar_init(&b_empty[s], 1);
         }
         mbar_init(acc_full, 1);
-        mbar_init(acc_empty, 4);
+        mbar_init(acc_empty, PT_DRAIN);
         mbar_init(fin, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -256,7 +377,12 @@ __global__ void __launch_bounds__(PT_THREADS, 1) prime_stage_kernel(const PtArgs
         if (!mbar_wait(fin, 0)) atomicExch(a.err, 36);
     } else if (warp >= 2 && warp < 2 + PT_BUILDERS) {
         // ------------------------------------------------ data pieces
-        const int tb = threadIdx.x - 64;
+        // two groups of four warps take alternate units, so that one group's loads are in
+        // flight while the other's are consumed
+        const int grp = (warp - 2) / PT_GROUP;
+        const int tb = threadIdx.x - 64 - grp * 32 * PT_GROUP;
+        const bool avec = ((a.ldg & 3) == 0) && ((reinterpret_cast<uintptr_t>(a.grid) & 15) == 0);
+        const bool svec = (K & 3) == 0 && ((reinterpret_cast<uintptr_t>(a.four) & 15) == 0);
         int u = 0;
         bool ok = true;
         for (int ix = blockIdx.x; ix < a.nitems && ok; ix += gridDim.x) {
@@ -266,10 +392,21 @@ __global__ void __launch_bounds__(PT_THREADS, 1) prime_stage_kernel(const PtArgs
             const int ncols = pr.nb * K;
             if (it.y * cpi >= ncols) continue;
             const RingDesc& rd = a.rings[pr.ring];
+            RingIn ri;
+            ri.off_n = rd.off_north;
+            ri.off_s = rd.off_south;
+            ri.gofs = rd.gofs;
+            ri.n = rd.n;
+            ri.mt = rd.mt;
+            ri.domega = rd.domega;
+            ri.coslat_inv = rd.coslat_inv;
             const int p = pr.p, h = pr.h, nb = pr.nb;
             const int c0 = it.y * cpi;
+            // four columns per task: analysis (ring offsets multiples of 4 points) or synthesis
+            const bool vec = (nb & 3) == 0 && (SYN ? svec : (avec && ((ri.off_n | ri.off_s) & 3) == 0));
             for (int kb = 0; kb < pr.kb && ok; ++kb)
                 for (int mat = 0; mat < 2; ++mat, ++u) {
+                    if ((u & 1) != grp) continue;
                     const int sb = u % PT_B_SLOTS;
                     const bool got = u < PT_B_SLOTS ||
                                      __all_sync(0xffffffffu, mbar_wait(&b_empty[sb], ((u / PT_B_SLOTS) - 1) & 1));
@@ -281,45 +418,53 @@ __global__ void __launch_bounds__(PT_THREADS, 1) prime_stage_kernel(const PtArgs
                     }
                     float* hi = reinterpret_cast<float*>(bslot + (size_t)sb * PT_B_SLOT);
                     float* lo = hi + pr.nc * 32;        // the lo rows follow the nc hi rows
-                    // task: (complex column cl, 4-deep chunk jc of the k-block)
-                    for (int w = tb; w < cpi * 8; w += 32 * PT_BUILDERS) {
-                        const int cl = w % cpi, jc = w / cpi;
-                        const int c = c0 + cl;
-                        float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
-                        if (c < ncols) {
+                    if (vec) {
+                        // task: (four complex columns g, 4-deep chunk jc of the k-block)
+                        for (int w = tb; w < (cpi / 4) * 8; w += 32 * PT_GROUP) {
+                            const int g = w % (cpi / 4), jc = w / (cpi / 4);
+                            const int c = c0 + 4 * g;
+                            if (c >= ncols) {
+#pragma unroll
+                                for (int d = 0; d < 8; ++d) put_row(hi, lo, 8 * g + d, jc, make_float4(0.f, 0.f, 0.f, 0.f));
+                                continue;
+                            }
                             int k, i0;
                             col_of<SYN>(c, nb, K, k, i0);
+                            if (SYN)
+                                build_syn4(a, ri, p, h, nb, k, i0, 32 * kb + 4 * jc, mat, hi, lo, 8 * g, jc);
+                            else
+                                build_ana4(a, ri, p, h, nb, k, i0, 32 * kb + 4 * jc, mat, hi, lo, 8 * g, jc);
+                        }
+                    } else {
+                        // task: (complex column cl, 4-deep chunk jc of the k-block)
+                        for (int w = tb; w < cpi * 8; w += 32 * PT_GROUP) {
+                            const int cl = w % cpi, jc = w / cpi;
+                            const int c = c0 + cl;
+                            float4 re = make_float4(0.f, 0.f, 0.f, 0.f), im = re;
+                            if (c < ncols) {
+                                int k, i0;
+                                col_of<SYN>(c, nb, K, k, i0);
 #pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                const int q = 32 * kb + 4 * jc + e;
-                                if (q == 0) {
-                                    if (mat == 0) {
-                                        const float2 x0 = stage_input<SYN>(a, rd, k, i0);
-                                        re[e] = x0.x;
-                                        im[e] = x0.y;
+                                for (int e = 0; e < 4; ++e) {
+                                    const int q = 32 * kb + 4 * jc + e;
+                                    if (q == 0) {
+                                        if (mat == 0) {
+                                            const float2 x0 = stage_input<SYN>(a, rd, k, i0);
+                                            setc(re, e, x0.x);
+                                            setc(im, e, x0.y);
+                                        }
+                                    } else if (q <= h) {
+                                        const float2 xa = stage_input<SYN>(a, rd, k, i0 + q * nb);
+                                        const float2 xb = stage_input<SYN>(a, rd, k, i0 + (p - q) * nb);
+                                        setc(re, e, mat == 0 ? xa.x + xb.x : xa.x - xb.x);
+                                        setc(im, e, mat == 0 ? xa.y + xb.y : xa.y - xb.y);
                                     }
-                                } else if (q <= h) {
-                                    const float2 xa = stage_input<SYN>(a, rd, k, i0 + q * nb);
-                                    const float2 xb = stage_input<SYN>(a, rd, k, i0 + (p - q) * nb);
-                                    re[e] = mat == 0 ? xa.x + xb.x : xa.x - xb.x;
-                                    im[e] = mat == 0 ? xa.y + xb.y : xa.y - xb.y;
                                 }
                             }
+                            // rows 2 cl (real parts) and 2 cl + 1 (imaginary parts)
+                            put_row(hi, lo, 2 * cl, jc, re);
+                            put_row(hi, lo, 2 * cl + 1, jc, im);
                         }
-                        float4 rh, rl, ih, il;
-                        rh.x = tf32_rn(re[0]); rl.x = tf32_rn(re[0] - rh.x);
-                        rh.y = tf32_rn(re[1]); rl.y = tf32_rn(re[1] - rh.y);
-                        rh.z = tf32_rn(re[2]); rl.z = tf32_rn(re[2] - rh.z);
-                        rh.w = tf32_rn(re[3]); rl.w = tf32_rn(re[3] - rh.w);
-                        ih.x = tf32_rn(im[0]); il.x = tf32_rn(im[0] - ih.x);
-                        ih.y = tf32_rn(im[1]); il.y = tf32_rn(im[1] - ih.y);
-                        ih.z = tf32_rn(im[2]); il.z = tf32_rn(im[2] - ih.z);
-                        ih.w = tf32_rn(im[3]); il.w = tf32_rn(im[3] - ih.w);
-                        // rows 2 cl (real parts) and 2 cl + 1 (imaginary parts)
-                        *reinterpret_cast<float4*>(hi + pt_swz(2 * cl, 4 * jc)) = rh;
-                        *reinterpret_cast<float4*>(lo + pt_swz(2 * cl, 4 * jc)) = rl;
-                        *reinterpret_cast<float4*>(hi + pt_swz(2 * cl + 1, 4 * jc)) = ih;
-                        *reinterpret_cast<float4*>(lo + pt_swz(2 * cl + 1, 4 * jc)) = il;
                     }
                     fence_proxy_async();           // the MMA reads these through the async proxy
                     __syncwarp();
@@ -329,6 +474,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1) prime_stage_kernel(const PtArgs
     } else if (warp >= 2 + PT_BUILDERS) {
         // ------------------------------------------------ drain and store y
         const int quarter = warp % 4;
+        const int half = (warp - 2 - PT_BUILDERS) / 4;       // this warp's 16-column chunks: half, half + 2, ...
         const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
         int it_no = 0;
         for (int ix = blockIdx.x; ix < a.nitems; ix += gridDim.x) {
@@ -350,28 +496,24 @@ __global__ void __launch_bounds__(PT_THREADS, 1) prime_stage_kernel(const PtArgs
             for (int mt = 0; mt < pr.mtiles; ++mt) {
                 const int r = mt * 128 + quarter * 32 + lane;
                 const uint32_t tc = tmem + lane_off + (uint32_t)(mt * 2) * 2 * nc;   // cosine set; sine 2 nc on
-                for (int ch = 0; ch < nc / 32; ++ch) {
-                    float cv[32], sv[32];
-                    {
-                        float x[32];
-                        tmem_ld32(tc + ch * 32, cv);
-                        tmem_ld32(tc + nc + ch * 32, x);
-#pragma unroll
-                        for (int e = 0; e < 32; ++e) cv[e] = __fadd_rn(cv[e], x[e]);
-                        tmem_ld32(tc + 2 * nc + ch * 32, sv);
-                        tmem_ld32(tc + 3 * nc + ch * 32, x);
-#pragma unroll
-                        for (int e = 0; e < 32; ++e) sv[e] = __fadd_rn(sv[e], x[e]);
-                    }
+                for (int ch = half; ch < nc / 16; ch += 2) {
+                    uint32_t v[64];     // cosine lead, cosine cross, sine lead, sine cross: 16 columns each
+                    tmem_ld16(tc + ch * 16, *reinterpret_cast<uint32_t(*)[16]>(v));
+                    tmem_ld16(tc + nc + ch * 16, *reinterpret_cast<uint32_t(*)[16]>(v + 16));
+                    tmem_ld16(tc + 2 * nc + ch * 16, *reinterpret_cast<uint32_t(*)[16]>(v + 32));
+                    tmem_ld16(tc + 3 * nc + ch * 16, *reinterpret_cast<uint32_t(*)[16]>(v + 48));
+                    tmem_wait_ld(v);
                     if (r > h) continue;
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        const int c = it.y * cpi + ch * 16 + e;
+                    for (int e = 0; e < 8; ++e) {
+                        const int c = it.y * cpi + ch * 8 + e;
                         if (c >= ncols) continue;
                         int k, i0;
                         col_of<SYN>(c, nb, K, k, i0);
-                        const float2 A = make_float2(cv[2 * e], cv[2 * e + 1]);
-                        const float2 B = make_float2(sv[2 * e], sv[2 * e + 1]);
+                        const float2 A = make_float2(__fadd_rn(__uint_as_float(v[2 * e]), __uint_as_float(v[16 + 2 * e])),
+                                                     __fadd_rn(__uint_as_float(v[2 * e + 1]), __uint_as_float(v[17 + 2 * e])));
+                        const float2 B = make_float2(__fadd_rn(__uint_as_float(v[32 + 2 * e]), __uint_as_float(v[48 + 2 * e])),
+                                                     __fadd_rn(__uint_as_float(v[33 + 2 * e]), __uint_as_float(v[49 + 2 * e])));
                         float2* yo = ybase + (int64_t)k * n + i0 * p;
                         if (!SYN) {
                             yo[r] = make_float2(A.x + B.y, A.y - B.x);
