@@ -24,12 +24,14 @@
 // tensor core truncates each accumulator update; the leading accumulator takes one update
 // per 8 terms (at most 25 for p <= 389), and the two are added with rounding to nearest.
 //
-// Data flow. The matrices of each prime are stored once, at plan creation, as swizzled
-// (SWIZZLE_128B, K-major) FP32 tiles of 128 rows x 32 deep, contiguous per (k-block,
-// matrix), and reach shared memory by one bulk copy per k-block. Eight builder warps read
-// the stage's inputs (grid rings, or Fourier scratch rows expanded to the packed spectrum
-// exactly as the FFT kernel does), form u or v, split them and write the swizzled data
-// tile. One thread issues the MMAs; four warps drain the accumulators and store y.
+// Data flow. The matrices of each prime are stored once, when the mode is first turned
+// on, as swizzled (SWIZZLE_128B, K-major) FP32 tiles of 128 rows x 32 deep, contiguous per
+// (k-block, matrix), and reach shared memory by one bulk copy per k-block. Two groups of
+// four builder warps take alternate (k-block, matrix) units: they read the stage's inputs
+// (grid rings, or Fourier scratch rows expanded to the packed spectrum exactly as the FFT
+// kernel does; 16-byte loads of four columns where the layout allows), form u or v, split
+// them and write the swizzled data tile. One thread issues the MMAs; eight warps (two per
+// TMEM lane quarter) drain the accumulators and store y.
 // Work item: (ring, 64 or 32 complex columns), costliest first, on a persistent grid of
 // one CTA per SM. Every wait is bounded (one second); on expiry the CTA records an error
 // in the plan's status word, stops, waits for its copies and MMAs in flight and frees its
