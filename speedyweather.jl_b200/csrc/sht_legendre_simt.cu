@@ -24,7 +24,8 @@ namespace {
 constexpr int BM = 64;    // rings (synthesis) or parity rows (analysis) per CTA
 constexpr int BK = 8;     // contraction depth per shared-memory stage
 constexpr int NT = 128;   // threads
-constexpr int SS = 3;     // shared-memory stages of the synthesis tiles (asynchronous copies)
+constexpr int SS = 3;     // shared-memory stages of the tiles (asynchronous copies)
+constexpr int BPAD = 4;   // floats of padding per B row: the synthesis copies of 8 rows land in distinct banks
 
 __device__ __forceinline__ void cp_async_zfill(void* dst, const void* src, int bytes, int src_bytes) {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
@@ -73,7 +74,7 @@ struct Cols {
 };
 
 template <int BN>
-__device__ __forceinline__ void mma_step(const float (&As)[BK][BM], const float (&Bs)[BK][BN], int tx, int ty,
+__device__ __forceinline__ void mma_step(const float (&As)[BK][BM], const float (&Bs)[BK][BN + BPAD], int tx, int ty,
                                          float (&acc)[8][BN / 16]) {
     constexpr int TN = Cols<BN>::TN, H = Cols<BN>::H;
 #pragma unroll
@@ -102,7 +103,7 @@ __device__ __forceinline__ int col_of(int tx, int c) {
 
 template <int BN>
 __device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[SS][BK][BM],
-                         float (&Bs)[SS][BK][BN]) {
+                         float (&Bs)[SS][BK][BN + BPAD]) {
     constexpr int TN = BN / 16;
     constexpr int NB = BN / 32;                   // complex coefficients per thread and stage
     const int j0 = tile * BM;
@@ -113,8 +114,10 @@ __device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, flo
     const int t = threadIdx.x;
     const int tx = t % 16, ty = t / 16;
     const int a_i = t / 16, a_j = (t % 16) * 4;   // one float4 of Lam per thread
-    const int b_k = t % (BN / 2), b_i0 = t / (BN / 2);
-    constexpr int BSTEP = NT / (BN / 2);          // rows of B covered per load pass
+    // B copies: lane (row b_r of the step, layer group b_g); a warp reads 4 layers x 8 rows,
+    // i.e. 4 runs of 128 contiguous bytes of the coefficients, per instruction
+    const int b_r = t % BK, b_g = t / BK;         // b_g < 16; layers b_g + 16 q
+    static_assert(NT / BK == 16 && BN / 2 == 16 * (BN / 32), "16 layer groups of NB layers");
 
     float acc[8][TN];
 #pragma unroll
@@ -126,17 +129,19 @@ __device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, flo
     // order's rows and degrees): the copies of step st + SS - 1 are in flight while step st
     // computes; the contraction order is the same as with any other staging
     const float* La = L + j0 + a_j;
-    const int kb = kt0 + b_k;
     auto issue = [&](int step) {
         const int stg = step % SS, i0 = step * BK;
         const int i = i0 + a_i;
         const bool aok = i < rows;
         cp_async_zfill(&As[stg][a_i][a_j], aok ? La + (int64_t)i * v.nh_pad : L, 16, aok ? 16 : 0);
+        const int ii = i0 + b_r;
+        const bool rok = ii < rows && m + 2 * ii + par < v.lmax;
 #pragma unroll
         for (int q = 0; q < NB; ++q) {
-            const int ii = i0 + b_i0 + BSTEP * q;
-            const bool bok = ii < rows && m + 2 * ii + par < v.lmax && kb < v.K;
-            cp_async_zfill(&Bs[stg][b_i0 + BSTEP * q][2 * b_k],
+            const int kl = b_g + 16 * q;
+            const int kb = kt0 + kl;
+            const bool bok = rok && kb < v.K;
+            cp_async_zfill(&Bs[stg][b_r][2 * kl],
                            bok ? (const void*)(v.cin + (int64_t)kb * v.ldc + lmo + 2 * ii + par) : (const void*)v.cin, 8,
                            bok ? 8 : 0);
         }
@@ -176,7 +181,7 @@ __device__ void syn_tile(const LegView& v, int m, int tile, int ct, int par, flo
 // copies Lam rows straight into shared memory: four k at a time, a float4 per row.
 // The FMA order per accumulator (k ascending) is that of mma_step.
 template <int BN>
-__device__ __forceinline__ void mma_step_rows(const float (&Ar)[BM][BK], const float (&Bs)[BK][BN], int tx, int ty,
+__device__ __forceinline__ void mma_step_rows(const float (&Ar)[BM][BK], const float (&Bs)[BK][BN + BPAD], int tx, int ty,
                                               float (&acc)[8][BN / 16]) {
     constexpr int TN = Cols<BN>::TN, H = Cols<BN>::H;
 #pragma unroll
@@ -210,7 +215,7 @@ __device__ __forceinline__ void mma_step_rows(const float (&Ar)[BM][BK], const f
 
 template <int BN>
 __device__ void ana_tile(const LegView& v, int m, int tile, int ct, int par, float (&As)[SS][BK][BM],
-                         float (&Bs)[SS][BK][BN]) {
+                         float (&Bs)[SS][BK][BN + BPAD]) {
     constexpr int TN = BN / 16;
     constexpr int NB = BN / 32;
     const int i_base = tile * BM;
@@ -293,7 +298,7 @@ template <int BN>
 __global__ void __launch_bounds__(NT) legendre_synthesis_fp32_kernel(const LegItem* __restrict__ items,
                                                                      const LegView v) {
     __shared__ __align__(16) float As[SS][BK][BM];
-    __shared__ __align__(16) float Bs[SS][BK][BN];
+    __shared__ __align__(16) float Bs[SS][BK][BN + BPAD];
     const LegItem it = items[blockIdx.x];
     syn_tile<BN>(v, it.m, it.tile, blockIdx.y, blockIdx.z, As, Bs);
 }
@@ -302,7 +307,7 @@ template <int BN>
 __global__ void __launch_bounds__(NT) legendre_analysis_fp32_kernel(const LegItem* __restrict__ items,
                                                                     const LegView v) {
     __shared__ __align__(16) float As[SS][BK][BM];
-    __shared__ __align__(16) float Bs[SS][BK][BN];
+    __shared__ __align__(16) float Bs[SS][BK][BN + BPAD];
     const LegItem it = items[blockIdx.x];
     ana_tile<BN>(v, it.m, it.tile, blockIdx.y, blockIdx.z, As, Bs);
 }
@@ -314,7 +319,7 @@ __global__ void __launch_bounds__(NT) legendre_grouped_kernel(const LegView* __r
                                                               const GroupItem* __restrict__ items, int nitems,
                                                               int synthesis) {
     __shared__ __align__(16) float As[SS][BK][BM];
-    __shared__ __align__(16) float Bs[SS][BK][BN];
+    __shared__ __align__(16) float Bs[SS][BK][BN + BPAD];
     for (int ix = blockIdx.x; ix < nitems; ix += gridDim.x) {
         const GroupItem it = items[ix];
         const LegView& v = views[it.task];
