@@ -136,8 +136,9 @@ struct TcState {
     int nsm = 148;                 // SMs of the device (persistent grid)
     int fp16 = 0;
     int32_t* d_mexp = nullptr;
-    float* d_absmax = nullptr;     // [2 nlayers]: synthesis, analysis max-abs of the call's input
-    float2* d_kscale = nullptr;    // [2 nlayers]: (2^(e_k - 15), 2^(15 - e_k)) per layer
+    float* d_absmax = nullptr;     // [2 nlayers]: the analysis input's max-abs in [nlayers, 2 nlayers)
+                                   // (the synthesis image kernel reduces its own per order and layer)
+    float2* d_kscale = nullptr;    // [2 nlayers]: (2^(e_k - 15), 2^(15 - e_k)) per layer, analysis half used
     float2* d_mkscale = nullptr;   // [mmax][nlayers]: the same per order and layer (synthesis input)
     float ana_mul = 0.f;
 };
